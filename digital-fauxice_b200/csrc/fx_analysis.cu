@@ -1,0 +1,729 @@
+// fx_analysis.cu -- per-pixel scoring and the 9x9 reconstruction stencil.
+//
+// Kernels (all exact binary64/binary32 in the reference's order):
+//   k_auxiliary   x3a.py:193-221 derive_auxiliary with the stage y+1 alpha
+//   k_planes      x3a.py:245-286 continuous_score + streaming.py:139-147
+//                 weighted planes, written into zero/pseudo-row/repeat padded
+//                 history planes (streaming.py:201-233)
+//   k_stencil     streaming.py:454-521: decision gate, five feature records,
+//                 RGB candidates, combiner, then the writer classification
+//   k_startup     startup.py:186-353 hidden centres -6..-1 (RNG-free part)
+#include "fx_internal.cuh"
+
+namespace fx {
+
+// ---------------------------------------------------------------------------
+// Planes
+// ---------------------------------------------------------------------------
+
+__global__ void k_auxiliary(const uint16_t *__restrict__ rgbi, int h, int w,
+                            const float *__restrict__ lut, const fx_stage *__restrict__ stages,
+                            int visible, float *__restrict__ aux, uint32_t *err) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y;
+    if (x >= w || y >= h) return;
+    const fx_stage st = stages[y];  // stage y+1 (stage_parameters.py:207-212)
+    float a;
+    if (st.alpha == 1.0f) {
+        if (!st.replacement_valid) raise_error(err, FX_ERR_ALPHA_ONE_UNBOUND);
+        a = st.replacement;
+    } else {
+        const uint2 raw = reinterpret_cast<const uint2 *>(rgbi)[(int64_t)y * w + x];
+        const uint32_t lanes[4] = {raw.x & 0xFFFFu, raw.x >> 16, raw.y & 0xFFFFu, raw.y >> 16};
+        const double vis = (double)__ldg(lut + lanes[visible]);
+        const double ir = (double)__ldg(lut + lanes[3]);
+        const double alpha = (double)st.alpha;
+        const double offset = (double)st.offset;
+        a = (float)((ir - alpha * vis) / (1.0 - alpha) - offset);
+    }
+    if (!isfinite(a)) raise_error(err, FX_ERR_NONFINITE_AUX);
+    aux[(int64_t)y * w + x] = a;
+}
+
+__global__ void k_planes(const uint16_t *__restrict__ rgbi, Geometry g,
+                         const float *__restrict__ lut, const fx_stage *__restrict__ stages,
+                         fx_params p, const float *__restrict__ aux, float *__restrict__ hs,
+                         float *__restrict__ hwa, float *__restrict__ hwr, int64_t plane) {
+    const int px = blockIdx.x * blockDim.x + threadIdx.x;
+    const int py = blockIdx.y;
+    if (px >= g.pitch) return;
+    const int y = py - kPad, x = px - kPad;
+    const float floor = p.score_floor;
+    float s = 0.0f, wa = 0.0f, wr[3] = {0.0f, 0.0f, 0.0f};
+    if (x >= 0 && x < g.w && y >= -1) {
+        const int r = y < 0 ? 0 : (y < g.h ? y : g.h - 1);
+        const int64_t i = (int64_t)r * g.w + x;
+        const uint2 raw = reinterpret_cast<const uint2 *>(rgbi)[i];
+        const float rgb[3] = {__ldg(lut + (raw.x & 0xFFFFu)), __ldg(lut + (raw.x >> 16)),
+                              __ldg(lut + (raw.y & 0xFFFFu))};
+        const float a = aux[i];
+        if (y == -1) {
+            // the pseudo row above the image (streaming.py:218-228)
+            s = floor;
+            wa = a * floor;
+            for (int c = 0; c < 3; ++c) wr[c] = rgb[c] * floor;
+        } else {
+            float sample = a;
+            if (p.horizontal_minimum && g.w > 2 && x > 0 && x < g.w - 1) {
+                const float l = aux[i - 1], rr = aux[i + 1];
+                const float m = (l < a) ? l : a;
+                sample = (m < rr) ? m : rr;
+            }
+            const double primary = (double)stages[r + 1].score_base;  // stage y+2
+            double sc = (((primary + (double)p.score_addend) - (double)sample) *
+                         (double)p.score_scale) + (double)p.score_offset;
+            sc = (sc > 1.0) ? 1.0 : sc;
+            sc = (sc < (double)floor) ? (double)floor : sc;
+            s = (float)sc;
+            wa = s * a;
+            for (int c = 0; c < 3; ++c) wr[c] = s * rgb[c];
+        }
+    }
+    const int64_t o = (int64_t)py * g.pitch + px;
+    hs[o] = s;
+    hwa[o] = wa;
+    hwr[o] = wr[0];
+    hwr[o + plane] = wr[1];
+    hwr[o + 2 * plane] = wr[2];
+}
+
+// ---------------------------------------------------------------------------
+// Shared scalar pieces
+// ---------------------------------------------------------------------------
+
+struct Record {
+    float a[4];
+    uint32_t fb;  // bit l: lane l takes the consumer row's fallback value
+};
+
+// Vertical chain of one column (reconstruction.py:187-237), p = 9 samples.
+struct ColumnSums {
+    float s3, s5, s7, s9, b16;
+};
+
+__device__ __forceinline__ ColumnSums column_sums(const float v[9]) {
+    ColumnSums o;
+    double acc = (double)v[3] + (double)v[4];
+    acc += (double)v[5];
+    o.s3 = (float)acc;
+    acc += (double)v[2];
+    acc += (double)v[6];
+    o.s5 = (float)acc;
+    acc += (double)v[1];
+    acc += (double)v[7];
+    o.s7 = (float)acc;
+    acc += (double)v[0];
+    acc += (double)v[8];
+    o.s9 = (float)acc;
+    const double center = (double)v[4];
+    double b = (double)v[3] + center;
+    b += (double)v[5];
+    b += center;
+    o.b16 = (float)(b * (double)(float)(1.0 / 16.0));
+    return o;
+}
+
+// Horizontal combination (reconstruction.py:240-268).  S(k) gives the
+// column sums of patch column k (0..8).
+template <class S3, class S5, class S7, class S9>
+__device__ __forceinline__ void q69_q21(S3 s3, S5 s5, S7 s7, S9 s9, double &q69, double &q21) {
+    double t21 = (double)s3(6) + (double)s3(2);
+    t21 += (double)s5(3);
+    t21 += (double)s5(4);
+    t21 += (double)s5(5);
+    double t69 = (double)s5(8) + (double)s5(0);
+    t69 += (double)s7(1);
+    t69 += (double)s7(7);
+#pragma unroll
+    for (int x = 2; x < 7; ++x) t69 += (double)s9(x);
+    q69 = t69 * (double)(float)(1.0 / 69.0);
+    q21 = t21 * (double)(float)(1.0 / 21.0);
+}
+
+template <class B>
+__device__ __forceinline__ double q16_wa(B b16) {
+    double t = (double)b16(4) + (double)b16(3);
+    t += (double)b16(5);
+    t += (double)b16(4);
+    return t;
+}
+
+// RGB Q16 (reconstruction.py:284-298): at(i, j) is patch row 3+i, col 3+j.
+template <class A>
+__device__ __forceinline__ double q16_rgb(A at) {
+    double rows[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const double center = (double)at(i, 1);
+        double h = (double)at(i, 0) + (double)at(i, 2);
+        h += center;
+        h += center;
+        rows[i] = h;
+    }
+    double total = rows[0] + rows[1];
+    total += rows[1];
+    total += rows[2];
+    return total * (double)(float)(1.0 / 16.0);
+}
+
+// recovered_rgb_candidates (reconstruction.py:425-462), UNNORMALIZED_SUM.
+__device__ __forceinline__ float rgb_candidate(double avg, float weight) {
+    if (weight > 0.0f) {
+        const double reciprocal = 1.0 / (double)weight;
+        return (float)(avg * reciprocal);
+    }
+    return (float)avg;
+}
+
+// combine_recovered_candidate (reconstruction.py:807-887).  feats[r][l].
+__device__ bool combine(const float cand[3][3], const float source[3], const float weights[4],
+                        const float feats[5][4], int records, float coarse_reference,
+                        const fx_params &p, double out[3]) {
+    bool finite = true;
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) finite &= isfinite(cand[k][c]);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) finite &= isfinite(source[c]);
+#pragma unroll
+    for (int l = 0; l < 4; ++l) finite &= isfinite(weights[l]);
+    for (int r = 0; r < records; ++r)
+#pragma unroll
+        for (int l = 0; l < 4; ++l) finite &= isfinite(feats[r][l]);
+    if (!finite) return false;
+
+    double rmin[3], rmax[3];
+#pragma unroll
+    for (int t = 0; t < 3; ++t) {
+        double mn = (double)feats[0][t + 1] - (double)feats[0][t];
+        double mx = mn;
+        for (int r = 1; r < records; ++r) {
+            const double d = (double)feats[r][t + 1] - (double)feats[r][t];
+            mn = (d < mn) ? d : mn;
+            mx = (d > mx) ? d : mx;
+        }
+        rmin[t] = (double)(float)mn;
+        rmax[t] = (double)(float)mx;
+    }
+    double strengths[3];
+    if (p.configured_strengths[0] == 0.0f) {
+        const double v = (double)(float)(2.0 * (double)weights[1]);
+        const double lower = (v > 0.0) ? v : 0.0;
+        const double clamped = (lower < 1.0) ? lower : 1.0;
+        strengths[0] = (double)(float)clamped;
+    } else {
+        strengths[0] = (double)p.configured_strengths[0];
+    }
+    if (p.configured_strengths[1] == 0.0f) {
+        const float m2 = (weights[2] < 0.0f) ? 0.0f : weights[2];
+        strengths[1] = (double)m2;
+    } else {
+        strengths[1] = (double)p.configured_strengths[1];
+    }
+    strengths[2] = (p.configured_strengths[2] == 0.0f)
+                       ? (double)weights[3] * (double)weights[3]
+                       : (double)p.configured_strengths[2];
+
+    double candidate[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) candidate[c] = (double)cand[0][c];
+    if (p.coarse_enabled) {
+        const double delta = (double)coarse_reference - (double)feats[0][0];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            candidate[c] = candidate[c] + (double)p.coarse_slopes[c] * delta;
+    }
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+        if (!p.band_enabled[b]) continue;
+        const double scale = (double)p.band_scales[b];
+        const double emin = rmin[b], emax = rmax[b];
+        const bool negative = emin < 0.0 && emax < 0.0;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const double coarse_v = (b == 0) ? (double)cand[0][c] : (b == 1) ? (double)cand[1][c]
+                                                                              : (double)cand[2][c];
+            const double fine_v = (b == 0) ? (double)cand[1][c] : (b == 1) ? (double)cand[2][c]
+                                                                            : (double)source[c];
+            const double diff = scale * (fine_v - coarse_v);
+            const double fa = (double)p.factors_a[b * 3 + c];
+            const double fb = (double)p.factors_b[b * 3 + c];
+            const double upper = negative ? fb * emax : fa * emax;
+            const double lower = negative ? fa * emin : fb * emin;
+            double residual;
+            if (diff > upper) residual = diff - upper;
+            else if (diff < lower) residual = diff - lower;
+            else residual = 0.0;
+            candidate[c] = candidate[c] + strengths[b] * residual;
+        }
+    }
+    out[0] = candidate[0];
+    out[1] = candidate[1];
+    out[2] = candidate[2];
+    return true;
+}
+
+// Writer draw classification for one attempted site (the RNG-free part of
+// reconstruction.py:916-982).  Per channel: 0 = no draw, 1 = one draw,
+// 2 = two draws, 3 = one or two draws depending on the state.
+__device__ uint8_t classify_site(const double cand[3], const float orig[3], bool floor_enabled,
+                                 const fx_params &p, const DitherConst &dc, uint32_t *err) {
+    uint8_t meta = 0x80;
+    bool valid = true;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) valid &= isfinite(cand[c]) && cand[c] > 0.0;
+    if (!valid) return meta;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const float c32 = (float)cand[c];
+        if (!isfinite(c32)) raise_error(err, FX_ERR_DITHER_INPUT);
+        const double cd = (double)c32;
+        int code;
+        if (!dc.low_lt_high || !(dc.low < cd && cd < dc.high)) {
+            code = 0;
+        } else if (!floor_enabled) {
+            code = 1;
+        } else {
+            const double env = ((dc.high - cd) * (cd - dc.low)) * dc.coefficient;
+            const float span = (float)((double)p.dither_scales[c] * cd);
+            const double da = dither_raw_delta(cd, env, span, 0u);
+            const double db = dither_raw_delta(cd, env, span, kLcgMask);
+            double lo = (da < db) ? da : db, hi = (da < db) ? db : da;
+            lo = (lo < 0.0) ? lo : 0.0;
+            hi = (hi > 0.0) ? hi : 0.0;
+            const double od = (double)orig[c];
+            if (cand[c] + hi <= od) code = 1;        // always copies the original
+            else if (!(cand[c] + lo <= od)) code = 2;  // never copies: redraws
+            else code = 3;
+        }
+        meta |= (uint8_t)(code << (2 * c));
+    }
+    return meta;
+}
+
+// ---------------------------------------------------------------------------
+// The stencil
+// ---------------------------------------------------------------------------
+
+constexpr int PR = kTileH + 10;   // history tile rows (y0-5 .. y0+TH+4)
+constexpr int PC = kTileW + 10;   // history tile cols (x0-5 .. x0+TW+4)
+constexpr int RR = kTileH + 8;    // rgb / decision tile rows (y0-4 ..)
+constexpr int RC = kTileW + 8;    // rgb / decision tile cols (x0-4 ..)
+constexpr int CR = kTileH + 2;    // record rows (y0-1 .. y0+TH)
+constexpr int CC = kTileW + 10;   // column-sum cols (x0-5 .. x0+TW+4)
+constexpr int RECC = kTileW + 2;  // record cols (x0-1 .. x0+TW)
+constexpr int kStencilThreads = kTileH * kTileW;
+
+struct StencilSmem {
+    float hs[PR][PC];
+    float hwa[PR][PC];
+    float hwr[3][RR][RC];
+    float paux[CR][RECC];
+    float cs[2][5][CR][CC];       // [score|waux][S3,S5,S7,S9,B16]
+    float rcs[3][4][kTileH][RC];  // [channel][S3,S5,S7,S9]
+    Record rec[CR][RECC];
+    float cw[kTileH][kTileW][4];
+    uint8_t low[RR][RC];
+};
+
+__global__ void __launch_bounds__(kStencilThreads)
+    k_stencil(const uint16_t *__restrict__ rgbi, Geometry g, const float *__restrict__ lut,
+              const fx_stage *__restrict__ stages, fx_params p, const float *__restrict__ aux,
+              const float *__restrict__ hs, const float *__restrict__ hwa,
+              const float *__restrict__ hwr, int64_t plane, double *__restrict__ cand_out,
+              uint8_t *__restrict__ meta_out, uint32_t *err) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    StencilSmem &S = *reinterpret_cast<StencilSmem *>(smem_raw);
+    const int tid = threadIdx.x;
+    const int y0 = blockIdx.y * kTileH, x0 = blockIdx.x * kTileW;
+    const int h = g.h, w = g.w;
+
+    // ---- stage the tile ---------------------------------------------------
+    for (int i = tid; i < PR * PC; i += kStencilThreads) {
+        const int r = i / PC, c = i % PC;
+        const int64_t o = (int64_t)(y0 + r) * g.pitch + (x0 + c);  // padded (y0-5+r, x0-5+c)
+        S.hs[r][c] = hs[o];
+        S.hwa[r][c] = hwa[o];
+    }
+    for (int i = tid; i < 3 * RR * RC; i += kStencilThreads) {
+        const int ch = i / (RR * RC), rem = i % (RR * RC);
+        const int r = rem / RC, c = rem % RC;
+        S.hwr[ch][r][c] = hwr[ch * plane + (int64_t)(y0 + 1 + r) * g.pitch + (x0 + 1 + c)];
+    }
+    const float thr = p.decision_threshold;
+    for (int i = tid; i < RR * RC; i += kStencilThreads) {
+        const int r = i / RC, c = i % RC;
+        int yy = y0 - 4 + r, xx = x0 - 4 + c;
+        yy = yy < 0 ? 0 : (yy > h - 1 ? h - 1 : yy);
+        xx = xx < 0 ? 0 : (xx > w - 1 ? w - 1 : xx);
+        S.low[r][c] = aux[(int64_t)yy * w + xx] < thr;
+    }
+    for (int i = tid; i < CR * RECC; i += kStencilThreads) {
+        const int r = i / RECC, c = i % RECC;
+        int yy = y0 - 1 + r;
+        const int xx = x0 - 1 + c;
+        yy = yy < 0 ? 0 : (yy > h - 1 ? h - 1 : yy);
+        S.paux[r][c] = (xx >= 0 && xx < w) ? aux[(int64_t)yy * w + xx] : 0.0f;
+    }
+    __syncthreads();
+
+    // ---- vertical column sums, shared by every record of the tile ---------
+    for (int i = tid; i < 2 * CR * CC; i += kStencilThreads) {
+        const int src = i / (CR * CC), rem = i % (CR * CC);
+        const int r = rem / CC, c = rem % CC;
+        const float(*pl)[PC] = src ? S.hwa : S.hs;
+        float v[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) v[k] = pl[r + k][c];
+        const ColumnSums cs = column_sums(v);
+        S.cs[src][0][r][c] = cs.s3;
+        S.cs[src][1][r][c] = cs.s5;
+        S.cs[src][2][r][c] = cs.s7;
+        S.cs[src][3][r][c] = cs.s9;
+        S.cs[src][4][r][c] = cs.b16;
+    }
+    for (int i = tid; i < 3 * kTileH * RC; i += kStencilThreads) {
+        const int ch = i / (kTileH * RC), rem = i % (kTileH * RC);
+        const int r = rem / RC, c = rem % RC;
+        float v[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) v[k] = S.hwr[ch][r + k][c];
+        const ColumnSums cs = column_sums(v);
+        S.rcs[ch][0][r][c] = cs.s3;
+        S.rcs[ch][1][r][c] = cs.s5;
+        S.rcs[ch][2][r][c] = cs.s7;
+        S.rcs[ch][3][r][c] = cs.s9;
+    }
+    __syncthreads();
+
+    // ---- feature records (streaming.py:236-308) ---------------------------
+    for (int i = tid; i < CR * RECC; i += kStencilThreads) {
+        const int r = i / RECC, c = i % RECC;
+        const int xx = x0 - 1 + c;
+        Record rec;
+        if (xx < 0 || xx >= w) {
+            // horizontal guard records stay zero (streaming.py:281-282)
+            rec.a[0] = rec.a[1] = rec.a[2] = rec.a[3] = 0.0f;
+            rec.fb = 0;
+        } else {
+            double wq[3], nq[3];
+#pragma unroll
+            for (int src = 0; src < 2; ++src) {
+                const float(*s3)[CC] = S.cs[src][0];
+                const float(*s5)[CC] = S.cs[src][1];
+                const float(*s7)[CC] = S.cs[src][2];
+                const float(*s9)[CC] = S.cs[src][3];
+                const float(*bb)[CC] = S.cs[src][4];
+                double q69, q21;
+                q69_q21([&](int k) { return s3[r][c + k]; }, [&](int k) { return s5[r][c + k]; },
+                        [&](int k) { return s7[r][c + k]; }, [&](int k) { return s9[r][c + k]; },
+                        q69, q21);
+                const double q16 = q16_wa([&](int k) { return bb[r][c + k]; });
+                double *dst = src ? nq : wq;
+                dst[0] = q69;
+                dst[1] = q21;
+                dst[2] = q16;
+            }
+            const float point_score = S.hs[r + 4][c + 4];
+            rec.fb = 0;
+#pragma unroll
+            for (int l = 0; l < 3; ++l) {
+                if (wq[l] > 0.0) {
+                    rec.a[l] = (float)(nq[l] / wq[l]);
+                } else {
+                    rec.a[l] = 0.0f;
+                    rec.fb |= 1u << l;
+                }
+            }
+            if (point_score > 0.0f) {
+                rec.a[3] = S.paux[r][c];
+            } else {
+                rec.a[3] = 0.0f;
+                rec.fb |= 8u;
+            }
+            if (r >= 1 && r <= kTileH && c >= 1 && c <= kTileW) {
+                float *cw = S.cw[r - 1][c - 1];
+                cw[0] = (float)wq[0];
+                cw[1] = (float)wq[1];
+                cw[2] = (float)wq[2];
+                cw[3] = point_score;
+            }
+        }
+        S.rec[r][c] = rec;
+    }
+    __syncthreads();
+
+    // ---- per output pixel --------------------------------------------------
+    const int ty = tid / kTileW, tx = tid % kTileW;
+    const int y = y0 + ty, x = x0 + tx;
+    if (y >= h || x >= w) return;
+    const int64_t site = 6 * (int64_t)w + (int64_t)y * w + x;
+    const fx_stage ws = stages[y + 6];  // writer stage y+7
+    const bool floor_enabled = p.driver_gate_primary || ws.gate_secondary;
+
+    // decision bars (streaming.py:157-198), edge-replicated via the tile
+    const int rad = p.radius;
+    int vl = 0, vr = 0, ha = 0, hb = 0;
+#pragma unroll
+    for (int d = -4; d <= 4; ++d) {
+        vl += S.low[ty + 4 + d][tx + 4 - rad];
+        vr += S.low[ty + 4 + d][tx + 4 + rad];
+        ha += S.low[ty + 4 - rad][tx + 4 + d];
+        hb += S.low[ty + 4 + rad][tx + 4 + d];
+    }
+    const int lim = p.count_limit;
+    bool eligible = !(vl > lim || ha > lim || vr > lim || hb > lim);
+    const float point_score = S.cw[ty][tx][3];
+    if (ws.row_gate != 0) eligible = false;
+    else if (floor_enabled && !(point_score < 1.0f)) eligible = false;
+    // driver_forces_fallback (reconstruction.py:890-904)
+    if (eligible && (ws.row_gate != 0 || (floor_enabled && point_score >= 1.0f))) eligible = false;
+    if (!eligible) {
+        meta_out[site] = 0;
+        return;
+    }
+
+    const float fallback = ws.coarse;
+    const int records = p.cross_neighbor ? 5 : 1;
+    float feats[5][4];
+    const int rr[5] = {ty + 1, ty + 1, ty + 1, ty, ty + 2};
+    const int rc[5] = {tx + 1, tx, tx + 2, tx + 1, tx + 1};
+    for (int k = 0; k < records; ++k) {
+        const Record &rec = S.rec[rr[k]][rc[k]];
+#pragma unroll
+        for (int l = 0; l < 4; ++l) feats[k][l] = (rec.fb >> l) & 1u ? fallback : rec.a[l];
+    }
+    float weights[4];
+#pragma unroll
+    for (int l = 0; l < 4; ++l) weights[l] = S.cw[ty][tx][l];
+
+    // RGB candidates (reconstruction.py:425-462)
+    float cand[3][3];
+#pragma unroll
+    for (int ch = 0; ch < 3; ++ch) {
+        const float(*s3)[RC] = S.rcs[ch][0];
+        const float(*s5)[RC] = S.rcs[ch][1];
+        const float(*s7)[RC] = S.rcs[ch][2];
+        const float(*s9)[RC] = S.rcs[ch][3];
+        double q69, q21;
+        q69_q21([&](int k) { return s3[ty][tx + k]; }, [&](int k) { return s5[ty][tx + k]; },
+                [&](int k) { return s7[ty][tx + k]; }, [&](int k) { return s9[ty][tx + k]; }, q69,
+                q21);
+        const float(*pl)[RC] = S.hwr[ch];
+        const double q16 = q16_rgb([&](int i, int j) { return pl[ty + 3 + i][tx + 3 + j]; });
+        cand[0][ch] = rgb_candidate(q69, weights[0]);
+        cand[1][ch] = rgb_candidate(q21, weights[1]);
+        cand[2][ch] = rgb_candidate(q16, weights[2]);
+    }
+    const uint2 raw = reinterpret_cast<const uint2 *>(rgbi)[(int64_t)y * w + x];
+    const float orig[3] = {__ldg(lut + (raw.x & 0xFFFFu)), __ldg(lut + (raw.x >> 16)),
+                           __ldg(lut + (raw.y & 0xFFFFu))};
+    double combined[3];
+    if (!combine(cand, orig, weights, feats, records, ws.coarse, p, combined)) {
+        raise_error(err, FX_ERR_COMBINER_INPUT);
+        meta_out[site] = 0;
+        return;
+    }
+    const DitherConst dc = dither_const(p);
+    meta_out[site] = classify_site(combined, orig, floor_enabled, p, dc, err);
+    double *dst = cand_out + 3 * site;
+    dst[0] = combined[0];
+    dst[1] = combined[1];
+    dst[2] = combined[2];
+}
+
+// ---------------------------------------------------------------------------
+// Hidden startup replay, RNG-free part (startup.py:74-353)
+// ---------------------------------------------------------------------------
+
+struct StartupView {
+    Geometry g;
+    const float *aux, *hs, *hwa, *hwr;
+    int64_t plane;
+    int rows;  // first real rows available (5 cross-neighbour, 4 centre-only)
+};
+
+// History rows of startup.py:82-117: x outside -> 0, row -1 pseudo row,
+// rows below -1 zero, real rows 0..rows-1 (the public padded planes hold
+// exactly these values for rows -5..rows-1).
+__device__ __forceinline__ float su_plane(const StartupView &v, const float *pl, int y, int x) {
+    if (x < 0 || x >= v.g.w || y < -5) return 0.0f;
+    return pl[v.g.padded_index(y, x)];
+}
+
+// Raw decision history (startup.py:119-126) at padded column xp = x + 4.
+__device__ __forceinline__ float su_raw(const StartupView &v, int y, int xp) {
+    const int w = v.g.w;
+    const float *src = v.aux + (int64_t)(y < 0 ? 0 : y) * w;
+    if (xp < 4) return src[0];
+    if (xp < 4 + w) return src[xp - 4];
+    return y >= 0 ? src[w - 1] : 0.0f;
+}
+
+// startup.py:131-183 (weights are only needed for the centre record).
+__device__ void su_record(const StartupView &v, int ly, int x, float fallback, float weights[4],
+                          float feature[4]) {
+    if (ly <= -6 || x < 0 || x >= v.g.w) {
+#pragma unroll
+        for (int l = 0; l < 4; ++l) weights[l] = feature[l] = 0.0f;
+        return;
+    }
+    ColumnSums sc[9], wc[9];
+#pragma unroll
+    for (int j = 0; j < 9; ++j) {
+        float a[9], b[9];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+            a[i] = su_plane(v, v.hs, ly - 4 + i, x - 4 + j);
+            b[i] = su_plane(v, v.hwa, ly - 4 + i, x - 4 + j);
+        }
+        sc[j] = column_sums(a);
+        wc[j] = column_sums(b);
+    }
+    double wq[3], nq[3];
+    q69_q21([&](int k) { return sc[k].s3; }, [&](int k) { return sc[k].s5; },
+            [&](int k) { return sc[k].s7; }, [&](int k) { return sc[k].s9; }, wq[0], wq[1]);
+    wq[2] = q16_wa([&](int k) { return sc[k].b16; });
+    q69_q21([&](int k) { return wc[k].s3; }, [&](int k) { return wc[k].s5; },
+            [&](int k) { return wc[k].s7; }, [&](int k) { return wc[k].s9; }, nq[0], nq[1]);
+    nq[2] = q16_wa([&](int k) { return wc[k].b16; });
+    weights[0] = (float)wq[0];
+    weights[1] = (float)wq[1];
+    weights[2] = (float)wq[2];
+    weights[3] = su_plane(v, v.hs, ly, x);
+#pragma unroll
+    for (int l = 0; l < 3; ++l) feature[l] = (wq[l] > 0.0) ? (float)(nq[l] / wq[l]) : fallback;
+    feature[3] = (weights[3] > 0.0f) ? su_raw(v, ly, x + 4) : fallback;
+}
+
+__device__ __forceinline__ int max1(int v) { return v < 1 ? 1 : v; }
+
+__global__ void k_startup(const uint16_t *__restrict__ rgbi, StartupView v,
+                          const float *__restrict__ lut, const fx_stage *__restrict__ stages,
+                          fx_params p, double *__restrict__ cand_out, uint8_t *__restrict__ meta_out,
+                          uint32_t *err) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = blockIdx.y;  // stage hit k+1, centre k-6
+    const int w = v.g.w;
+    if (x >= w) return;
+    const int64_t site = (int64_t)k * w + x;
+    const int hit = k + 1, center = k - 6;
+    const fx_stage act = stages[hit - 1];
+    const bool floor_enabled = p.driver_gate_primary || act.gate_secondary;
+    const int writer_width = (p.cross_neighbor && hit <= 2) ? w - 4 : w;
+    if (x >= writer_width) {
+        meta_out[site] = 0;
+        return;
+    }
+    const int r = p.radius;
+    bool fallback_hit = false;
+    for (int gi = 0; gi < 4 && !fallback_hit; ++gi) {
+        int count = 0;
+        for (int s = 0; s < 9; ++s) {
+            const int axis = s - 4;
+            const int dy = (gi == 0 || gi == 2) ? axis : (gi == 1 ? -r : r);
+            const int dx = (gi == 0) ? -r : (gi == 2 ? r : axis);
+            count += su_raw(v, center + dy, x + 4 + dx) < p.decision_threshold;
+        }
+        if (count > p.count_limit) fallback_hit = true;
+    }
+    const float fb_center = stages[max1(center + 6) - 1].coarse;
+    float weights[4], feats[5][4];
+    su_record(v, center, x, fb_center, weights, feats[0]);
+    if (fallback_hit || act.row_gate != 0 || (floor_enabled && weights[3] >= 1.0f)) {
+        meta_out[site] = 0;
+        return;
+    }
+    float cand[3][3];
+#pragma unroll
+    for (int ch = 0; ch < 3; ++ch) {
+        const float *pl = v.hwr + ch * v.plane;
+        ColumnSums cs[9];
+#pragma unroll
+        for (int j = 0; j < 9; ++j) {
+            float a[9];
+#pragma unroll
+            for (int i = 0; i < 9; ++i) a[i] = su_plane(v, pl, center - 4 + i, x - 4 + j);
+            cs[j] = column_sums(a);
+        }
+        double q69, q21;
+        q69_q21([&](int kk) { return cs[kk].s3; }, [&](int kk) { return cs[kk].s5; },
+                [&](int kk) { return cs[kk].s7; }, [&](int kk) { return cs[kk].s9; }, q69, q21);
+        const double q16 = q16_rgb(
+            [&](int i, int j) { return su_plane(v, pl, center - 1 + i, x - 1 + j); });
+        cand[0][ch] = rgb_candidate(q69, weights[0]);
+        cand[1][ch] = rgb_candidate(q21, weights[1]);
+        cand[2][ch] = rgb_candidate(q16, weights[2]);
+    }
+    const int records = p.cross_neighbor ? 5 : 1;
+    if (records == 5) {
+        float wn[4];
+        const float fb_up = stages[max1(center + 5) - 1].coarse;
+        const float fb_down = stages[max1(center + 7) - 1].coarse;
+        su_record(v, center, x - 1, fb_center, wn, feats[1]);
+        su_record(v, center, x + 1, fb_center, wn, feats[2]);
+        su_record(v, center - 1, x, fb_up, wn, feats[3]);
+        su_record(v, center + 1, x, fb_down, wn, feats[4]);
+    }
+    const uint2 raw = reinterpret_cast<const uint2 *>(rgbi)[x];  // row 0
+    const float orig[3] = {__ldg(lut + (raw.x & 0xFFFFu)), __ldg(lut + (raw.x >> 16)),
+                           __ldg(lut + (raw.y & 0xFFFFu))};
+    double combined[3];
+    if (!combine(cand, orig, weights, feats, records, act.coarse, p, combined)) {
+        raise_error(err, FX_ERR_COMBINER_INPUT);
+        meta_out[site] = 0;
+        return;
+    }
+    const DitherConst dc = dither_const(p);
+    meta_out[site] = classify_site(combined, orig, floor_enabled, p, dc, err);
+    double *dst = cand_out + 3 * site;
+    dst[0] = combined[0];
+    dst[1] = combined[1];
+    dst[2] = combined[2];
+}
+
+// ---------------------------------------------------------------------------
+// Launchers
+// ---------------------------------------------------------------------------
+
+cudaError_t launch_analysis(const uint16_t *rgbi, const Geometry &g, const float *lut,
+                            const fx_stage *stages, const fx_params &p, float *aux, float *hs,
+                            float *hwa, float *hwr, int64_t plane, double *cand, uint8_t *meta,
+                            uint32_t *err, cudaStream_t stream) {
+    {
+        dim3 block(256), grid((g.w + 255) / 256, g.h);
+        k_auxiliary<<<grid, block, 0, stream>>>(rgbi, g.h, g.w, lut, stages, p.visible_channel,
+                                                aux, err);
+    }
+    {
+        dim3 block(256), grid((g.pitch + 255) / 256, g.prow);
+        k_planes<<<grid, block, 0, stream>>>(rgbi, g, lut, stages, p, aux, hs, hwa, hwr, plane);
+    }
+    {
+        dim3 grid(g.tw, g.th);
+        k_stencil<<<grid, kStencilThreads, sizeof(StencilSmem), stream>>>(
+            rgbi, g, lut, stages, p, aux, hs, hwa, hwr, plane, cand, meta, err);
+    }
+    {
+        StartupView v{g, aux, hs, hwa, hwr, plane, p.cross_neighbor ? 5 : 4};
+        dim3 block(128), grid((g.w + 127) / 128, 6);
+        k_startup<<<grid, block, 0, stream>>>(rgbi, v, lut, stages, p, cand, meta, err);
+    }
+    return cudaGetLastError();
+}
+
+size_t stencil_smem_bytes() { return sizeof(StencilSmem); }
+
+cudaError_t producer_init();
+
+// Opt in to the dynamic shared memory the tiled kernels use (once per
+// device, with the device current).
+cudaError_t analysis_init() {
+    cudaError_t e = cudaFuncSetAttribute(k_stencil, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)sizeof(StencilSmem));
+    if (e != cudaSuccess) return e;
+    return producer_init();
+}
+
+}  // namespace fx

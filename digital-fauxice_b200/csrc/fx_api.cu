@@ -1,0 +1,736 @@
+// fx_api.cu -- C ABI, device memory and per-frame pipelines.
+#include <chrono>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "fx_internal.cuh"
+
+namespace fx {
+
+static Geometry make_geometry(int h, int w) {
+    Geometry g;
+    g.h = h;
+    g.w = w;
+    g.th = (h + kTileH - 1) / kTileH;
+    g.tw = (w + kTileW - 1) / kTileW;
+    g.hp = g.th * kTileH;
+    g.wp = g.tw * kTileW;
+    g.prow = g.hp + 2 * kPad;
+    g.pitch = ((g.wp + 2 * kPad) + 31) / 32 * 32;
+    g.sites = 6 * (int64_t)w + (int64_t)h * w;
+    g.segments = (g.sites + kSegment - 1) / kSegment;
+    return g;
+}
+
+static int64_t default_amb_capacity(const Geometry &g) {
+    const int64_t c = g.sites / 2;
+    return c < 65536 ? 65536 : c;
+}
+
+// One frame's device buffers, carved from a single allocation.
+struct Arena {
+    void *base = nullptr;
+    size_t bytes = 0;
+    uint16_t *rgbi = nullptr;
+    fx_stage *stages = nullptr;
+    float *aux = nullptr, *hs = nullptr, *hwa = nullptr, *hwr = nullptr;
+    double *cand = nullptr;
+    uint8_t *meta = nullptr;
+    uint32_t *seg_base = nullptr, *seg_amb = nullptr;
+    AmbEntry *entries = nullptr;
+    uint32_t *pos = nullptr, *extra = nullptr;
+    void *producer = nullptr;
+    float *rows = nullptr;
+    uint16_t *out = nullptr;
+    uint8_t *changed = nullptr;
+    void *counters = nullptr;
+    uint32_t *err = nullptr;
+    int64_t amb_capacity = 0;
+};
+
+static size_t arena_layout(const Geometry &g, int64_t amb_cap, Arena *a) {
+    size_t off = 0;
+    auto take = [&](size_t n) {
+        const size_t o = off;
+        off += (n + 255) & ~(size_t)255;
+        return o;
+    };
+    const int64_t px = (int64_t)g.h * g.w;
+    const int64_t plane = (int64_t)g.prow * g.pitch;
+    const size_t o_rgbi = take(px * 8);
+    const size_t o_stages = take((g.h + 6) * sizeof(fx_stage));
+    const size_t o_aux = take(px * 4);
+    const size_t o_hs = take(plane * 4);
+    const size_t o_hwa = take(plane * 4);
+    const size_t o_hwr = take(3 * plane * 4);
+    const size_t o_cand = take(g.sites * 24);
+    const size_t o_meta = take(g.sites);
+    const size_t o_sb = take((g.segments + 1) * 4);
+    const size_t o_sa = take((g.segments + 1) * 4);
+    const size_t o_ent = take(amb_cap * sizeof(AmbEntry) + 64);
+    const size_t o_pos = take(amb_cap * 4);
+    const size_t o_ext = take(amb_cap * 4);
+    const size_t o_prod = take(producer_bytes(g.h, g.w));
+    const size_t o_rows = take(4 * (size_t)g.h * 4);
+    const size_t o_out = take(px * 6);
+    const size_t o_chg = take(px);
+    const size_t o_ctr = take(dev_counters_bytes());
+    const size_t o_err = take(16);
+    if (a) {
+        char *b = reinterpret_cast<char *>(a->base);
+        a->rgbi = (uint16_t *)(b + o_rgbi);
+        a->stages = (fx_stage *)(b + o_stages);
+        a->aux = (float *)(b + o_aux);
+        a->hs = (float *)(b + o_hs);
+        a->hwa = (float *)(b + o_hwa);
+        a->hwr = (float *)(b + o_hwr);
+        a->cand = (double *)(b + o_cand);
+        a->meta = (uint8_t *)(b + o_meta);
+        a->seg_base = (uint32_t *)(b + o_sb);
+        a->seg_amb = (uint32_t *)(b + o_sa);
+        a->entries = (AmbEntry *)(b + o_ent);
+        a->pos = (uint32_t *)(b + o_pos);
+        a->extra = (uint32_t *)(b + o_ext);
+        a->producer = (void *)(b + o_prod);
+        a->rows = (float *)(b + o_rows);
+        a->out = (uint16_t *)(b + o_out);
+        a->changed = (uint8_t *)(b + o_chg);
+        a->counters = (void *)(b + o_ctr);
+        a->err = (uint32_t *)(b + o_err);
+        a->amb_capacity = amb_cap;
+    }
+    return off;
+}
+
+struct Slot {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+    Arena arena;
+    // pinned staging for asynchronous requests
+    void *h_in = nullptr;
+    size_t h_in_bytes = 0;
+    void *h_out = nullptr;
+    size_t h_out_bytes = 0;
+    void *h_ctr = nullptr;  // DevCounters copy + error word
+    // request in flight
+    bool busy = false;
+    int64_t ticket = -1;
+    fx_frame frame{};
+    fx_params params{};
+    std::vector<fx_stage> stages;
+    bool has_stages = false;
+    Geometry g{};
+};
+
+}  // namespace fx
+
+struct fx_context {
+    int device = 0;
+    float *lut = nullptr;
+    uint32_t *high = nullptr, *low = nullptr;
+    bool tables = false;
+    std::vector<fx::Slot> slots;
+    int64_t next_ticket = 1;
+    std::mutex mu;
+    char error[512] = {0};
+};
+
+namespace fx {
+
+static char g_error[512];
+
+static int fail(fx_context *ctx, int code, const char *fmt, ...) {
+    char *buf = ctx ? ctx->error : g_error;
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, 512, fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+#define FX_CUDA(ctx, call)                                                                 \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess)                                                             \
+            return fail((ctx), FX_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+static int ensure_arena(fx_context *ctx, Slot &s, const Geometry &g, int64_t amb_cap) {
+    Arena probe;
+    const size_t need = arena_layout(g, amb_cap, nullptr);
+    if (s.arena.base && s.arena.bytes >= need) {
+        const size_t bytes = s.arena.bytes;
+        void *base = s.arena.base;
+        s.arena = Arena();
+        s.arena.base = base;
+        s.arena.bytes = bytes;
+        arena_layout(g, amb_cap, &s.arena);
+        return FX_OK;
+    }
+    if (s.arena.base) {
+        cudaStreamSynchronize(s.stream);
+        cudaFree(s.arena.base);
+        s.arena = Arena();
+    }
+    void *base = nullptr;
+    const cudaError_t e = cudaMalloc(&base, need);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(ctx, FX_ERR_OUT_OF_MEMORY, "device allocation of %zu bytes failed: %s", need,
+                    cudaGetErrorString(e));
+    }
+    s.arena.base = base;
+    s.arena.bytes = need;
+    arena_layout(g, amb_cap, &s.arena);
+    (void)probe;
+    return FX_OK;
+}
+
+static int check_frame(fx_context *ctx, const fx_params *p, int h, int w) {
+    if (!ctx) return FX_ERR_INVALID_ARGUMENT;
+    if (!ctx->tables) return fail(ctx, FX_ERR_TABLES, "fx_set_tables has not been called");
+    if (!p || h < 1 || w < 1) return fail(ctx, FX_ERR_INVALID_ARGUMENT, "bad frame arguments");
+    if ((int64_t)h * w > (int64_t)1 << 30)
+        return fail(ctx, FX_ERR_INVALID_ARGUMENT, "frame too large");
+    if (p->visible_channel < 0 || p->visible_channel > 2 || p->radius < 1 || p->radius > 4)
+        return fail(ctx, FX_ERR_INVALID_ARGUMENT, "bad parameters");
+    // streaming.py:391-392 and startup.py:210-213 / fast_cpu/engine.py:148-154
+    if (h < 4) return fail(ctx, FX_ERR_GEOMETRY, "streaming startup requires at least four main rows");
+    if (p->cross_neighbor && h < 5)
+        return fail(ctx, FX_ERR_GEOMETRY, "cross-neighbor startup requires the first five real rows");
+    if (p->cross_neighbor && w < 4)
+        return fail(ctx, FX_ERR_GEOMETRY, "cross-neighbor startup requires at least four columns");
+    if (!isfinite(p->dither_low) || !isfinite(p->dither_high))
+        return fail(ctx, FX_ERR_DITHER_INPUT, "dither inputs must be finite");
+    for (int c = 0; c < 3; ++c)
+        if (!isfinite(p->dither_scales[c]))
+            return fail(ctx, FX_ERR_DITHER_INPUT, "dither inputs must be finite");
+    return FX_OK;
+}
+
+// Enqueue the whole pass for one frame whose input already sits in
+// s.arena.rgbi (or `d_in`).  Outputs land in the arena (or `d_out`).
+static int enqueue_pass(fx_context *ctx, Slot &s, const Geometry &g, const fx_params &p,
+                        const fx_stage *host_stages, uint32_t rng, const uint16_t *d_in,
+                        uint16_t *d_out, uint8_t *d_changed, bool producer_rows) {
+    Arena &a = s.arena;
+    cudaStream_t st = s.stream;
+    FX_CUDA(ctx, cudaMemsetAsync(a.err, 0, 16, st));
+    if (host_stages) {
+        FX_CUDA(ctx, cudaMemcpyAsync(a.stages, host_stages, (g.h + 6) * sizeof(fx_stage),
+                                     cudaMemcpyHostToDevice, st));
+    } else {
+        FX_CUDA(ctx, launch_producer(d_in, g.h, g.w, ctx->lut, a.producer, a.stages,
+                                     producer_rows ? a.rows : nullptr, a.err, st));
+    }
+    FX_CUDA(ctx, launch_analysis(d_in, g, ctx->lut, a.stages, p, a.aux, a.hs, a.hwa, a.hwr,
+                                 (int64_t)g.prow * g.pitch, a.cand, a.meta, a.err, st));
+    WriterBuffers wb{a.seg_base, a.seg_amb, a.entries, a.pos, a.extra, a.counters,
+                     a.amb_capacity};
+    FX_CUDA(ctx, launch_writer(g, a.meta, a.cand, d_in, ctx->lut, ctx->high, ctx->low, a.stages,
+                               p, rng, wb, d_out, d_changed, a.err, st));
+    return FX_OK;
+}
+
+static int error_from_device(fx_context *ctx, uint32_t code) {
+    switch (code) {
+    case FX_ERR_NONFINITE_AUX:
+        return fail(ctx, (int)code, "auxiliary score input must be a finite HxW plane");
+    case FX_ERR_NONFINITE_WORK:
+        return fail(ctx, (int)code, "work RGB must be finite");
+    case FX_ERR_COMBINER_INPUT:
+        return fail(ctx, (int)code, "combiner inputs must be finite");
+    case FX_ERR_DITHER_INPUT:
+        return fail(ctx, (int)code, "dither inputs must be finite");
+    case FX_ERR_SETTER_ONE:
+        return fail(ctx, (int)code, "X3A setter scale cannot equal one");
+    case FX_ERR_STAGE_NONFINITE:
+        return fail(ctx, (int)code, "stage calibration contains a non-finite value");
+    case FX_ERR_ALPHA_ONE_UNBOUND:
+        return fail(ctx, (int)code,
+                    "alpha==1 requires the runtime-configured auxiliary replacement");
+    default:
+        return fail(ctx, FX_ERR_INTERNAL, "device consistency check failed (code %u)", code);
+    }
+}
+
+// Counters + error word of the slot, after the stream completed.
+static int finish_counters(fx_context *ctx, Slot &s, const void *ctr_copy, uint32_t err,
+                           fx_counters *out, bool *overflow) {
+    *overflow = false;
+    if (err) return error_from_device(ctx, err);
+    if ((int64_t)counters_n_amb(ctr_copy) > s.arena.amb_capacity) {
+        *overflow = true;
+        return FX_OK;
+    }
+    if (out) counters_to_host(ctr_copy, out);
+    return FX_OK;
+}
+
+static Slot &slot0(fx_context *ctx) { return ctx->slots[0]; }
+
+static int ensure_slots(fx_context *ctx, int n) {
+    while ((int)ctx->slots.size() < n) {
+        ctx->slots.emplace_back();
+        Slot &s = ctx->slots.back();
+        FX_CUDA(ctx, cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking));
+        FX_CUDA(ctx, cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming));
+        FX_CUDA(ctx, cudaMallocHost(&s.h_ctr, dev_counters_bytes() + 64));
+    }
+    return FX_OK;
+}
+
+// Synchronous pass over device buffers on the slot's stream, with the
+// amb-capacity retry.
+static int run_device(fx_context *ctx, Slot &s, const Geometry &g, const fx_params &p,
+                      const fx_stage *stages, uint32_t rng, const uint16_t *d_in, uint16_t *d_out,
+                      uint8_t *d_changed, fx_counters *counters, bool producer_rows) {
+    int64_t cap = s.arena.base ? s.arena.amb_capacity : default_amb_capacity(g);
+    if (cap < default_amb_capacity(g)) cap = default_amb_capacity(g);
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        // keep caller-side device pointers stable: the arena may move only
+        // when the input/outputs live in it
+        int rc = ensure_arena(ctx, s, g, cap);
+        if (rc) return rc;
+        const uint16_t *in = d_in ? d_in : s.arena.rgbi;
+        uint16_t *out = d_out ? d_out : s.arena.out;
+        uint8_t *chg = d_changed ? d_changed : s.arena.changed;
+        rc = enqueue_pass(ctx, s, g, p, stages, rng, in, out, chg, producer_rows);
+        if (rc) return rc;
+        char *hc = reinterpret_cast<char *>(s.h_ctr);
+        FX_CUDA(ctx, cudaMemcpyAsync(hc, s.arena.counters, dev_counters_bytes(),
+                                     cudaMemcpyDeviceToHost, s.stream));
+        FX_CUDA(ctx, cudaMemcpyAsync(hc + dev_counters_bytes(), s.arena.err, 4,
+                                     cudaMemcpyDeviceToHost, s.stream));
+        FX_CUDA(ctx, cudaStreamSynchronize(s.stream));
+        uint32_t err;
+        std::memcpy(&err, hc + dev_counters_bytes(), 4);
+        bool overflow;
+        rc = finish_counters(ctx, s, hc, err, counters, &overflow);
+        if (rc) return rc;
+        if (!overflow) return FX_OK;
+        cap = (int64_t)counters_n_amb(hc) + 1024;
+        if (!d_in) return fail(ctx, FX_ERR_INTERNAL, "amb capacity retry needs the input");
+    }
+    return fail(ctx, FX_ERR_INTERNAL, "amb capacity retry failed");
+}
+
+}  // namespace fx
+
+using namespace fx;
+
+extern "C" {
+
+FX_API int fx_version(void) { return FX_ABI_VERSION; }
+
+FX_API int fx_device_check(int device, char *reason, size_t reason_len) {
+    auto say = [&](int code, const char *msg) {
+        if (reason && reason_len) snprintf(reason, reason_len, "%s", msg);
+        return code;
+    };
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return say(FX_ERR_NO_DEVICE, "no CUDA device is visible");
+    }
+    if (device < 0 || device >= count) return say(FX_ERR_NO_DEVICE, "device index out of range");
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess)
+        return say(FX_ERR_NO_DEVICE, "cannot query the CUDA device");
+    if (prop.major != 10 || prop.minor != 0) {
+        char buf[160];
+        snprintf(buf, sizeof(buf), "device %s is sm_%d%d; this library is built for sm_100a",
+                 prop.name, prop.major, prop.minor);
+        return say(FX_ERR_UNSUPPORTED_DEVICE, buf);
+    }
+    return say(FX_OK, "ok");
+}
+
+FX_API int fx_context_create(int device, fx_context **out) {
+    if (!out) return FX_ERR_INVALID_ARGUMENT;
+    *out = nullptr;
+    char reason[160];
+    const int rc = fx_device_check(device, reason, sizeof(reason));
+    if (rc) return fail(nullptr, rc, "%s", reason);
+    fx_context *ctx = new fx_context();
+    ctx->device = device;
+    if (cudaSetDevice(device) != cudaSuccess) {
+        delete ctx;
+        return fail(nullptr, FX_ERR_CUDA, "cudaSetDevice failed");
+    }
+    if (analysis_init() != cudaSuccess || ensure_slots(ctx, 1) != FX_OK ||
+        cudaMalloc(&ctx->lut, 65536 * 4) != cudaSuccess ||
+        cudaMalloc(&ctx->high, 256 * 4) != cudaSuccess ||
+        cudaMalloc(&ctx->low, 256 * 4) != cudaSuccess) {
+        cudaGetLastError();
+        fx_context_destroy(ctx);
+        return fail(nullptr, FX_ERR_CUDA, "context initialisation failed");
+    }
+    *out = ctx;
+    return FX_OK;
+}
+
+FX_API void fx_context_destroy(fx_context *ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    for (Slot &s : ctx->slots) {
+        if (s.stream) cudaStreamSynchronize(s.stream);
+        if (s.arena.base) cudaFree(s.arena.base);
+        if (s.h_in) cudaFreeHost(s.h_in);
+        if (s.h_out) cudaFreeHost(s.h_out);
+        if (s.h_ctr) cudaFreeHost(s.h_ctr);
+        if (s.done) cudaEventDestroy(s.done);
+        if (s.stream) cudaStreamDestroy(s.stream);
+    }
+    if (ctx->lut) cudaFree(ctx->lut);
+    if (ctx->high) cudaFree(ctx->high);
+    if (ctx->low) cudaFree(ctx->low);
+    delete ctx;
+}
+
+FX_API int fx_last_error(const fx_context *ctx, char *buf, size_t len) {
+    if (!buf || !len) return FX_ERR_INVALID_ARGUMENT;
+    snprintf(buf, len, "%s", ctx ? ctx->error : g_error);
+    return FX_OK;
+}
+
+FX_API int fx_set_tables(fx_context *ctx, const float *lut, const uint32_t *high,
+                         const uint32_t *low) {
+    if (!ctx || !lut || !high || !low) return FX_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    cudaSetDevice(ctx->device);
+    FX_CUDA(ctx, cudaMemcpy(ctx->lut, lut, 65536 * 4, cudaMemcpyHostToDevice));
+    FX_CUDA(ctx, cudaMemcpy(ctx->high, high, 256 * 4, cudaMemcpyHostToDevice));
+    FX_CUDA(ctx, cudaMemcpy(ctx->low, low, 256 * 4, cudaMemcpyHostToDevice));
+    ctx->tables = true;
+    return FX_OK;
+}
+
+FX_API int fx_reduce_prepass(const uint16_t *prepass, int32_t h, int32_t w, const float *lut,
+                             uint8_t payload[64], int64_t *valid, int64_t *tiles) {
+    if (!prepass || !lut || !payload || h < 1 || w < 1) return FX_ERR_INVALID_ARGUMENT;
+    return host_reduce_prepass(prepass, h, w, lut, payload, valid, tiles);
+}
+
+FX_API int fx_stage_table(int32_t h, const float *p1, const float *p2, const float *mv,
+                          const float *mi, float factor_b, fx_stage *stages) {
+    if (h < 1 || !p1 || !p2 || !mv || !mi || !stages) return FX_ERR_INVALID_ARGUMENT;
+    return host_stage_table(h, p1, p2, mv, mi, factor_b, stages);
+}
+
+FX_API int fx_producer_rows(fx_context *ctx, const uint16_t *main_rgbi, int32_t h, int32_t w,
+                            float *p1, float *p2, float *mv, float *mi) {
+    if (!ctx || !main_rgbi || h < 1 || w < 8 || !p1 || !p2 || !mv || !mi)
+        return FX_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    cudaSetDevice(ctx->device);
+    if (!ctx->tables) return fail(ctx, FX_ERR_TABLES, "fx_set_tables has not been called");
+    Slot &s = slot0(ctx);
+    const Geometry g = make_geometry(h, w);
+    int rc = ensure_arena(ctx, s, g, default_amb_capacity(g));
+    if (rc) return rc;
+    FX_CUDA(ctx, cudaMemsetAsync(s.arena.err, 0, 16, s.stream));
+    FX_CUDA(ctx, cudaMemcpyAsync(s.arena.rgbi, main_rgbi, (size_t)h * w * 8,
+                                 cudaMemcpyHostToDevice, s.stream));
+    FX_CUDA(ctx, launch_producer(s.arena.rgbi, h, w, ctx->lut, s.arena.producer, s.arena.stages,
+                                 s.arena.rows, s.arena.err, s.stream));
+    std::vector<float> rows(4 * (size_t)h);
+    uint32_t err = 0;
+    FX_CUDA(ctx, cudaMemcpyAsync(rows.data(), s.arena.rows, rows.size() * 4,
+                                 cudaMemcpyDeviceToHost, s.stream));
+    FX_CUDA(ctx, cudaMemcpyAsync(&err, s.arena.err, 4, cudaMemcpyDeviceToHost, s.stream));
+    FX_CUDA(ctx, cudaStreamSynchronize(s.stream));
+    std::memcpy(p1, rows.data(), h * 4);
+    std::memcpy(p2, rows.data() + h, h * 4);
+    std::memcpy(mv, rows.data() + 2 * (size_t)h, h * 4);
+    std::memcpy(mi, rows.data() + 3 * (size_t)h, h * 4);
+    if (err && err != FX_ERR_SETTER_ONE && err != FX_ERR_STAGE_NONFINITE)
+        return error_from_device(ctx, err);
+    return FX_OK;
+}
+
+FX_API int fx_process(fx_context *ctx, const fx_frame *f, fx_counters *counters) {
+    if (!ctx || !f || !f->main_rgbi || !f->rgb_out) return FX_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    cudaSetDevice(ctx->device);
+    int rc = check_frame(ctx, f->params, f->height, f->width);
+    if (rc) return rc;
+    if (!f->stages && f->width < 8)
+        return fail(ctx, FX_ERR_GEOMETRY, "main RGBI frame has no complete producer cell");
+    Slot &s = slot0(ctx);
+    const Geometry g = make_geometry(f->height, f->width);
+    const size_t px = (size_t)g.h * g.w;
+    int64_t cap = default_amb_capacity(g);
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        rc = ensure_arena(ctx, s, g, cap);
+        if (rc) return rc;
+        FX_CUDA(ctx, cudaMemcpyAsync(s.arena.rgbi, f->main_rgbi, px * 8, cudaMemcpyHostToDevice,
+                                     s.stream));
+        rc = enqueue_pass(ctx, s, g, *f->params, f->stages, f->rng_state, s.arena.rgbi,
+                          s.arena.out, s.arena.changed, false);
+        if (rc) return rc;
+        char *hc = reinterpret_cast<char *>(s.h_ctr);
+        FX_CUDA(ctx, cudaMemcpyAsync(hc, s.arena.counters, dev_counters_bytes(),
+                                     cudaMemcpyDeviceToHost, s.stream));
+        FX_CUDA(ctx, cudaMemcpyAsync(hc + dev_counters_bytes(), s.arena.err, 4,
+                                     cudaMemcpyDeviceToHost, s.stream));
+        FX_CUDA(ctx, cudaStreamSynchronize(s.stream));
+        uint32_t err;
+        std::memcpy(&err, hc + dev_counters_bytes(), 4);
+        bool overflow;
+        rc = finish_counters(ctx, s, hc, err, counters, &overflow);
+        if (rc) return rc;
+        if (overflow) {
+            cap = (int64_t)counters_n_amb(hc) + 1024;
+            continue;
+        }
+        FX_CUDA(ctx, cudaMemcpy(f->rgb_out, s.arena.out, px * 6, cudaMemcpyDeviceToHost));
+        if (f->score_out)
+            FX_CUDA(ctx, cudaMemcpy2D(f->score_out, (size_t)g.w * 4,
+                                      s.arena.hs + g.padded_index(0, 0), (size_t)g.pitch * 4,
+                                      (size_t)g.w * 4, g.h, cudaMemcpyDeviceToHost));
+        if (f->changed_out)
+            FX_CUDA(ctx, cudaMemcpy(f->changed_out, s.arena.changed, px, cudaMemcpyDeviceToHost));
+        return FX_OK;
+    }
+    return fail(ctx, FX_ERR_INTERNAL, "amb capacity retry failed");
+}
+
+FX_API int fx_process_device(fx_context *ctx, const uint16_t *d_rgbi, int32_t h, int32_t w,
+                             const fx_params *params, const fx_stage *stages, uint32_t rng,
+                             uint16_t *d_out, float *d_score, uint8_t *d_changed, void *stream,
+                             fx_counters *counters) {
+    if (!ctx || !d_rgbi || !d_out) return FX_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    cudaSetDevice(ctx->device);
+    int rc = check_frame(ctx, params, h, w);
+    if (rc) return rc;
+    if (!stages && w < 8)
+        return fail(ctx, FX_ERR_GEOMETRY, "main RGBI frame has no complete producer cell");
+    Slot &s = slot0(ctx);
+    cudaStream_t user = reinterpret_cast<cudaStream_t>(stream);
+    cudaStream_t saved = s.stream;
+    if (user) s.stream = user;
+    const Geometry g = make_geometry(h, w);
+    if (counters) {
+        rc = run_device(ctx, s, g, *params, stages, rng, d_rgbi, d_out, d_changed, counters, false);
+    } else {
+        rc = ensure_arena(ctx, s, g, default_amb_capacity(g));
+        if (!rc) rc = enqueue_pass(ctx, s, g, *params, stages, rng, d_rgbi, d_out, d_changed, false);
+    }
+    if (!rc && d_score)
+        rc = cudaMemcpy2DAsync(d_score, (size_t)w * 4, s.arena.hs + g.padded_index(0, 0),
+                               (size_t)g.pitch * 4, (size_t)w * 4, h, cudaMemcpyDeviceToDevice,
+                               s.stream) == cudaSuccess
+                 ? FX_OK
+                 : fail(ctx, FX_ERR_CUDA, "score copy failed");
+    s.stream = saved;
+    return rc;
+}
+
+FX_API int fx_sync_counters(fx_context *ctx, fx_counters *counters) {
+    if (!ctx || !counters) return FX_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    cudaSetDevice(ctx->device);
+    Slot &s = slot0(ctx);
+    char *hc = reinterpret_cast<char *>(s.h_ctr);
+    FX_CUDA(ctx, cudaMemcpy(hc, s.arena.counters, dev_counters_bytes(), cudaMemcpyDeviceToHost));
+    uint32_t err;
+    FX_CUDA(ctx, cudaMemcpy(&err, s.arena.err, 4, cudaMemcpyDeviceToHost));
+    bool overflow;
+    const int rc = finish_counters(ctx, s, hc, err, counters, &overflow);
+    if (rc) return rc;
+    if (overflow) return fail(ctx, FX_ERR_INTERNAL, "amb capacity exceeded; rerun with counters");
+    return FX_OK;
+}
+
+FX_API int fx_set_slots(fx_context *ctx, int32_t slots) {
+    if (!ctx || slots < 1 || slots > 64) return FX_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    cudaSetDevice(ctx->device);
+    return ensure_slots(ctx, slots);
+}
+
+FX_API int fx_submit(fx_context *ctx, const fx_frame *f, int64_t *ticket) {
+    if (!ctx || !f || !f->main_rgbi || !f->rgb_out || !ticket) return FX_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    cudaSetDevice(ctx->device);
+    int rc = check_frame(ctx, f->params, f->height, f->width);
+    if (rc) return rc;
+    if (!f->stages && f->width < 8)
+        return fail(ctx, FX_ERR_GEOMETRY, "main RGBI frame has no complete producer cell");
+    Slot *slot = nullptr;
+    for (Slot &s : ctx->slots)
+        if (!s.busy) {
+            slot = &s;
+            break;
+        }
+    if (!slot) return fail(ctx, FX_PENDING, "no free slot");
+    Slot &s = *slot;
+    const Geometry g = make_geometry(f->height, f->width);
+    const size_t px = (size_t)g.h * g.w;
+    rc = ensure_arena(ctx, s, g, default_amb_capacity(g));
+    if (rc) return rc;
+    const size_t in_bytes = px * 8;
+    const size_t out_bytes = px * 6 + px * 4 + px;
+    if (s.h_in_bytes < in_bytes) {
+        if (s.h_in) cudaFreeHost(s.h_in);
+        s.h_in = nullptr;
+        s.h_in_bytes = 0;
+        FX_CUDA(ctx, cudaMallocHost(&s.h_in, in_bytes));
+        s.h_in_bytes = in_bytes;
+    }
+    if (s.h_out_bytes < out_bytes) {
+        if (s.h_out) cudaFreeHost(s.h_out);
+        s.h_out = nullptr;
+        s.h_out_bytes = 0;
+        FX_CUDA(ctx, cudaMallocHost(&s.h_out, out_bytes));
+        s.h_out_bytes = out_bytes;
+    }
+    std::memcpy(s.h_in, f->main_rgbi, in_bytes);
+    s.frame = *f;
+    s.params = *f->params;
+    s.frame.params = &s.params;
+    s.has_stages = f->stages != nullptr;
+    if (s.has_stages) s.stages.assign(f->stages, f->stages + (g.h + 6));
+    s.g = g;
+    FX_CUDA(ctx, cudaMemcpyAsync(s.arena.rgbi, s.h_in, in_bytes, cudaMemcpyHostToDevice, s.stream));
+    rc = enqueue_pass(ctx, s, g, s.params, s.has_stages ? s.stages.data() : nullptr,
+                      f->rng_state, s.arena.rgbi, s.arena.out, s.arena.changed, false);
+    if (rc) return rc;
+    char *ho = reinterpret_cast<char *>(s.h_out);
+    FX_CUDA(ctx, cudaMemcpyAsync(ho, s.arena.out, px * 6, cudaMemcpyDeviceToHost, s.stream));
+    if (f->score_out)
+        FX_CUDA(ctx, cudaMemcpy2DAsync(ho + px * 6, (size_t)g.w * 4,
+                                       s.arena.hs + g.padded_index(0, 0), (size_t)g.pitch * 4,
+                                       (size_t)g.w * 4, g.h, cudaMemcpyDeviceToHost, s.stream));
+    if (f->changed_out)
+        FX_CUDA(ctx, cudaMemcpyAsync(ho + px * 10, s.arena.changed, px, cudaMemcpyDeviceToHost,
+                                     s.stream));
+    char *hc = reinterpret_cast<char *>(s.h_ctr);
+    FX_CUDA(ctx, cudaMemcpyAsync(hc, s.arena.counters, dev_counters_bytes(),
+                                 cudaMemcpyDeviceToHost, s.stream));
+    FX_CUDA(ctx, cudaMemcpyAsync(hc + dev_counters_bytes(), s.arena.err, 4,
+                                 cudaMemcpyDeviceToHost, s.stream));
+    FX_CUDA(ctx, cudaEventRecord(s.done, s.stream));
+    s.busy = true;
+    s.ticket = ctx->next_ticket++;
+    *ticket = s.ticket;
+    return FX_OK;
+}
+
+static Slot *find_ticket(fx_context *ctx, int64_t ticket) {
+    for (Slot &s : ctx->slots)
+        if (s.busy && s.ticket == ticket) return &s;
+    return nullptr;
+}
+
+FX_API int fx_poll(fx_context *ctx, int64_t ticket) {
+    if (!ctx) return FX_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    cudaSetDevice(ctx->device);
+    Slot *s = find_ticket(ctx, ticket);
+    if (!s) return fail(ctx, FX_ERR_INVALID_ARGUMENT, "unknown ticket");
+    const cudaError_t e = cudaEventQuery(s->done);
+    if (e == cudaErrorNotReady) return FX_PENDING;
+    if (e != cudaSuccess) return fail(ctx, FX_ERR_CUDA, "%s", cudaGetErrorString(e));
+    return FX_OK;
+}
+
+FX_API int fx_wait(fx_context *ctx, int64_t ticket, int64_t timeout_ns, fx_counters *counters) {
+    if (!ctx) return FX_ERR_INVALID_ARGUMENT;
+    const auto start = std::chrono::steady_clock::now();
+    for (;;) {
+        {
+            std::lock_guard<std::mutex> lock(ctx->mu);
+            cudaSetDevice(ctx->device);
+            Slot *sp = find_ticket(ctx, ticket);
+            if (!sp) return fail(ctx, FX_ERR_INVALID_ARGUMENT, "unknown ticket");
+            Slot &s = *sp;
+            const cudaError_t e = cudaEventQuery(s.done);
+            if (e == cudaSuccess) {
+                const size_t px = (size_t)s.g.h * s.g.w;
+                char *hc = reinterpret_cast<char *>(s.h_ctr);
+                uint32_t err;
+                std::memcpy(&err, hc + dev_counters_bytes(), 4);
+                bool overflow;
+                int rc = finish_counters(ctx, s, hc, err, counters, &overflow);
+                if (!rc && overflow) {
+                    // rare: more RNG-dependent channels than the default
+                    // capacity; rerun synchronously with room for all
+                    fx_frame f = s.frame;
+                    f.main_rgbi = reinterpret_cast<const uint16_t *>(s.h_in);
+                    const int64_t cap = (int64_t)counters_n_amb(hc) + 1024;
+                    rc = ensure_arena(ctx, s, s.g, cap);
+                    if (!rc) {
+                        cudaMemcpyAsync(s.arena.rgbi, s.h_in, px * 8, cudaMemcpyHostToDevice,
+                                        s.stream);
+                        rc = enqueue_pass(ctx, s, s.g, s.params,
+                                          s.has_stages ? s.stages.data() : nullptr, f.rng_state,
+                                          s.arena.rgbi, s.arena.out, s.arena.changed, false);
+                    }
+                    if (!rc) {
+                        char *ho = reinterpret_cast<char *>(s.h_out);
+                        cudaMemcpyAsync(ho, s.arena.out, px * 6, cudaMemcpyDeviceToHost, s.stream);
+                        if (f.score_out)
+                            cudaMemcpy2DAsync(ho + px * 6, (size_t)s.g.w * 4,
+                                              s.arena.hs + s.g.padded_index(0, 0),
+                                              (size_t)s.g.pitch * 4, (size_t)s.g.w * 4, s.g.h,
+                                              cudaMemcpyDeviceToHost, s.stream);
+                        if (f.changed_out)
+                            cudaMemcpyAsync(ho + px * 10, s.arena.changed, px,
+                                            cudaMemcpyDeviceToHost, s.stream);
+                        cudaMemcpyAsync(hc, s.arena.counters, dev_counters_bytes(),
+                                        cudaMemcpyDeviceToHost, s.stream);
+                        cudaMemcpyAsync(hc + dev_counters_bytes(), s.arena.err, 4,
+                                        cudaMemcpyDeviceToHost, s.stream);
+                        if (cudaStreamSynchronize(s.stream) != cudaSuccess)
+                            rc = fail(ctx, FX_ERR_CUDA, "retry failed");
+                        std::memcpy(&err, hc + dev_counters_bytes(), 4);
+                        if (!rc) rc = finish_counters(ctx, s, hc, err, counters, &overflow);
+                        if (!rc && overflow) rc = fail(ctx, FX_ERR_INTERNAL, "capacity retry");
+                    }
+                }
+                if (!rc) {
+                    const char *ho = reinterpret_cast<const char *>(s.h_out);
+                    std::memcpy(s.frame.rgb_out, ho, px * 6);
+                    if (s.frame.score_out) std::memcpy(s.frame.score_out, ho + px * 6, px * 4);
+                    if (s.frame.changed_out) std::memcpy(s.frame.changed_out, ho + px * 10, px);
+                }
+                s.busy = false;
+                s.ticket = -1;
+                return rc;
+            }
+            if (e != cudaErrorNotReady) {
+                s.busy = false;
+                return fail(ctx, FX_ERR_CUDA, "%s", cudaGetErrorString(e));
+            }
+        }
+        if (timeout_ns >= 0) {
+            const auto el = std::chrono::steady_clock::now() - start;
+            if (std::chrono::duration_cast<std::chrono::nanoseconds>(el).count() > timeout_ns)
+                return FX_ERR_TIMEOUT;
+        }
+        std::this_thread::sleep_for(std::chrono::microseconds(50));
+    }
+}
+
+FX_API int fx_mem_info(fx_context *ctx, size_t *free_bytes, size_t *total_bytes) {
+    if (!ctx || !free_bytes || !total_bytes) return FX_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(ctx->device);
+    FX_CUDA(ctx, cudaMemGetInfo(free_bytes, total_bytes));
+    return FX_OK;
+}
+
+FX_API int64_t fx_frame_bytes(int32_t h, int32_t w) {
+    if (h < 1 || w < 1) return -1;
+    const Geometry g = make_geometry(h, w);
+    return (int64_t)arena_layout(g, default_amb_capacity(g), nullptr);
+}
+
+}  // extern "C"

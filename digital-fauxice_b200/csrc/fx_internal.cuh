@@ -1,0 +1,186 @@
+// fx_internal.cuh -- shared device definitions of the B200 Digital ICE core.
+//
+// Numerics: every kernel is compiled with --fmad=false and without fast
+// math, so each binary64 / binary32 add, multiply and divide rounds once,
+// in the order written, exactly like the reference's scalar NumPy path.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/fauxice_b200.h"
+
+namespace fx {
+
+constexpr uint32_t kLcgMask = 0x00FFFFFFu;
+// rng.py:135: float32 bits 0x337fffff widened = (2^24 - 1) * 2^-48.
+constexpr double kNormalization = 0x1.fffffep-25;
+constexpr int kPad = 5;          // history-plane border (rows/cols)
+constexpr int kTileH = 8;        // stencil tile rows
+constexpr int kTileW = 32;       // stencil tile cols
+constexpr int kSegment = 1024;   // chain sites per scan segment
+constexpr int kSegThreads = 256; // threads per segment block
+
+// Device error word: the first failing status wins.
+__device__ __forceinline__ void raise_error(uint32_t *err, uint32_t code) {
+    if (*reinterpret_cast<volatile uint32_t *>(err) == 0) atomicCAS(err, 0u, code);
+}
+
+// ---------------------------------------------------------------------------
+// Frame geometry and buffers
+// ---------------------------------------------------------------------------
+
+struct Geometry {
+    int h, w;              // logical frame
+    int th, tw;            // tiles
+    int hp, wp;            // rows/cols rounded up to whole tiles
+    int prow;              // padded rows = hp + 2*kPad
+    int pitch;             // floats per padded row (>= wp + 2*kPad, multiple of 32)
+    int64_t sites;         // chain sites = 6*w (startup) + h*w (public)
+    int64_t segments;      // ceil(sites / kSegment)
+    __host__ __device__ int64_t padded_index(int y, int x) const {
+        return (int64_t)(y + kPad) * pitch + (x + kPad);
+    }
+};
+
+// Per-site meta byte: bit 7 attempted, bits 2c..2c+1 draw code of channel c
+// (0: no draw, 1: one draw, 2: two draws, 3: RNG-dependent: one or two).
+__host__ __device__ __forceinline__ int meta_code(uint8_t m, int c) { return (m >> (2 * c)) & 3; }
+__host__ __device__ __forceinline__ int meta_base(uint8_t m) {
+    int b = 0;
+    for (int c = 0; c < 3; ++c) {
+        const int k = meta_code(m, c);
+        b += (k == 3) ? 1 : k;
+    }
+    return b;
+}
+__host__ __device__ __forceinline__ int meta_amb(uint8_t m) {
+    int a = 0;
+    for (int c = 0; c < 3; ++c) a += meta_code(m, c) == 3;
+    return a;
+}
+
+// One RNG-dependent channel for the serial walk.  In "T space" the 24-bit
+// state s is held as T = s << 8, so the LCG s -> 125 s + 1 (mod 2^24)
+// becomes T -> 125 T + 256 (mod 2^32) and interval tests need no masking.
+struct AmbEntry {
+    uint32_t l1, w1, l2, w2; // copy iff (T - l1) <= w1 || (T - l2) <= w2
+    uint32_t a, c;           // T_first_draw = a * T_prev + c  (no extra draw before)
+};
+
+// ---------------------------------------------------------------------------
+// LCG jump-ahead: g^n as an affine map, composed by binary powering.
+// ---------------------------------------------------------------------------
+
+struct Affine {
+    uint32_t a, c;
+};
+
+__host__ __device__ __forceinline__ Affine affine_compose(Affine f, Affine g) {
+    // (f o g)(x) = f.a * (g.a x + g.c) + f.c
+    return Affine{f.a * g.a, f.a * g.c + f.c};
+}
+
+// g^n in T space (mod 2^32): a = 125^n, c = 256 * (125^n - 1) / 124.
+__host__ __device__ __forceinline__ Affine lcg_power_t(uint64_t n) {
+    Affine result{1u, 0u};
+    Affine base{125u, 256u};
+    while (n) {
+        if (n & 1u) result = affine_compose(base, result);
+        base = affine_compose(base, base);
+        n >>= 1;
+    }
+    return result;
+}
+
+// g^n applied to a 24-bit state.
+__host__ __device__ __forceinline__ uint32_t lcg_jump(uint32_t s, uint64_t n) {
+    const Affine f = lcg_power_t(n);
+    return ((f.a * (s << 8) + f.c) >> 8) & kLcgMask;
+}
+
+// ---------------------------------------------------------------------------
+// Exact scalar pieces of the writer (dither.py:59-104, reconstruction.py:916-982)
+// ---------------------------------------------------------------------------
+
+struct DitherConst {
+    double low, high;      // widened float32 bounds
+    double coefficient;    // 4 / (width * width)
+    int low_lt_high;
+};
+
+__device__ __forceinline__ DitherConst dither_const(const fx_params &p) {
+    DitherConst d;
+    d.low = (double)p.dither_low;
+    d.high = (double)p.dither_high;
+    d.low_lt_high = d.low < d.high;
+    const double width = d.high - d.low;
+    d.coefficient = 4.0 / (width * width);
+    return d;
+}
+
+// Raw delta for a first-draw state s1 (before the accept test).
+__device__ __forceinline__ double dither_raw_delta(double cand, double envelope, float span,
+                                                   uint32_t s1) {
+    const double unit = (double)(s1 + 1u) * kNormalization - 0.5;
+    const double random_value = 0.0 + unit * (double)span;
+    return envelope * random_value;
+}
+
+// conditional_dither_delta with the state advanced in place.  Returns the
+// accepted delta (or 0).  `drew` reports whether the LCG advanced.
+__device__ __forceinline__ double dither_delta(double value, float scale32, const DitherConst &dc,
+                                               uint32_t &state, int &drew) {
+    const float cand32 = (float)value;
+    const double cand = (double)cand32;
+    drew = 0;
+    if (!dc.low_lt_high) return 0.0;
+    if (!(dc.low < cand && cand < dc.high)) return 0.0;
+    const double envelope = ((dc.high - cand) * (cand - dc.low)) * dc.coefficient;
+    const float span = (float)((double)scale32 * cand);
+    state = (125u * state + 1u) & kLcgMask;
+    drew = 1;
+    const double d = dither_raw_delta(cand, envelope, span, state);
+    const double changed = cand + d;
+    return (dc.low < changed && changed < dc.high) ? d : 0.0;
+}
+
+// ---------------------------------------------------------------------------
+// Host-visible launch helpers (defined in the .cu files)
+// ---------------------------------------------------------------------------
+
+// Writer scratch of one frame.  `capacity` bounds the RNG-dependent channel
+// list; when a frame has more, the counters report it and the host reruns
+// the writer with a larger list (every access below is clamped to it).
+struct WriterBuffers {
+    uint32_t *seg_base, *seg_amb;  // segments + 1 each
+    AmbEntry *entries;             // capacity (+64 bytes slack)
+    uint32_t *pos;                 // capacity
+    uint32_t *extra_after;         // capacity
+    void *counters;                // DevCounters
+    int64_t capacity;
+};
+
+cudaError_t analysis_init();
+cudaError_t launch_analysis(const uint16_t *rgbi, const Geometry &g, const float *lut,
+                            const fx_stage *stages, const fx_params &p, float *aux, float *hs,
+                            float *hwa, float *hwr, int64_t plane, double *cand, uint8_t *meta,
+                            uint32_t *err, cudaStream_t stream);
+cudaError_t launch_writer(const Geometry &g, const uint8_t *meta, const double *cand,
+                          const uint16_t *rgbi, const float *lut, const uint32_t *high,
+                          const uint32_t *low, const fx_stage *stages, const fx_params &p,
+                          uint32_t s0, const WriterBuffers &b, uint16_t *rgb_out,
+                          uint8_t *changed_out, uint32_t *err, cudaStream_t stream);
+size_t dev_counters_bytes();
+void counters_to_host(const void *dev_copy, fx_counters *out);
+uint32_t counters_n_amb(const void *dev_copy);
+size_t producer_bytes(int h, int w);
+cudaError_t launch_producer(const uint16_t *rgbi, int h, int w, const float *lut, void *scratch,
+                            fx_stage *stages, float *rows_out, uint32_t *err,
+                            cudaStream_t stream);
+int host_reduce_prepass(const uint16_t *px, int h, int w, const float *lut, uint8_t payload[64],
+                        int64_t *valid_pixels, int64_t *fully_valid_tiles);
+int host_stage_table(int h, const float *p1, const float *p2, const float *mv, const float *mi,
+                     float factor_b, fx_stage *stages);
+
+}  // namespace fx

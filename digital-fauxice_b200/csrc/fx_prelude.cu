@@ -1,0 +1,527 @@
+// fx_prelude.cu -- content-derived calibration for the main pass.
+//
+// Device kernels for producer_parameters.py:266-495 (cumulative per-row
+// means and the eight-row scale epochs) and the stage table of
+// producer_parameters.py:498-541 / stage_parameters.py:93-197, plus the host
+// prepass reducer of prepass.py:96-236.  Every reduction keeps the
+// reference's strictly sequential binary64 order: the per-row sums run one
+// row per thread along the columns, the cumulative sums and the epoch chain
+// run in one warp.
+#include <cmath>
+#include <cstring>
+
+#include "fx_internal.cuh"
+
+namespace fx {
+
+constexpr float kIrThreshold = 8847.2255859375f;  // producer_parameters.py:36
+constexpr float kInitialVisibleMean = 46618.78515625f;
+constexpr float kInitialInfraredMean = 56239.65625f;
+constexpr float kInitialScale = 0.15f;
+constexpr float kScaleMultiplier = 1.5f;
+
+// ---------------------------------------------------------------------------
+// X3A setter (stage_parameters.py:93-128, 151-197), shared host/device
+// ---------------------------------------------------------------------------
+
+__host__ __device__ inline int setter_stage(float p1, float p2, float p3, float p4,
+                                            float factor_b, fx_stage *out) {
+    if (!isfinite(p1) || !isfinite(p2) || !isfinite(p3) || !isfinite(p4))
+        return FX_ERR_STAGE_NONFINITE;
+    if (p2 < 0.0f) {
+        p1 = -p1;
+        p2 = -p2;
+    }
+    const double d1 = 1.0 - (double)p1, d2 = 1.0 - (double)p2;
+    if (d1 == 0.0 || d2 == 0.0) return FX_ERR_SETTER_ONE;
+    const float base = (float)(((double)p4 - (double)p3 * (double)p2) / d2);
+    const int gate_secondary = !(p3 != 0.0f && p2 <= 0.075f);
+    const float alpha = p2 * factor_b;
+    if (!isfinite(alpha) || !isfinite(base)) return FX_ERR_STAGE_NONFINITE;
+    out->alpha = alpha;
+    out->offset = 1.0f;
+    out->replacement = base;
+    out->replacement_valid = 1;
+    out->score_base = base;
+    out->coarse = base;
+    out->gate_secondary = gate_secondary;
+    out->row_gate = 0;
+    return FX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Cells: first failing IR position per (8-row block, 8-column cell) and, for
+// complete eight-row epochs, the four quadrant terms of
+// _scale_epoch_additions (producer_parameters.py:183-263).
+// ---------------------------------------------------------------------------
+
+struct ProducerBuffers {
+    uint8_t *failpos;      // [nb][cells]
+    uint8_t *cell_ok;      // [ne][cells]
+    double2 *terms;        // [ne][cells][4]  (term, ratio * term)
+    double *row_sums;      // [3][h]  visible, infrared, weight
+    double *cum;           // [3][h]
+    float *add;            // [2][ne]
+    float *p_epoch;        // [2][ne] p1, p2 after epoch e
+};
+
+__device__ __forceinline__ float quadrant_tree(const float v[8][8], int ry, int cx) {
+    double first = (double)v[ry][cx];
+    first += (double)v[ry][cx + 1];
+    first += (double)v[ry][cx + 2];
+    first += (double)v[ry][cx + 3];
+    first += (double)v[ry + 1][cx];
+    first += (double)v[ry + 1][cx + 1];
+    const double second_tail = (double)v[ry + 1][cx + 2] + (double)v[ry + 1][cx + 3];
+    first += second_tail;
+    double third = (double)v[ry + 2][cx] + (double)v[ry + 2][cx + 1];
+    const double third_tail = (double)v[ry + 2][cx + 2] + (double)v[ry + 2][cx + 3];
+    third += third_tail;
+    double fourth = (double)v[ry + 3][cx] + (double)v[ry + 3][cx + 1];
+    const double fourth_tail = (double)v[ry + 3][cx + 2] + (double)v[ry + 3][cx + 3];
+    fourth += fourth_tail;
+    third += fourth;
+    const double total = first + third;
+    return (float)(total * 0.0625);
+}
+
+__device__ __forceinline__ void center_quadrants(const float q[4], float out[4]) {
+    double t = (double)q[0];
+    t += (double)q[1];
+    t += (double)q[2];
+    t += (double)q[3];
+    const float mean = (float)(t * 0.25);
+#pragma unroll
+    for (int i = 0; i < 4; ++i) out[i] = (float)((double)q[i] - (double)mean);
+}
+
+__global__ void k_producer_cells(const uint16_t *__restrict__ rgbi, int h, int w, int cells,
+                                 const float *__restrict__ lut, ProducerBuffers b) {
+    const int nb = (h + 7) / 8;
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (int64_t)nb * cells) return;
+    const int blk = (int)(idx / cells), cell = (int)(idx % cells);
+    const int r0 = blk * 8, rows = min(8, h - r0);
+    const double thr = (double)kIrThreshold;
+    int failpos = 64;
+    for (int i = 0; i < rows && failpos == 64; ++i) {
+        for (int j = 0; j < 8; ++j) {
+            const uint32_t ir = (uint32_t)rgbi[((int64_t)(r0 + i) * w + cell * 8 + j) * 4 + 3];
+            if (!(thr < (double)ir)) {
+                failpos = i * 8 + j;
+                break;
+            }
+        }
+    }
+    b.failpos[idx] = (uint8_t)failpos;
+    if (rows < 8) return;  // no complete epoch in a partial final block
+    const int64_t e_idx = (int64_t)blk * cells + cell;
+    if (failpos != 64) {
+        b.cell_ok[e_idx] = 0;
+        return;
+    }
+    b.cell_ok[e_idx] = 1;
+    float vr[8][8], ir[8][8];
+    float raw_sum = 0.0f;
+    for (int i = 0; i < 8; ++i)
+        for (int j = 0; j < 8; ++j) {
+            const uint16_t *px = rgbi + ((int64_t)(r0 + i) * w + cell * 8 + j) * 4;
+            vr[i][j] = __ldg(lut + px[0]);
+            ir[i][j] = __ldg(lut + px[3]);
+            raw_sum = (float)((double)raw_sum + (double)px[3]);
+        }
+    const int qy[4] = {0, 0, 4, 4}, qx[4] = {0, 4, 0, 4};
+    float vq[4], iq[4], vd[4], id[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        vq[q] = quadrant_tree(vr, qy[q], qx[q]);
+        iq[q] = quadrant_tree(ir, qy[q], qx[q]);
+    }
+    center_quadrants(vq, vd);
+    center_quadrants(iq, id);
+    const double rs = (double)raw_sum;
+    const double low = (double)-0.125f, full_high = (double)0.3f, high = (double)0.425f;
+    const double outer = (double)0.70710677f;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const double vw = (double)vd[q];
+        double ratio, weight;
+        if (vw == 0.0) {
+            ratio = 0.0;
+            weight = 0.0;
+        } else {
+            ratio = (double)id[q] / vw;
+            if (ratio < low || ratio > high) weight = 0.0;
+            else if (ratio < 0.0 || ratio > full_high) weight = vw * outer;
+            else weight = vw;
+        }
+        double term = weight * weight;
+        term *= rs;
+        term *= rs;
+        b.terms[e_idx * 4 + q] = make_double2(term, ratio * term);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Per-row sums in strict column order, one row per lane.  A warp owns 32
+// rows; 32x32-pixel tiles stream through a cp.async ring in shared memory so
+// each lane reads its own row without uncoalesced global loads.
+// ---------------------------------------------------------------------------
+
+constexpr int kRowStages = 6;
+
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
+    const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
+}
+
+__global__ void __launch_bounds__(32)
+    k_producer_rows(const uint16_t *__restrict__ rgbi, int h, int w, int active_width, int cells,
+                    const float *__restrict__ lut, ProducerBuffers b) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    uint2(*tile)[32][33] = reinterpret_cast<uint2(*)[32][33]>(smem_raw);
+    const int lane = threadIdx.x;
+    const int r0 = blockIdx.x * 32;
+    const int row = r0 + lane;
+    const int tiles = (active_width + 31) / 32;
+    auto issue = [&](int t) {
+        if (t < tiles) {
+            const int col = t * 32 + lane;
+            if (col < active_width) {
+                for (int k = 0; k < 32; ++k) {
+                    const int rr = r0 + k;
+                    if (rr < h)
+                        cp_async8(&tile[t % kRowStages][k][lane],
+                                  rgbi + ((int64_t)rr * w + col) * 4);
+                }
+            }
+        }
+        asm volatile("cp.async.commit_group;\n" ::);
+    };
+#pragma unroll
+    for (int t = 0; t < kRowStages - 1; ++t) issue(t);
+    double rv = 0.0, ri = 0.0, rw = 0.0;
+    const int blk = row >> 3, local_row = row & 7;
+    for (int t = 0; t < tiles; ++t) {
+        issue(t + kRowStages - 1);
+        asm volatile("cp.async.wait_group %0;\n" ::"n"(kRowStages - 1));
+        __syncwarp();
+        if (row < h) {
+            const uint2 *tr = tile[t % kRowStages][lane];
+            const int col0 = t * 32;
+            const int n = min(32, active_width - col0);
+            for (int j = 0; j < n; ++j) {
+                const int col = col0 + j;
+                const int fp = b.failpos[(int64_t)blk * cells + (col >> 3)];
+                if (local_row * 8 + (col & 7) < fp) {
+                    const uint2 px = tr[j];
+                    const uint32_t vis = px.x & 0xFFFFu, irv = px.y >> 16;
+                    const double weight = (double)((uint64_t)irv * irv);
+                    rv += weight * (double)__ldg(lut + vis);
+                    ri += weight * (double)__ldg(lut + irv);
+                    rw += weight;
+                }
+            }
+        }
+        __syncwarp();
+    }
+    asm volatile("cp.async.wait_group 0;\n" ::);
+    if (row < h) {
+        b.row_sums[row] = rv;
+        b.row_sums[h + row] = ri;
+        b.row_sums[2 * h + row] = rw;
+    }
+}
+
+// Epoch sums: one warp per complete epoch, sequential over cells and
+// quadrants (every lane carries the same running sums).
+__global__ void __launch_bounds__(32)
+    k_producer_epochs(int cells, int ne, ProducerBuffers b) {
+    const int e = blockIdx.x;
+    if (e >= ne) return;
+    const int lane = threadIdx.x;
+    double den = 0.0, num = 0.0;
+    for (int c0 = 0; c0 < cells; c0 += 32) {
+        const int c = c0 + lane;
+        const bool ok = c < cells && b.cell_ok[(int64_t)e * cells + c];
+        double2 t[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            t[q] = ok ? b.terms[((int64_t)e * cells + c) * 4 + q] : make_double2(0.0, 0.0);
+        const int n = min(32, cells - c0);
+        for (int j = 0; j < n; ++j) {
+            const bool okj = __shfl_sync(0xFFFFFFFFu, ok, j);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const double tx = __shfl_sync(0xFFFFFFFFu, t[q].x, j);
+                const double ty = __shfl_sync(0xFFFFFFFFu, t[q].y, j);
+                if (okj) {
+                    den += tx;
+                    num += ty;
+                }
+            }
+        }
+    }
+    if (lane == 0) {
+        b.add[e] = (float)den;
+        b.add[ne + e] = (float)num;
+    }
+}
+
+// Cumulative row sums (3 binary64 chains) and the epoch p1/p2 chain.
+__global__ void __launch_bounds__(32)
+    k_producer_scan(int h, int ne, ProducerBuffers b) {
+    const int lane = threadIdx.x;
+    double tv = 0.0, ti = 0.0, tw = 0.0;
+    for (int r0 = 0; r0 < h; r0 += 32) {
+        const int r = r0 + lane;
+        const double v = (r < h) ? b.row_sums[r] : 0.0;
+        const double i = (r < h) ? b.row_sums[h + r] : 0.0;
+        const double wv = (r < h) ? b.row_sums[2 * h + r] : 0.0;
+        double mv = 0.0, mi = 0.0, mw = 0.0;
+        const int n = min(32, h - r0);
+        for (int j = 0; j < n; ++j) {
+            tv += __shfl_sync(0xFFFFFFFFu, v, j);
+            ti += __shfl_sync(0xFFFFFFFFu, i, j);
+            tw += __shfl_sync(0xFFFFFFFFu, wv, j);
+            if (lane == j) {
+                mv = tv;
+                mi = ti;
+                mw = tw;
+            }
+        }
+        if (r < h) {
+            b.cum[r] = mv;
+            b.cum[h + r] = mi;
+            b.cum[2 * h + r] = mw;
+        }
+    }
+    if (lane == 0) {
+        float den = 0.0f, num = 0.0f, p1 = kInitialScale, p2 = kInitialScale;
+        for (int e = 0; e < ne; ++e) {
+            const double dw = (double)den + (double)b.add[e];
+            const double nw = (double)num + (double)b.add[ne + e];
+            den = (float)dw;
+            num = (float)nw;
+            if (dw != 0.0) {
+                const double ratio = nw / dw;
+                p2 = (float)ratio;
+                p1 = (float)((double)kScaleMultiplier * ratio);
+            }
+            b.p_epoch[e] = p1;
+            b.p_epoch[ne + e] = p2;
+        }
+    }
+}
+
+// Per-row record fields: the four float32 values the setter reads.
+__device__ __forceinline__ void row_fields(int row, int ne, const ProducerBuffers &b, int h,
+                                           float &p1, float &p2, float &mv, float &mi) {
+    const double tw = b.cum[2 * h + row];
+    if (tw != 0.0) {
+        mv = (float)(b.cum[row] / tw);
+        mi = (float)(b.cum[h + row] / tw);
+    } else {
+        mv = kInitialVisibleMean;
+        mi = kInitialInfraredMean;
+    }
+    const int done = (row + 1) / 8;  // epochs finalised at rows 7, 15, ...
+    if (done > 0 && done <= ne) {
+        p1 = b.p_epoch[done - 1];
+        p2 = b.p_epoch[ne + done - 1];
+    } else {
+        p1 = kInitialScale;
+        p2 = kInitialScale;
+    }
+}
+
+__global__ void k_stage_table(int h, int ne, float factor_b, ProducerBuffers b, fx_stage *stages,
+                              float *rows_out, uint32_t *err) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x + 1;  // stage hit
+    if (s > h + 6) return;
+    const int row = min(s - 1, h - 1);
+    float p1, p2, mv, mi;
+    row_fields(row, ne, b, h, p1, p2, mv, mi);
+    if (rows_out && s <= h) {
+        rows_out[row] = p1;
+        rows_out[h + row] = p2;
+        rows_out[2 * h + row] = mv;
+        rows_out[3 * h + row] = mi;
+    }
+    fx_stage st;
+    const int rc = setter_stage(p1, p2, mv, mi, factor_b, &st);
+    if (rc != FX_OK) {
+        raise_error(err, (uint32_t)rc);
+        st = fx_stage{0.0f, 0.0f, 0.0f, 0, 0.0f, 0.0f, 0, 0};
+    }
+    stages[s - 1] = st;
+}
+
+cudaError_t producer_init() {
+    return cudaFuncSetAttribute(k_producer_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)((size_t)kRowStages * 32 * 33 * sizeof(uint2)));
+}
+
+size_t producer_bytes(int h, int w) {
+    const int64_t aw = (w / 8) * 8, cells = aw / 8, nb = (h + 7) / 8, ne = h / 8;
+    size_t b = 0;
+    auto add = [&](size_t n) { b += (n + 255) & ~(size_t)255; };
+    add(nb * cells);
+    add(ne * cells);
+    add(ne * cells * 4 * sizeof(double2));
+    add(3 * (size_t)h * sizeof(double));
+    add(3 * (size_t)h * sizeof(double));
+    add(2 * (size_t)ne * sizeof(float));
+    add(2 * (size_t)ne * sizeof(float));
+    return b;
+}
+
+cudaError_t launch_producer(const uint16_t *rgbi, int h, int w, const float *lut, void *scratch,
+                            fx_stage *stages, float *rows_out, uint32_t *err,
+                            cudaStream_t stream) {
+    const int aw = (w / 8) * 8, cells = aw / 8, nb = (h + 7) / 8, ne = h / 8;
+    ProducerBuffers b;
+    char *p = reinterpret_cast<char *>(scratch);
+    auto take = [&](size_t n) {
+        void *r = p;
+        p += (n + 255) & ~(size_t)255;
+        return r;
+    };
+    b.failpos = (uint8_t *)take((size_t)nb * cells);
+    b.cell_ok = (uint8_t *)take((size_t)ne * cells);
+    b.terms = (double2 *)take((size_t)ne * cells * 4 * sizeof(double2));
+    b.row_sums = (double *)take(3 * (size_t)h * sizeof(double));
+    b.cum = (double *)take(3 * (size_t)h * sizeof(double));
+    b.add = (float *)take(2 * (size_t)ne * sizeof(float));
+    b.p_epoch = (float *)take(2 * (size_t)ne * sizeof(float));
+    {
+        const int64_t n = (int64_t)nb * cells;
+        k_producer_cells<<<(unsigned)((n + 127) / 128), 128, 0, stream>>>(rgbi, h, w, cells, lut, b);
+    }
+    {
+        const size_t smem = (size_t)kRowStages * 32 * 33 * sizeof(uint2);
+        k_producer_rows<<<(h + 31) / 32, 32, smem, stream>>>(rgbi, h, w, aw, cells, lut, b);
+    }
+    if (ne > 0) k_producer_epochs<<<ne, 32, 0, stream>>>(cells, ne, b);
+    k_producer_scan<<<1, 32, 0, stream>>>(h, ne, b);
+    k_stage_table<<<(h + 6 + 255) / 256, 256, 0, stream>>>(h, ne, 1.0f, b, stages, rows_out, err);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Host prepass (prepass.py:96-236), fresh record, selector-8 parameters
+// ---------------------------------------------------------------------------
+
+static float prepass_quadrant(const float v[8][8], int fy, int fx) {
+    double total = 0.0;
+    for (int y = fy; y < fy + 4; ++y)
+        for (int x = fx; x < fx + 4; ++x) total += (double)v[y][x];
+    return (float)(total * 0.0625);
+}
+
+int host_reduce_prepass(const uint16_t *px, int h, int w, const float *lut, uint8_t payload[64],
+                        int64_t *valid_pixels, int64_t *fully_valid_tiles) {
+    const float threshold = 8847.2255859375f;
+    const double ratio_min = (double)-0.2f, ratio_max = (double)0.2f;
+    const double alpha_scale = (double)1.5f;
+    const int ph = (h + 7) & ~7, pw = (w + 7) & ~7;
+    double cal_r = 0.0, cal_ir = 0.0, cal_sq = 0.0;
+    float reg_den = 0.0f, reg_num = 0.0f;
+    int64_t valid = 0, tiles = 0;
+    for (int ty = 0; ty < ph; ty += 8) {
+        for (int tx = 0; tx < pw; tx += 8) {
+            float rr[8][8] = {}, ri[8][8] = {};
+            float sum_raw_ir = 0.0f;
+            bool tile_valid = true;
+            for (int y = 0; y < 8; ++y) {
+                for (int x = 0; x < 8; ++x) {
+                    const int yy = ty + y, xx = tx + x;
+                    uint32_t raw_r = 0, raw_ir = 0;  // zero padding to whole tiles
+                    if (yy < h && xx < w) {
+                        raw_r = px[((size_t)yy * w + xx) * 4];
+                        raw_ir = px[((size_t)yy * w + xx) * 4 + 3];
+                    }
+                    if ((float)raw_ir <= threshold) {
+                        tile_valid = false;
+                        continue;
+                    }
+                    ++valid;
+                    const float cr = lut[raw_r], ci = lut[raw_ir];
+                    rr[y][x] = cr;
+                    ri[y][x] = ci;
+                    const double sq = (double)((uint64_t)raw_ir * raw_ir);
+                    cal_r += sq * (double)cr;
+                    cal_ir += sq * (double)ci;
+                    cal_sq += sq;
+                    sum_raw_ir = (float)((double)sum_raw_ir + (double)raw_ir);
+                }
+            }
+            if (!tile_valid) continue;
+            ++tiles;
+            const int qy[4] = {0, 0, 4, 4}, qx[4] = {0, 4, 0, 4};
+            float rm[4], im[4];
+            for (int q = 0; q < 4; ++q) {
+                rm[q] = prepass_quadrant(rr, qy[q], qx[q]);
+                im[q] = prepass_quadrant(ri, qy[q], qx[q]);
+            }
+            double tr = (double)rm[0];
+            tr += (double)rm[1];
+            tr += (double)rm[2];
+            tr += (double)rm[3];
+            double ti = (double)im[0];
+            ti += (double)im[1];
+            ti += (double)im[2];
+            ti += (double)im[3];
+            const float rg = (float)(tr * 0.25), ig = (float)(ti * 0.25);
+            double den = (double)reg_den, num = (double)reg_num;
+            const double scalar = (double)sum_raw_ir;
+            for (int q = 0; q < 4; ++q) {
+                const float rd = (float)((double)rm[q] - (double)rg);
+                const float id = (float)((double)im[q] - (double)ig);
+                if (rd == 0.0f) continue;
+                const double ratio = (double)id / (double)rd;
+                if (ratio < ratio_min || ratio > ratio_max) continue;
+                const double weight = (double)rd * (double)rd * scalar * scalar;
+                den += weight;
+                num += ratio * weight;
+            }
+            reg_den = (float)den;
+            reg_num = (float)num;
+        }
+    }
+    const double unrounded =
+        (reg_den == 0.0f) ? (double)0.17f : (double)reg_num / (double)reg_den;
+    const float alpha = (float)unrounded;
+    const float scaled = (float)(unrounded * alpha_scale);
+    std::memset(payload, 0, 64);
+    const uint32_t one = 1u, marker = 16u;
+    std::memcpy(payload + 0x00, &one, 4);
+    std::memcpy(payload + 0x04, &alpha, 4);
+    std::memcpy(payload + 0x08, &scaled, 4);
+    std::memcpy(payload + 0x10, &cal_r, 8);
+    std::memcpy(payload + 0x18, &cal_ir, 8);
+    std::memcpy(payload + 0x20, &cal_sq, 8);
+    if (cal_sq != 0.0) {
+        const float mr = (float)(cal_r / cal_sq), mi = (float)(cal_ir / cal_sq);
+        std::memcpy(payload + 0x28, &mr, 4);
+        std::memcpy(payload + 0x2C, &mi, 4);
+    }
+    std::memcpy(payload + 0x30, &reg_den, 4);
+    std::memcpy(payload + 0x34, &reg_num, 4);
+    std::memcpy(payload + 0x38, &marker, 4);
+    if (valid_pixels) *valid_pixels = valid;
+    if (fully_valid_tiles) *fully_valid_tiles = tiles;
+    return FX_OK;
+}
+
+int host_stage_table(int h, const float *p1, const float *p2, const float *mv, const float *mi,
+                     float factor_b, fx_stage *stages) {
+    for (int s = 1; s <= h + 6; ++s) {
+        const int row = (s - 1) < (h - 1) ? (s - 1) : (h - 1);
+        const int rc = setter_stage(p1[row], p2[row], mv[row], mi[row], factor_b, &stages[s - 1]);
+        if (rc != FX_OK) return rc;
+    }
+    return FX_OK;
+}
+
+}  // namespace fx

@@ -1,0 +1,611 @@
+// fx_writer.cu -- the sequential dither writer, restructured for the GPU.
+//
+// The reference writes attempted sites in strict row-major order, threading
+// one 24-bit LCG through every conditional draw (reconstruction.py:916-982,
+// dither.py:59-104, rng.py:159-172).  The number of draws a channel takes is
+// a function of the state only when its first draw happens, the floor gate
+// is on and the floor comparison is not settled by the largest possible
+// |delta|.  So:
+//   1. k_stencil / k_startup classify every channel: 0, 1 or 2 fixed draws,
+//      or "RNG-dependent" (one or two).
+//   2. k_seg_sums + k_seg_scan: exclusive prefix of fixed draws and of
+//      RNG-dependent channels along the chain (startup sites, then public
+//      sites in row-major order).
+//   3. k_amb: for each RNG-dependent channel, the set of first-draw states
+//      that copy the original, as at most two state intervals (found by
+//      binary search on the exact binary64 expressions, which are monotone
+//      in the state).
+//   4. k_coef: the affine LCG jump g^gap between consecutive such channels.
+//   5. k_walk: ONE thread walks only the RNG-dependent channels: a jump, an
+//      interval test, a select.  Output: the running count of extra draws.
+//   6. k_apply: every public site recomputes its exact draws and values from
+//      its own start state g^(fixed + extra before it)(s0), in parallel, and
+//      emits public RGB16 with the counters.
+#include "fx_internal.cuh"
+
+namespace fx {
+
+struct DevCounters {
+    unsigned long long attempted, written, public_advances, changed;
+    unsigned long long su_attempted[6], su_advances[6];
+    unsigned long long public_base, public_amb;
+    uint32_t final_state, su_final_state;
+    uint32_t startup_base, startup_amb, startup_extra;
+    uint32_t n_amb;
+};
+
+// ---------------------------------------------------------------------------
+// Block scan helpers (256 threads)
+// ---------------------------------------------------------------------------
+
+template <int NT>
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t &total,
+                                                         uint32_t *warp_sums) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) warp_sums[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t s = (lane < NT / 32) ? warp_sums[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, s, o);
+            if (lane >= o) s += y;
+        }
+        if (lane < NT / 32) warp_sums[lane] = s;
+    }
+    __syncthreads();
+    const uint32_t prefix = warp ? warp_sums[warp - 1] : 0u;
+    total = warp_sums[NT / 32 - 1];
+    __syncthreads();
+    return prefix + x - v;
+}
+
+template <int NT, typename T>
+__device__ __forceinline__ T block_sum(T v, T *scratch) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xFFFFFFFFu, v, o);
+    if (lane == 0) scratch[warp] = v;
+    __syncthreads();
+    T total = 0;
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < NT / 32; ++i) total += scratch[i];
+        scratch[0] = total;
+    }
+    __syncthreads();
+    total = scratch[0];
+    __syncthreads();
+    return total;
+}
+
+constexpr int kPer = kSegment / kSegThreads;  // sites per thread
+
+// Running extra-draw count after `count` RNG-dependent channels (clamped to
+// the list capacity; an overflowing frame is rerun by the host).
+__device__ __forceinline__ uint32_t extra_before(const uint32_t *extra_after, uint32_t count,
+                                                 int64_t capacity) {
+    if (count == 0) return 0u;
+    const int64_t i = (int64_t)count - 1;
+    return extra_after[i < capacity ? i : capacity - 1];
+}
+
+// Packed local (base << 16 | amb) of one thread's sites.
+__device__ __forceinline__ void load_meta(const uint8_t *meta, int64_t first, int64_t sites,
+                                          uint8_t m[kPer]) {
+#pragma unroll
+    for (int i = 0; i < kPer; ++i) {
+        const int64_t s = first + i;
+        m[i] = (s < sites) ? meta[s] : 0;
+    }
+}
+
+__global__ void k_seg_sums(const uint8_t *__restrict__ meta, int64_t sites,
+                           uint32_t *__restrict__ seg_base, uint32_t *__restrict__ seg_amb) {
+    __shared__ uint32_t scratch[kSegThreads / 32];
+    const int64_t first = (int64_t)blockIdx.x * kSegment + threadIdx.x * kPer;
+    uint8_t m[kPer];
+    load_meta(meta, first, sites, m);
+    uint32_t packed = 0;
+#pragma unroll
+    for (int i = 0; i < kPer; ++i) packed += ((uint32_t)meta_base(m[i]) << 16) | meta_amb(m[i]);
+    const uint32_t total = block_sum<kSegThreads, uint32_t>(packed, scratch);
+    if (threadIdx.x == 0) {
+        seg_base[blockIdx.x] = total >> 16;
+        seg_amb[blockIdx.x] = total & 0xFFFFu;
+    }
+}
+
+// Exclusive scan of the per-segment sums; entry [n] holds the totals.
+__global__ void k_seg_scan(uint32_t *__restrict__ seg_base, uint32_t *__restrict__ seg_amb,
+                           int64_t n) {
+    __shared__ uint32_t ws[32];
+    uint32_t carry_b = 0, carry_a = 0;
+    for (int64_t base = 0; base < n; base += 1024) {
+        const int64_t i = base + threadIdx.x;
+        const uint32_t vb = (i < n) ? seg_base[i] : 0u;
+        const uint32_t va = (i < n) ? seg_amb[i] : 0u;
+        uint32_t tb, ta;
+        const uint32_t eb = block_exclusive_scan<1024>(vb, tb, ws);
+        const uint32_t ea = block_exclusive_scan<1024>(va, ta, ws);
+        if (i < n) {
+            seg_base[i] = carry_b + eb;
+            seg_amb[i] = carry_a + ea;
+        }
+        carry_b += tb;
+        carry_a += ta;
+    }
+    if (threadIdx.x == 0) {
+        seg_base[n] = carry_b;
+        seg_amb[n] = carry_a;
+    }
+}
+
+// Per-site exclusive chain offsets inside a segment block.
+__device__ __forceinline__ void site_offsets(const uint8_t m[kPer], const uint32_t *seg_base,
+                                             const uint32_t *seg_amb, uint32_t *warp_sums,
+                                             uint32_t &P, uint32_t &A) {
+    uint32_t packed = 0;
+#pragma unroll
+    for (int i = 0; i < kPer; ++i) packed += ((uint32_t)meta_base(m[i]) << 16) | meta_amb(m[i]);
+    uint32_t total;
+    const uint32_t ex = block_exclusive_scan<kSegThreads>(packed, total, warp_sums);
+    P = seg_base[blockIdx.x] + (ex >> 16);
+    A = seg_amb[blockIdx.x] + (ex & 0xFFFFu);
+}
+
+struct SiteInfo {
+    float orig[3];
+    bool floor_enabled;
+};
+
+__device__ __forceinline__ SiteInfo site_info(int64_t site, int w, const uint16_t *rgbi,
+                                              const float *lut, const fx_stage *stages,
+                                              const fx_params &p) {
+    SiteInfo si;
+    const int64_t su = 6 * (int64_t)w;
+    int64_t pixel;
+    int stage_index;
+    if (site < su) {
+        pixel = site % w;  // startup originals are row 0 (startup.py:327-336)
+        stage_index = (int)(site / w);
+    } else {
+        pixel = site - su;
+        stage_index = (int)(pixel / w) + 6;
+    }
+    const uint2 raw = reinterpret_cast<const uint2 *>(rgbi)[pixel];
+    si.orig[0] = __ldg(lut + (raw.x & 0xFFFFu));
+    si.orig[1] = __ldg(lut + (raw.x >> 16));
+    si.orig[2] = __ldg(lut + (raw.y & 0xFFFFu));
+    si.floor_enabled = p.driver_gate_primary || stages[stage_index].gate_secondary;
+    return si;
+}
+
+// ---------------------------------------------------------------------------
+// Copy intervals of one RNG-dependent channel
+// ---------------------------------------------------------------------------
+
+struct ChannelView {
+    double cand, cd, env, od;
+    float span;
+    DitherConst dc;
+    __device__ double raw(uint32_t s1) const { return dither_raw_delta(cd, env, span, s1); }
+    __device__ bool low_ok(uint32_t s1) const { return dc.low < cd + raw(s1); }
+    __device__ bool high_ok(uint32_t s1) const { return cd + raw(s1) < dc.high; }
+    __device__ bool floor_test(uint32_t s1) const { return cand + raw(s1) <= od; }
+    __device__ bool copies(uint32_t s1) const {
+        const double d = raw(s1);
+        const double changed = cd + d;
+        const double eff = (dc.low < changed && changed < dc.high) ? d : 0.0;
+        return cand + eff <= od;
+    }
+};
+
+// First state where a monotone predicate differs from its value at 0
+// (2^24 when it never does).
+template <class F>
+__device__ __forceinline__ uint32_t switch_point(F pred) {
+    const bool p0 = pred(0u);
+    if (pred(kLcgMask) == p0) return kLcgMask + 1u;
+    uint32_t lo = 0u, hi = kLcgMask;
+    while (hi - lo > 1u) {
+        const uint32_t mid = lo + ((hi - lo) >> 1);
+        if (pred(mid) == p0) lo = mid;
+        else hi = mid;
+    }
+    return hi;
+}
+
+__device__ void copy_intervals(const ChannelView &cv, AmbEntry &e, uint32_t *err) {
+    uint32_t b[3] = {switch_point([&](uint32_t s) { return cv.low_ok(s); }),
+                     switch_point([&](uint32_t s) { return cv.high_ok(s); }),
+                     switch_point([&](uint32_t s) { return cv.floor_test(s); })};
+    // sort the three breakpoints
+    if (b[0] > b[1]) { const uint32_t t = b[0]; b[0] = b[1]; b[1] = t; }
+    if (b[1] > b[2]) { const uint32_t t = b[1]; b[1] = b[2]; b[2] = t; }
+    if (b[0] > b[1]) { const uint32_t t = b[0]; b[0] = b[1]; b[1] = t; }
+    uint32_t starts[4];
+    int n = 0;
+    starts[n++] = 0u;
+    for (int i = 0; i < 3; ++i)
+        if (b[i] <= kLcgMask && b[i] != starts[n - 1]) starts[n++] = b[i];
+    uint32_t lo[2], hi[2];
+    int intervals = 0;
+    bool open = false;
+    for (int i = 0; i < n; ++i) {
+        const uint32_t first = starts[i];
+        const uint32_t last = (i + 1 < n) ? starts[i + 1] - 1u : kLcgMask;
+        const bool c = cv.copies(first);
+        if (c) {
+            if (open) {
+                hi[intervals - 1] = last;
+            } else {
+                if (intervals == 2) { raise_error(err, FX_ERR_INTERNAL); return; }
+                lo[intervals] = first;
+                hi[intervals] = last;
+                ++intervals;
+                open = true;
+            }
+        } else {
+            open = false;
+        }
+    }
+    // empty interval: l = 0x80 can never match a T value (low byte zero)
+    e.l1 = 0x80u; e.w1 = 0u; e.l2 = 0x80u; e.w2 = 0u;
+    if (intervals >= 1) { e.l1 = lo[0] << 8; e.w1 = (hi[0] - lo[0]) << 8; }
+    if (intervals == 2) { e.l2 = lo[1] << 8; e.w2 = (hi[1] - lo[1]) << 8; }
+}
+
+__global__ void __launch_bounds__(kSegThreads)
+    k_amb(const uint8_t *__restrict__ meta, const double *__restrict__ cand, int64_t sites, int w,
+          const uint16_t *__restrict__ rgbi, const float *__restrict__ lut,
+          const fx_stage *__restrict__ stages, fx_params p, const uint32_t *__restrict__ seg_base,
+          const uint32_t *__restrict__ seg_amb, AmbEntry *__restrict__ entries,
+          uint32_t *__restrict__ pos_out, int64_t capacity, uint32_t *err) {
+    __shared__ uint32_t ws[kSegThreads / 32];
+    const int64_t first = (int64_t)blockIdx.x * kSegment + threadIdx.x * kPer;
+    uint8_t m[kPer];
+    load_meta(meta, first, sites, m);
+    uint32_t P, A;
+    site_offsets(m, seg_base, seg_amb, ws, P, A);
+    const DitherConst dc = dither_const(p);
+#pragma unroll 1
+    for (int i = 0; i < kPer; ++i) {
+        const int64_t site = first + i;
+        if (meta_amb(m[i])) {
+            const SiteInfo si = site_info(site, w, rgbi, lut, stages, p);
+            uint32_t pos = P;
+            uint32_t a = A;
+            for (int c = 0; c < 3; ++c) {
+                const int code = meta_code(m[i], c);
+                if (code == 3) {
+                    ChannelView cv;
+                    cv.cand = cand[3 * site + c];
+                    cv.cd = (double)(float)cv.cand;
+                    cv.dc = dc;
+                    cv.env = ((dc.high - cv.cd) * (cv.cd - dc.low)) * dc.coefficient;
+                    cv.span = (float)((double)p.dither_scales[c] * cv.cd);
+                    cv.od = (double)si.orig[c];
+                    AmbEntry e;
+                    copy_intervals(cv, e, err);
+                    e.a = 0u;
+                    e.c = 0u;
+                    if ((int64_t)a < capacity) {
+                        entries[a] = e;
+                        pos_out[a] = pos;
+                    }
+                    ++a;
+                    pos += 1u;
+                } else {
+                    pos += (uint32_t)code;
+                }
+            }
+        }
+        P += meta_base(m[i]);
+        A += meta_amb(m[i]);
+    }
+}
+
+__global__ void k_coef(AmbEntry *__restrict__ entries, const uint32_t *__restrict__ pos,
+                       const uint32_t *__restrict__ n_amb_ptr, int64_t capacity) {
+    const uint32_t n = (uint32_t)min((int64_t)*n_amb_ptr, capacity);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint64_t gap = (i == 0) ? (uint64_t)pos[0] + 1u : (uint64_t)(pos[i] - pos[i - 1]);
+        const Affine f = lcg_power_t(gap);
+        entries[i].a = f.a;
+        entries[i].c = f.c;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// The serial walk (one resident warp per frame; lane 0 walks)
+// ---------------------------------------------------------------------------
+
+constexpr int kWalkChunk = 256;  // entries per staged chunk (6 KB)
+constexpr int kWalkRing = 4;
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+__global__ void __launch_bounds__(32)
+    k_walk(const AmbEntry *__restrict__ entries, const uint32_t *__restrict__ n_amb_ptr,
+           uint32_t s0, uint32_t *__restrict__ extra_after, int64_t capacity) {
+    __shared__ __align__(16) AmbEntry ring[kWalkRing][kWalkChunk];
+    __shared__ uint32_t out[kWalkRing][kWalkChunk];
+    const int lane = threadIdx.x;
+    const uint32_t n = (uint32_t)min((int64_t)*n_amb_ptr, capacity);
+    const uint32_t chunks = (n + kWalkChunk - 1) / kWalkChunk;
+    constexpr int kVec = kWalkChunk * (int)sizeof(AmbEntry) / 16;
+
+    auto issue = [&](uint32_t k) {
+        if (k < chunks) {
+            const uint32_t first = k * kWalkChunk;
+            const uint32_t count = min((uint32_t)kWalkChunk, n - first);
+            const int vecs = (int)((count * sizeof(AmbEntry) + 15) / 16);
+            const char *src = reinterpret_cast<const char *>(entries + first);
+            char *dst = reinterpret_cast<char *>(ring[k % kWalkRing]);
+            for (int v = lane; v < vecs && v < kVec; v += 32) cp_async16(dst + 16 * v, src + 16 * v);
+        }
+        cp_async_commit();
+    };
+#pragma unroll
+    for (int k = 0; k < kWalkRing - 1; ++k) issue(k);
+
+    uint32_t T = s0 << 8;
+    uint32_t extra = 0u;  // whether the previous channel drew twice
+    uint32_t total = 0u;
+    for (uint32_t k = 0; k < chunks; ++k) {
+        issue(k + kWalkRing - 1);
+        cp_async_wait<kWalkRing - 1>();
+        __syncwarp();
+        const uint32_t count = min((uint32_t)kWalkChunk, n - k * kWalkChunk);
+        if (lane == 0) {
+            const AmbEntry *e = ring[k % kWalkRing];
+            uint32_t *o = out[k % kWalkRing];
+#pragma unroll 4
+            for (uint32_t i = 0; i < count; ++i) {
+                const AmbEntry en = e[i];
+                const uint32_t u0 = en.a * T + en.c;
+                const uint32_t u1 = (en.a * 125u) * T + (en.c * 125u + 256u);
+                T = extra ? u1 : u0;
+                const bool copy = (T - en.l1) <= en.w1 || (T - en.l2) <= en.w2;
+                extra = copy ? 0u : 1u;
+                total += extra;
+                o[i] = total;
+            }
+        }
+        __syncwarp();
+        const uint32_t *o = out[k % kWalkRing];
+        for (uint32_t i = lane; i < count; i += 32) extra_after[k * kWalkChunk + i] = o[i];
+        __syncwarp();
+    }
+    cp_async_wait<0>();
+}
+
+// ---------------------------------------------------------------------------
+// Startup counters, apply + emit, final state
+// ---------------------------------------------------------------------------
+
+__global__ void k_startup_counts(const uint8_t *__restrict__ meta, int w,
+                                 const uint32_t *__restrict__ extra_after, uint32_t s0,
+                                 DevCounters *ctr, int64_t capacity) {
+    __shared__ unsigned long long scratch[8];
+    uint32_t a_run = 0, p_run = 0;
+    for (int k = 0; k < 6; ++k) {
+        unsigned long long att = 0, base = 0, amb = 0;
+        for (int x = threadIdx.x; x < w; x += blockDim.x) {
+            const uint8_t m = meta[(int64_t)k * w + x];
+            att += (m >> 7) & 1u;
+            base += meta_base(m);
+            amb += meta_amb(m);
+        }
+        att = block_sum<256, unsigned long long>(att, scratch);
+        base = block_sum<256, unsigned long long>(base, scratch);
+        amb = block_sum<256, unsigned long long>(amb, scratch);
+        const uint32_t e_start = extra_before(extra_after, a_run, capacity);
+        const uint32_t a_end = a_run + (uint32_t)amb;
+        const uint32_t e_end = extra_before(extra_after, a_end, capacity);
+        if (threadIdx.x == 0) {
+            ctr->su_attempted[k] = att;
+            ctr->su_advances[k] = base + (e_end - e_start);
+        }
+        a_run = a_end;
+        p_run += (uint32_t)base;
+    }
+    if (threadIdx.x == 0) {
+        const uint32_t e = extra_before(extra_after, a_run, capacity);
+        ctr->startup_base = p_run;
+        ctr->startup_amb = a_run;
+        ctr->startup_extra = e;
+        ctr->su_final_state = lcg_jump(s0, (uint64_t)p_run + e);
+    }
+}
+
+__device__ __forceinline__ bool emit_one(float v, const uint32_t *hi, const uint32_t *lo,
+                                         uint16_t &out) {
+    if (!isfinite(v)) return false;
+    double wv = (double)v + 0.5;
+    wv = (wv < 0.0) ? 0.0 : wv;
+    wv = (wv > 65535.0) ? 65535.0 : wv;
+    const uint32_t idx = (uint32_t)wv;  // truncation (output.py:61-73)
+    const unsigned long long prod = (unsigned long long)hi[idx >> 8] * lo[idx & 0xFFu];
+    out = (uint16_t)((prod >> 20) - 1ull);
+    return true;
+}
+
+__global__ void __launch_bounds__(kSegThreads)
+    k_apply(const uint8_t *__restrict__ meta, const double *__restrict__ cand, int64_t sites,
+            int w, const uint16_t *__restrict__ rgbi, const float *__restrict__ lut,
+            const uint32_t *__restrict__ g_high, const uint32_t *__restrict__ g_low,
+            const fx_stage *__restrict__ stages, fx_params p,
+            const uint32_t *__restrict__ seg_base, const uint32_t *__restrict__ seg_amb,
+            const uint32_t *__restrict__ extra_after, uint32_t s0, uint16_t *__restrict__ rgb_out,
+            uint8_t *__restrict__ changed_out, DevCounters *ctr, uint32_t *err,
+            int64_t capacity) {
+    __shared__ uint32_t ws[kSegThreads / 32];
+    __shared__ uint32_t hi[256], lo[256];
+    __shared__ unsigned long long scratch[8];
+    for (int i = threadIdx.x; i < 256; i += kSegThreads) {
+        hi[i] = g_high[i];
+        lo[i] = g_low[i];
+    }
+    const int64_t su = 6 * (int64_t)w;
+    const int64_t first = (int64_t)blockIdx.x * kSegment + threadIdx.x * kPer;
+    uint8_t m[kPer];
+    load_meta(meta, first, sites, m);
+    uint32_t P, A;
+    site_offsets(m, seg_base, seg_amb, ws, P, A);  // contains __syncthreads
+    const DitherConst dc = dither_const(p);
+    unsigned long long att = 0, written = 0, changed = 0, draws_total = 0;
+#pragma unroll 1
+    for (int i = 0; i < kPer; ++i) {
+        const int64_t site = first + i;
+        const uint8_t mi = m[i];
+        if (site >= su && site < sites) {
+            const int64_t pixel = site - su;
+            const SiteInfo si = site_info(site, w, rgbi, lut, stages, p);
+            float values[3] = {si.orig[0], si.orig[1], si.orig[2]};
+            if (mi & 0x80u) {
+                const int amb = meta_amb(mi);
+                const uint32_t e_before = extra_before(extra_after, A, capacity);
+                const uint32_t extra = extra_before(extra_after, A + amb, capacity) - e_before;
+                uint32_t state = lcg_jump(s0, (uint64_t)P + e_before);
+                const double *cd = cand + 3 * site;
+                const double c3[3] = {cd[0], cd[1], cd[2]};
+                bool valid = true;
+#pragma unroll
+                for (int c = 0; c < 3; ++c) valid &= isfinite(c3[c]) && c3[c] > 0.0;
+                uint32_t draws = 0;
+                if (valid) {
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        int drew;
+                        const double firstd = dither_delta(c3[c], p.dither_scales[c], dc, state, drew);
+                        draws += drew;
+                        if (si.floor_enabled && c3[c] + firstd <= (double)si.orig[c]) {
+                            values[c] = si.orig[c];
+                        } else {
+                            double d = firstd;
+                            if (si.floor_enabled) {
+                                d = dither_delta(c3[c], p.dither_scales[c], dc, state, drew);
+                                draws += drew;
+                            }
+                            values[c] = (float)(c3[c] + d);
+                        }
+                    }
+                }
+                if ((int64_t)(A + amb) <= capacity && draws != (uint32_t)meta_base(mi) + extra)
+                    raise_error(err, FX_ERR_INTERNAL);
+                att += 1;
+                draws_total += draws;
+                written += (values[0] != si.orig[0] || values[1] != si.orig[1] ||
+                            values[2] != si.orig[2]);
+            }
+            uint16_t e[3], e0[3];
+            bool ok = true;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                ok &= emit_one(values[c], hi, lo, e[c]);
+                ok &= emit_one(si.orig[c], hi, lo, e0[c]);
+            }
+            if (!ok) raise_error(err, FX_ERR_NONFINITE_WORK);
+            const bool ch = (e[0] != e0[0]) || (e[1] != e0[1]) || (e[2] != e0[2]);
+            changed += ch;
+            uint16_t *o = rgb_out + 3 * pixel;
+            o[0] = e[0];
+            o[1] = e[1];
+            o[2] = e[2];
+            if (changed_out) changed_out[pixel] = ch ? 1 : 0;
+        }
+        P += meta_base(mi);
+        A += meta_amb(mi);
+    }
+    att = block_sum<kSegThreads, unsigned long long>(att, scratch);
+    written = block_sum<kSegThreads, unsigned long long>(written, scratch);
+    changed = block_sum<kSegThreads, unsigned long long>(changed, scratch);
+    draws_total = block_sum<kSegThreads, unsigned long long>(draws_total, scratch);
+    if (threadIdx.x == 0) {
+        if (att) atomicAdd(&ctr->attempted, att);
+        if (written) atomicAdd(&ctr->written, written);
+        if (changed) atomicAdd(&ctr->changed, changed);
+        if (draws_total) atomicAdd(&ctr->public_advances, draws_total);
+    }
+}
+
+__global__ void k_final(const uint32_t *__restrict__ seg_base, const uint32_t *__restrict__ seg_amb,
+                        int64_t segments, const uint32_t *__restrict__ extra_after, uint32_t s0,
+                        DevCounters *ctr, uint32_t *err, int64_t capacity) {
+    const uint32_t p_total = seg_base[segments];
+    const uint32_t a_total = seg_amb[segments];
+    const uint32_t e_total = extra_before(extra_after, a_total, capacity);
+    ctr->n_amb = a_total;
+    ctr->final_state = lcg_jump(s0, (uint64_t)p_total + e_total);
+    const unsigned long long expect =
+        (unsigned long long)(p_total - ctr->startup_base) + (e_total - ctr->startup_extra);
+    if ((int64_t)a_total <= capacity && expect != ctr->public_advances)
+        raise_error(err, FX_ERR_INTERNAL);
+}
+
+// ---------------------------------------------------------------------------
+// Launcher
+// ---------------------------------------------------------------------------
+
+cudaError_t launch_writer(const Geometry &g, const uint8_t *meta, const double *cand,
+                          const uint16_t *rgbi, const float *lut, const uint32_t *high,
+                          const uint32_t *low, const fx_stage *stages, const fx_params &p,
+                          uint32_t s0, const WriterBuffers &b, uint16_t *rgb_out,
+                          uint8_t *changed_out, uint32_t *err, cudaStream_t stream) {
+    const int64_t segs = g.segments;
+    DevCounters *ctr = reinterpret_cast<DevCounters *>(b.counters);
+    cudaMemsetAsync(ctr, 0, sizeof(DevCounters), stream);
+    k_seg_sums<<<(unsigned)segs, kSegThreads, 0, stream>>>(meta, g.sites, b.seg_base, b.seg_amb);
+    k_seg_scan<<<1, 1024, 0, stream>>>(b.seg_base, b.seg_amb, segs);
+    k_amb<<<(unsigned)segs, kSegThreads, 0, stream>>>(meta, cand, g.sites, g.w, rgbi, lut, stages,
+                                                      p, b.seg_base, b.seg_amb, b.entries, b.pos,
+                                                      b.capacity, err);
+    const uint32_t *n_amb = b.seg_amb + segs;
+    k_coef<<<1184, 256, 0, stream>>>(b.entries, b.pos, n_amb, b.capacity);
+    k_walk<<<1, 32, 0, stream>>>(b.entries, n_amb, s0 & kLcgMask, b.extra_after, b.capacity);
+    k_startup_counts<<<1, 256, 0, stream>>>(meta, g.w, b.extra_after, s0 & kLcgMask, ctr,
+                                            b.capacity);
+    k_apply<<<(unsigned)segs, kSegThreads, 0, stream>>>(
+        meta, cand, g.sites, g.w, rgbi, lut, high, low, stages, p, b.seg_base, b.seg_amb,
+        b.extra_after, s0 & kLcgMask, rgb_out, changed_out, ctr, err, b.capacity);
+    k_final<<<1, 1, 0, stream>>>(b.seg_base, b.seg_amb, segs, b.extra_after, s0 & kLcgMask,
+                                 ctr, err, b.capacity);
+    return cudaGetLastError();
+}
+
+size_t dev_counters_bytes() { return sizeof(DevCounters); }
+
+void counters_to_host(const void *dev_copy, fx_counters *out) {
+    const DevCounters &c = *reinterpret_cast<const DevCounters *>(dev_copy);
+    out->attempted = (int64_t)c.attempted;
+    out->written = (int64_t)c.written;
+    out->public_advances = (int64_t)c.public_advances;
+    out->changed = (int64_t)c.changed;
+    out->final_state = c.final_state;
+    out->startup_final_state = c.su_final_state;
+    for (int k = 0; k < 6; ++k) {
+        out->startup_attempted[k] = (int64_t)c.su_attempted[k];
+        out->startup_advances[k] = (int64_t)c.su_advances[k];
+    }
+}
+
+uint32_t counters_n_amb(const void *dev_copy) {
+    return reinterpret_cast<const DevCounters *>(dev_copy)->n_amb;
+}
+
+}  // namespace fx

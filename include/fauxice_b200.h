@@ -1,0 +1,185 @@
+/*
+ * fauxice_b200.h -- C ABI of the B200 Digital ICE processing core.
+ *
+ * One shared library, libfauxice_b200.so, built for sm_100a.  Every entry
+ * point takes plain pointers and sizes and returns an int status (FX_OK on
+ * success); no C++ exception crosses the boundary.  Host buffers are caller
+ * owned; device memory is owned by the context.
+ *
+ * The reference package (portable_digital_ice 0.3.1) has no foreign-function
+ * interface of its own: its backends are Python functions.  Each entry point
+ * below states which reference function (src/portable_digital_ice/...:line)
+ * it stands in for, so a Python shim can expose the reference's backend
+ * contract (process_cuda / run_streaming_replay_cuda signatures) on top.
+ */
+#ifndef FAUXICE_B200_H
+#define FAUXICE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define FX_API __attribute__((visibility("default")))
+#else
+#define FX_API
+#endif
+
+#define FX_ABI_VERSION 1
+
+/* Status codes.  The non-finite and geometry codes carry the same meaning as
+ * the ValueError messages the reference raises (messages in comments). */
+enum fx_status {
+    FX_OK = 0,
+    FX_ERR_INVALID_ARGUMENT = 1,
+    FX_ERR_NO_DEVICE = 2,          /* no CUDA device visible */
+    FX_ERR_UNSUPPORTED_DEVICE = 3, /* not an sm_100 (B200-class) device */
+    FX_ERR_OUT_OF_MEMORY = 4,      /* device allocation / admission failed */
+    FX_ERR_NONFINITE_AUX = 5,      /* "auxiliary score input must be a finite HxW plane" */
+    FX_ERR_NONFINITE_WORK = 6,     /* "work RGB must be finite" */
+    FX_ERR_COMBINER_INPUT = 7,     /* "combiner inputs must be finite" */
+    FX_ERR_DITHER_INPUT = 8,       /* "dither inputs must be finite" */
+    FX_ERR_SETTER_ONE = 9,         /* "X3A setter scale cannot equal one" */
+    FX_ERR_STAGE_NONFINITE = 10,   /* stage calibration field not finite float32 */
+    FX_ERR_ALPHA_ONE_UNBOUND = 11, /* "alpha==1 requires the runtime-configured ..." */
+    FX_ERR_GEOMETRY = 12,          /* frame too small for the startup replay */
+    FX_ERR_CANCELLED = 13,
+    FX_ERR_TIMEOUT = 14,
+    FX_ERR_CUDA = 15,              /* a CUDA runtime call failed */
+    FX_ERR_INTERNAL = 16,          /* a device self-consistency check failed */
+    FX_ERR_TABLES = 17,            /* fx_set_tables was not called */
+    FX_PENDING = 18                /* fx_poll: request still running */
+};
+
+/* Constants of the hot path, as float32 values.  Field meanings follow the
+ * reference's AuxiliaryParameters / ScoreParameters (x3a.py:166-242),
+ * DecisionParameters (x3a.py:337-348), ReconstructionParameters
+ * (reconstruction.py:613-669) and DitherBounds (dither.py:34-56). */
+typedef struct fx_params {
+    float score_addend, score_scale, score_offset, score_floor;
+    int32_t horizontal_minimum; /* cutoff < resolution metric (x3a.py:266-268) */
+    int32_t visible_channel;    /* 0, 1 or 2 */
+    float decision_threshold;
+    int32_t count_limit, radius;
+    int32_t cross_neighbor;     /* metric > cross-neighbor cutoff */
+    int32_t coarse_enabled;
+    float coarse_slopes[3];
+    int32_t band_enabled[3];
+    float band_scales[3];
+    float factors_a[9], factors_b[9]; /* [band][channel] */
+    float configured_strengths[3];
+    int32_t driver_gate_primary;
+    float dither_scales[3];
+    float dither_low, dither_high;
+} fx_params;
+
+/* Dynamic calibration of one scheduler stage (stage_parameters.py:131-149).
+ * A table holds stages 1..H+6 at indices 0..H+5.  Row y reads the auxiliary
+ * fields of stage y+1, the score base of stage y+2 and the writer fields of
+ * stage y+7 (stage_parameters.py:207-232). */
+typedef struct fx_stage {
+    float alpha, offset, replacement;
+    int32_t replacement_valid;
+    float score_base, coarse;
+    int32_t gate_secondary, row_gate;
+} fx_stage;
+
+/* StreamingReplayResult / StartupReplayResult counters
+ * (streaming.py:63-75, startup.py:37-43). */
+typedef struct fx_counters {
+    int64_t attempted, written, public_advances, changed;
+    uint32_t final_state, startup_final_state;
+    int64_t startup_attempted[6];
+    int64_t startup_advances[6];
+} fx_counters;
+
+/* One frame for fx_process / fx_submit.  Host pointers. */
+typedef struct fx_frame {
+    const uint16_t *main_rgbi; /* H x W x 4, C order */
+    int32_t height, width;
+    const fx_params *params;
+    const fx_stage *stages;    /* H+6 entries, or NULL: derive them on the device
+                                  from the frame (content-derived provider) */
+    uint32_t rng_state;        /* 24-bit LCG state at job start (0x3045) */
+    uint16_t *rgb_out;         /* H x W x 3 */
+    float *score_out;          /* optional H x W */
+    uint8_t *changed_out;      /* optional H x W */
+} fx_frame;
+
+typedef struct fx_context fx_context;
+
+/* Library ABI version (FX_ABI_VERSION). */
+FX_API int fx_version(void);
+
+/* 0 when `device` is a usable sm_100 GPU; otherwise a status and a reason.
+ * Stands in for the device probe of cuda_backend/engine.py:168-224. */
+FX_API int fx_device_check(int device, char *reason, size_t reason_len);
+
+FX_API int fx_context_create(int device, fx_context **out);
+FX_API void fx_context_destroy(fx_context *ctx);
+
+/* Last error text of the context (or of the library when ctx is NULL). */
+FX_API int fx_last_error(const fx_context *ctx, char *buf, size_t len);
+
+/* Upload the response LUT (x3a.py:111-132) and the two inverse-response
+ * factor tables (output.py:40-58).  The caller hash-checks them. */
+FX_API int fx_set_tables(fx_context *ctx, const float *lut65536, const uint32_t *high256,
+                         const uint32_t *low256);
+
+/* prepass.py:96-236 (reduce_prepass_frame) for a fresh record with the
+ * captured selector-8 parameters; host computation. */
+FX_API int fx_reduce_prepass(const uint16_t *prepass_rgbi, int32_t height, int32_t width,
+                             const float *lut65536, uint8_t payload[64], int64_t *valid_pixels,
+                             int64_t *fully_valid_tiles);
+
+/* producer_parameters.py:266-495 (derive_producer_record_schedule) on the
+ * device: the four per-row record fields the X3A setter reads. */
+FX_API int fx_producer_rows(fx_context *ctx, const uint16_t *main_rgbi, int32_t height,
+                            int32_t width, float *scaled_input, float *input_scale,
+                            float *mean_visible, float *mean_infrared);
+
+/* producer_parameters.py:498-541 with stage_parameters.py:93-197: the stage
+ * table (H+6 entries) built from per-row producer fields; host computation. */
+FX_API int fx_stage_table(int32_t height, const float *scaled_input, const float *input_scale,
+                          const float *mean_visible, const float *mean_infrared,
+                          float auxiliary_factor_b, fx_stage *stages);
+
+/* The whole main-scan pass for one frame, synchronous, host buffers:
+ * streaming.py:365-552 (run_streaming_replay) / cuda_backend/engine.py:183
+ * (run_streaming_replay_cuda), including the hidden startup replay, the
+ * sequential dither writer, emit, counters and diagnostics. */
+FX_API int fx_process(fx_context *ctx, const fx_frame *frame, fx_counters *counters);
+
+/* Same pass on device-resident buffers, enqueued on `stream` (a
+ * cudaStream_t, or NULL for the context stream).  d_rgbi, d_rgb_out,
+ * d_score_out and d_changed_out are device pointers.  When `counters` is
+ * non-NULL the call waits for completion and fills it; otherwise it returns
+ * after enqueueing and fx_sync_counters fetches them later. */
+FX_API int fx_process_device(fx_context *ctx, const uint16_t *d_rgbi, int32_t height,
+                             int32_t width, const fx_params *params, const fx_stage *stages,
+                             uint32_t rng_state, uint16_t *d_rgb_out, float *d_score_out,
+                             uint8_t *d_changed_out, void *stream, fx_counters *counters);
+FX_API int fx_sync_counters(fx_context *ctx, fx_counters *counters);
+
+/* Asynchronous requests for batching and serving (no reference counterpart:
+ * the reference processes one job per call).  Up to `slots` frames run
+ * concurrently, each on its own stream with its own device buffers. */
+FX_API int fx_set_slots(fx_context *ctx, int32_t slots);
+FX_API int fx_submit(fx_context *ctx, const fx_frame *frame, int64_t *ticket);
+FX_API int fx_poll(fx_context *ctx, int64_t ticket);
+FX_API int fx_wait(fx_context *ctx, int64_t ticket, int64_t timeout_ns, fx_counters *counters);
+
+/* Free / total device memory, for admission control. */
+FX_API int fx_mem_info(fx_context *ctx, size_t *free_bytes, size_t *total_bytes);
+
+/* Device bytes one frame of the given size needs (admission estimate). */
+FX_API int64_t fx_frame_bytes(int32_t height, int32_t width);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FAUXICE_B200_H */
