@@ -690,7 +690,7 @@ __global__ void k_startup(const uint16_t *__restrict__ rgbi, StartupView v,
 cudaError_t launch_analysis(const uint16_t *rgbi, const Geometry &g, const float *lut,
                             const fx_stage *stages, const fx_params &p, float *aux, float *hs,
                             float *hwa, float *hwr, int64_t plane, double *cand, uint8_t *meta,
-                            uint32_t *err, cudaStream_t stream) {
+                            uint32_t *err, cudaStream_t stream, const Marks &marks) {
     {
         dim3 block(256), grid((g.w + 255) / 256, g.h);
         k_auxiliary<<<grid, block, 0, stream>>>(rgbi, g.h, g.w, lut, stages, p.visible_channel,
@@ -700,28 +700,34 @@ cudaError_t launch_analysis(const uint16_t *rgbi, const Geometry &g, const float
         dim3 block(256), grid((g.pitch + 255) / 256, g.prow);
         k_planes<<<grid, block, 0, stream>>>(rgbi, g, lut, stages, p, aux, hs, hwa, hwr, plane);
     }
+    marks.mark(2, stream);
     {
         dim3 grid(g.tw, g.th);
         k_stencil<<<grid, kStencilThreads, sizeof(StencilSmem), stream>>>(
             rgbi, g, lut, stages, p, aux, hs, hwa, hwr, plane, cand, meta, err);
     }
+    marks.mark(3, stream);
     {
         StartupView v{g, aux, hs, hwa, hwr, plane, p.cross_neighbor ? 5 : 4};
         dim3 block(128), grid((g.w + 127) / 128, 6);
         k_startup<<<grid, block, 0, stream>>>(rgbi, v, lut, stages, p, cand, meta, err);
     }
+    marks.mark(4, stream);
     return cudaGetLastError();
 }
 
 size_t stencil_smem_bytes() { return sizeof(StencilSmem); }
 
 cudaError_t producer_init();
+cudaError_t writer_init();
 
 // Opt in to the dynamic shared memory the tiled kernels use (once per
 // device, with the device current).
 cudaError_t analysis_init() {
     cudaError_t e = cudaFuncSetAttribute(k_stencil, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)sizeof(StencilSmem));
+    if (e != cudaSuccess) return e;
+    e = writer_init();
     if (e != cudaSuccess) return e;
     return producer_init();
 }

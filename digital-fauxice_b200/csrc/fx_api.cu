@@ -108,6 +108,7 @@ static size_t arena_layout(const Geometry &g, int64_t amb_cap, Arena *a) {
 
 struct Slot {
     cudaStream_t stream = nullptr;
+    cudaStream_t last_stream = nullptr;  // stream of the last device-buffer pass
     cudaEvent_t done = nullptr;
     Arena arena;
     // pinned staging for asynchronous requests
@@ -130,6 +131,11 @@ struct Slot {
 
 struct fx_context {
     int device = 0;
+    bool profile = false;
+    std::vector<std::vector<cudaEvent_t>> pending;  // recorded, not yet read
+    std::vector<std::vector<cudaEvent_t>> spare;
+    double profile_ms[fx::kProfileStages] = {0};
+    int64_t profile_passes = 0;
     float *lut = nullptr;
     uint32_t *high = nullptr, *low = nullptr;
     bool tables = false;
@@ -219,7 +225,21 @@ static int enqueue_pass(fx_context *ctx, Slot &s, const Geometry &g, const fx_pa
                         uint16_t *d_out, uint8_t *d_changed, bool producer_rows) {
     Arena &a = s.arena;
     cudaStream_t st = s.stream;
+    Marks marks;
+    if (ctx->profile) {
+        std::vector<cudaEvent_t> ev;
+        if (!ctx->spare.empty()) {
+            ev = std::move(ctx->spare.back());
+            ctx->spare.pop_back();
+        } else {
+            ev.resize(kProfileStages + 1);
+            for (auto &e : ev) FX_CUDA(ctx, cudaEventCreate(&e));
+        }
+        ctx->pending.push_back(std::move(ev));
+        marks.events = ctx->pending.back().data();
+    }
     FX_CUDA(ctx, cudaMemsetAsync(a.err, 0, 16, st));
+    marks.mark(0, st);
     if (host_stages) {
         FX_CUDA(ctx, cudaMemcpyAsync(a.stages, host_stages, (g.h + 6) * sizeof(fx_stage),
                                      cudaMemcpyHostToDevice, st));
@@ -227,12 +247,13 @@ static int enqueue_pass(fx_context *ctx, Slot &s, const Geometry &g, const fx_pa
         FX_CUDA(ctx, launch_producer(d_in, g.h, g.w, ctx->lut, a.producer, a.stages,
                                      producer_rows ? a.rows : nullptr, a.err, st));
     }
+    marks.mark(1, st);
     FX_CUDA(ctx, launch_analysis(d_in, g, ctx->lut, a.stages, p, a.aux, a.hs, a.hwa, a.hwr,
-                                 (int64_t)g.prow * g.pitch, a.cand, a.meta, a.err, st));
+                                 (int64_t)g.prow * g.pitch, a.cand, a.meta, a.err, st, marks));
     WriterBuffers wb{a.seg_base, a.seg_amb, a.entries, a.pos, a.extra, a.counters,
                      a.amb_capacity};
     FX_CUDA(ctx, launch_writer(g, a.meta, a.cand, d_in, ctx->lut, ctx->high, ctx->low, a.stages,
-                               p, rng, wb, d_out, d_changed, a.err, st));
+                               p, rng, wb, d_out, d_changed, a.err, st, marks));
     return FX_OK;
 }
 
@@ -387,6 +408,10 @@ FX_API void fx_context_destroy(fx_context *ctx) {
         if (s.done) cudaEventDestroy(s.done);
         if (s.stream) cudaStreamDestroy(s.stream);
     }
+    for (auto &v : ctx->pending)
+        for (auto e : v) cudaEventDestroy(e);
+    for (auto &v : ctx->spare)
+        for (auto e : v) cudaEventDestroy(e);
     if (ctx->lut) cudaFree(ctx->lut);
     if (ctx->high) cudaFree(ctx->high);
     if (ctx->low) cudaFree(ctx->low);
@@ -523,6 +548,7 @@ FX_API int fx_process_device(fx_context *ctx, const uint16_t *d_rgbi, int32_t h,
         rc = ensure_arena(ctx, s, g, default_amb_capacity(g));
         if (!rc) rc = enqueue_pass(ctx, s, g, *params, stages, rng, d_rgbi, d_out, d_changed, false);
     }
+    s.last_stream = s.stream;
     if (!rc && d_score)
         rc = cudaMemcpy2DAsync(d_score, (size_t)w * 4, s.arena.hs + g.padded_index(0, 0),
                                (size_t)g.pitch * 4, (size_t)w * 4, h, cudaMemcpyDeviceToDevice,
@@ -538,10 +564,15 @@ FX_API int fx_sync_counters(fx_context *ctx, fx_counters *counters) {
     std::lock_guard<std::mutex> lock(ctx->mu);
     cudaSetDevice(ctx->device);
     Slot &s = slot0(ctx);
+    cudaStream_t st = s.last_stream ? s.last_stream : s.stream;
     char *hc = reinterpret_cast<char *>(s.h_ctr);
-    FX_CUDA(ctx, cudaMemcpy(hc, s.arena.counters, dev_counters_bytes(), cudaMemcpyDeviceToHost));
+    FX_CUDA(ctx, cudaMemcpyAsync(hc, s.arena.counters, dev_counters_bytes(),
+                                 cudaMemcpyDeviceToHost, st));
+    FX_CUDA(ctx, cudaMemcpyAsync(hc + dev_counters_bytes(), s.arena.err, 4,
+                                 cudaMemcpyDeviceToHost, st));
+    FX_CUDA(ctx, cudaStreamSynchronize(st));
     uint32_t err;
-    FX_CUDA(ctx, cudaMemcpy(&err, s.arena.err, 4, cudaMemcpyDeviceToHost));
+    std::memcpy(&err, hc + dev_counters_bytes(), 4);
     bool overflow;
     const int rc = finish_counters(ctx, s, hc, err, counters, &overflow);
     if (rc) return rc;
@@ -718,6 +749,38 @@ FX_API int fx_wait(fx_context *ctx, int64_t ticket, int64_t timeout_ns, fx_count
         }
         std::this_thread::sleep_for(std::chrono::microseconds(50));
     }
+}
+
+FX_API int fx_profile_enable(fx_context *ctx, int enable) {
+    if (!ctx) return FX_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    ctx->profile = enable != 0;
+    return FX_OK;
+}
+
+FX_API int fx_profile_read(fx_context *ctx, double *ms, int64_t *passes, int reset) {
+    if (!ctx) return FX_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    cudaSetDevice(ctx->device);
+    for (auto &ev : ctx->pending) {
+        FX_CUDA(ctx, cudaEventSynchronize(ev[kProfileStages]));
+        for (int i = 0; i < kProfileStages; ++i) {
+            float t = 0.0f;
+            FX_CUDA(ctx, cudaEventElapsedTime(&t, ev[i], ev[i + 1]));
+            ctx->profile_ms[i] += t;
+        }
+        ctx->profile_passes += 1;
+        ctx->spare.push_back(std::move(ev));
+    }
+    ctx->pending.clear();
+    if (ms)
+        for (int i = 0; i < kProfileStages; ++i) ms[i] = ctx->profile_ms[i];
+    if (passes) *passes = ctx->profile_passes;
+    if (reset) {
+        for (int i = 0; i < kProfileStages; ++i) ctx->profile_ms[i] = 0.0;
+        ctx->profile_passes = 0;
+    }
+    return FX_OK;
 }
 
 FX_API int fx_mem_info(fx_context *ctx, size_t *free_bytes, size_t *total_bytes) {

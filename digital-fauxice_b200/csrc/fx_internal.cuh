@@ -63,9 +63,10 @@ __host__ __device__ __forceinline__ int meta_amb(uint8_t m) {
 // One RNG-dependent channel for the serial walk.  In "T space" the 24-bit
 // state s is held as T = s << 8, so the LCG s -> 125 s + 1 (mod 2^24)
 // becomes T -> 125 T + 256 (mod 2^32) and interval tests need no masking.
-struct AmbEntry {
+struct __align__(16) AmbEntry {
     uint32_t l1, w1, l2, w2; // copy iff (T - l1) <= w1 || (T - l2) <= w2
-    uint32_t a, c;           // T_first_draw = a * T_prev + c  (no extra draw before)
+    uint32_t a0, c0;         // T_first_draw = a0 * T_prev + c0 (previous channel drew once)
+    uint32_t a1, c1;         // T_first_draw = a1 * T_prev + c1 (previous channel drew twice)
 };
 
 // ---------------------------------------------------------------------------
@@ -161,16 +162,27 @@ struct WriterBuffers {
     int64_t capacity;
 };
 
+// Optional CUDA events between kernel groups (measurement only).
+// mark(i) records boundary i: 0 before the producer, then after each stage.
+struct Marks {
+    cudaEvent_t *events = nullptr;  // kProfileStages + 1 events, or null
+    __host__ void mark(int i, cudaStream_t s) const {
+        if (events) cudaEventRecord(events[i], s);
+    }
+};
+constexpr int kProfileStages = 7;
+
 cudaError_t analysis_init();
 cudaError_t launch_analysis(const uint16_t *rgbi, const Geometry &g, const float *lut,
                             const fx_stage *stages, const fx_params &p, float *aux, float *hs,
                             float *hwa, float *hwr, int64_t plane, double *cand, uint8_t *meta,
-                            uint32_t *err, cudaStream_t stream);
+                            uint32_t *err, cudaStream_t stream, const Marks &marks);
 cudaError_t launch_writer(const Geometry &g, const uint8_t *meta, const double *cand,
                           const uint16_t *rgbi, const float *lut, const uint32_t *high,
                           const uint32_t *low, const fx_stage *stages, const fx_params &p,
                           uint32_t s0, const WriterBuffers &b, uint16_t *rgb_out,
-                          uint8_t *changed_out, uint32_t *err, cudaStream_t stream);
+                          uint8_t *changed_out, uint32_t *err, cudaStream_t stream,
+                          const Marks &marks);
 size_t dev_counters_bytes();
 void counters_to_host(const void *dev_copy, fx_counters *out);
 uint32_t counters_n_amb(const void *dev_copy);

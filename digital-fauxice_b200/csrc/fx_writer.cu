@@ -293,8 +293,7 @@ __global__ void __launch_bounds__(kSegThreads)
                     cv.od = (double)si.orig[c];
                     AmbEntry e;
                     copy_intervals(cv, e, err);
-                    e.a = 0u;
-                    e.c = 0u;
+                    e.a0 = e.c0 = e.a1 = e.c1 = 0u;
                     if ((int64_t)a < capacity) {
                         entries[a] = e;
                         pos_out[a] = pos;
@@ -317,8 +316,11 @@ __global__ void k_coef(AmbEntry *__restrict__ entries, const uint32_t *__restric
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint64_t gap = (i == 0) ? (uint64_t)pos[0] + 1u : (uint64_t)(pos[i] - pos[i - 1]);
         const Affine f = lcg_power_t(gap);
-        entries[i].a = f.a;
-        entries[i].c = f.c;
+        const Affine f1 = affine_compose(Affine{125u, 256u}, f);  // one more draw
+        entries[i].a0 = f.a;
+        entries[i].c0 = f.c;
+        entries[i].a1 = (i == 0) ? f.a : f1.a;  // no previous channel before the first
+        entries[i].c1 = (i == 0) ? f.c : f1.c;
     }
 }
 
@@ -326,8 +328,9 @@ __global__ void k_coef(AmbEntry *__restrict__ entries, const uint32_t *__restric
 // The serial walk (one resident warp per frame; lane 0 walks)
 // ---------------------------------------------------------------------------
 
-constexpr int kWalkChunk = 256;  // entries per staged chunk (6 KB)
+constexpr int kWalkChunk = 512;  // entries per staged chunk (16 KB)
 constexpr int kWalkRing = 4;
+constexpr int kWalkGroup = 8;    // steps per register batch
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
     const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
@@ -339,11 +342,29 @@ __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
+struct WalkSmem {
+    AmbEntry ring[kWalkRing][kWalkChunk];
+    uint32_t out[kWalkRing][kWalkChunk];
+};
+
+// One walk step.  The select on the previous step's outcome is the only
+// serial dependency besides the multiply: both candidate states are formed
+// while the previous interval test resolves.
+__device__ __forceinline__ void walk_step(const uint4 &lw, const uint4 &ac, uint32_t &T,
+                                          uint32_t &extra, uint32_t &total) {
+    const uint32_t u0 = ac.x * T + ac.y;
+    const uint32_t u1 = ac.z * T + ac.w;
+    T = extra ? u1 : u0;
+    const bool hit = (T - lw.x) <= lw.y || (T - lw.z) <= lw.w;
+    extra = hit ? 0u : 1u;
+    total += extra;
+}
+
 __global__ void __launch_bounds__(32)
     k_walk(const AmbEntry *__restrict__ entries, const uint32_t *__restrict__ n_amb_ptr,
            uint32_t s0, uint32_t *__restrict__ extra_after, int64_t capacity) {
-    __shared__ __align__(16) AmbEntry ring[kWalkRing][kWalkChunk];
-    __shared__ uint32_t out[kWalkRing][kWalkChunk];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    WalkSmem &S = *reinterpret_cast<WalkSmem *>(smem_raw);
     const int lane = threadIdx.x;
     const uint32_t n = (uint32_t)min((int64_t)*n_amb_ptr, capacity);
     const uint32_t chunks = (n + kWalkChunk - 1) / kWalkChunk;
@@ -353,9 +374,9 @@ __global__ void __launch_bounds__(32)
         if (k < chunks) {
             const uint32_t first = k * kWalkChunk;
             const uint32_t count = min((uint32_t)kWalkChunk, n - first);
-            const int vecs = (int)((count * sizeof(AmbEntry) + 15) / 16);
+            const int vecs = (int)(count * sizeof(AmbEntry) / 16);
             const char *src = reinterpret_cast<const char *>(entries + first);
-            char *dst = reinterpret_cast<char *>(ring[k % kWalkRing]);
+            char *dst = reinterpret_cast<char *>(S.ring[k % kWalkRing]);
             for (int v = lane; v < vecs && v < kVec; v += 32) cp_async16(dst + 16 * v, src + 16 * v);
         }
         cp_async_commit();
@@ -372,26 +393,58 @@ __global__ void __launch_bounds__(32)
         __syncwarp();
         const uint32_t count = min((uint32_t)kWalkChunk, n - k * kWalkChunk);
         if (lane == 0) {
-            const AmbEntry *e = ring[k % kWalkRing];
-            uint32_t *o = out[k % kWalkRing];
-#pragma unroll 4
-            for (uint32_t i = 0; i < count; ++i) {
-                const AmbEntry en = e[i];
-                const uint32_t u0 = en.a * T + en.c;
-                const uint32_t u1 = (en.a * 125u) * T + (en.c * 125u + 256u);
-                T = extra ? u1 : u0;
-                const bool copy = (T - en.l1) <= en.w1 || (T - en.l2) <= en.w2;
-                extra = copy ? 0u : 1u;
-                total += extra;
+            const uint4 *__restrict__ e4 = reinterpret_cast<const uint4 *>(S.ring[k % kWalkRing]);
+            uint32_t *__restrict__ o = S.out[k % kWalkRing];
+            const uint32_t groups = count / kWalkGroup;
+            uint4 lw[kWalkGroup], ac[kWalkGroup];
+            if (groups) {
+#pragma unroll
+                for (int j = 0; j < kWalkGroup; ++j) {
+                    lw[j] = e4[2 * j];
+                    ac[j] = e4[2 * j + 1];
+                }
+            }
+            for (uint32_t g = 0; g < groups; ++g) {
+                uint4 nlw[kWalkGroup], nac[kWalkGroup];
+                const uint32_t next = (g + 1 < groups) ? (g + 1) * kWalkGroup : g * kWalkGroup;
+#pragma unroll
+                for (int j = 0; j < kWalkGroup; ++j) {
+                    nlw[j] = e4[2 * (next + j)];
+                    nac[j] = e4[2 * (next + j) + 1];
+                }
+                uint32_t tot[kWalkGroup];
+#pragma unroll
+                for (int j = 0; j < kWalkGroup; ++j) {
+                    walk_step(lw[j], ac[j], T, extra, total);
+                    tot[j] = total;
+                }
+                uint4 *o4 = reinterpret_cast<uint4 *>(o + g * kWalkGroup);
+                o4[0] = make_uint4(tot[0], tot[1], tot[2], tot[3]);
+                o4[1] = make_uint4(tot[4], tot[5], tot[6], tot[7]);
+#pragma unroll
+                for (int j = 0; j < kWalkGroup; ++j) {
+                    lw[j] = nlw[j];
+                    ac[j] = nac[j];
+                }
+            }
+            for (uint32_t i = groups * kWalkGroup; i < count; ++i) {
+                walk_step(e4[2 * i], e4[2 * i + 1], T, extra, total);
                 o[i] = total;
             }
         }
         __syncwarp();
-        const uint32_t *o = out[k % kWalkRing];
+        const uint32_t *o = S.out[k % kWalkRing];
         for (uint32_t i = lane; i < count; i += 32) extra_after[k * kWalkChunk + i] = o[i];
         __syncwarp();
     }
     cp_async_wait<0>();
+}
+
+size_t walk_smem_bytes() { return sizeof(WalkSmem); }
+
+cudaError_t writer_init() {
+    return cudaFuncSetAttribute(k_walk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(WalkSmem));
 }
 
 // ---------------------------------------------------------------------------
@@ -566,7 +619,8 @@ cudaError_t launch_writer(const Geometry &g, const uint8_t *meta, const double *
                           const uint16_t *rgbi, const float *lut, const uint32_t *high,
                           const uint32_t *low, const fx_stage *stages, const fx_params &p,
                           uint32_t s0, const WriterBuffers &b, uint16_t *rgb_out,
-                          uint8_t *changed_out, uint32_t *err, cudaStream_t stream) {
+                          uint8_t *changed_out, uint32_t *err, cudaStream_t stream,
+                          const Marks &marks) {
     const int64_t segs = g.segments;
     DevCounters *ctr = reinterpret_cast<DevCounters *>(b.counters);
     cudaMemsetAsync(ctr, 0, sizeof(DevCounters), stream);
@@ -577,7 +631,10 @@ cudaError_t launch_writer(const Geometry &g, const uint8_t *meta, const double *
                                                       b.capacity, err);
     const uint32_t *n_amb = b.seg_amb + segs;
     k_coef<<<1184, 256, 0, stream>>>(b.entries, b.pos, n_amb, b.capacity);
-    k_walk<<<1, 32, 0, stream>>>(b.entries, n_amb, s0 & kLcgMask, b.extra_after, b.capacity);
+    marks.mark(5, stream);
+    k_walk<<<1, 32, sizeof(WalkSmem), stream>>>(b.entries, n_amb, s0 & kLcgMask, b.extra_after,
+                                                 b.capacity);
+    marks.mark(6, stream);
     k_startup_counts<<<1, 256, 0, stream>>>(meta, g.w, b.extra_after, s0 & kLcgMask, ctr,
                                             b.capacity);
     k_apply<<<(unsigned)segs, kSegThreads, 0, stream>>>(
@@ -585,6 +642,7 @@ cudaError_t launch_writer(const Geometry &g, const uint8_t *meta, const double *
         b.extra_after, s0 & kLcgMask, rgb_out, changed_out, ctr, err, b.capacity);
     k_final<<<1, 1, 0, stream>>>(b.seg_base, b.seg_amb, segs, b.extra_after, s0 & kLcgMask,
                                  ctr, err, b.capacity);
+    marks.mark(7, stream);
     return cudaGetLastError();
 }
 
@@ -602,6 +660,7 @@ void counters_to_host(const void *dev_copy, fx_counters *out) {
         out->startup_attempted[k] = (int64_t)c.su_attempted[k];
         out->startup_advances[k] = (int64_t)c.su_advances[k];
     }
+    out->rng_dependent = (int64_t)c.n_amb;
 }
 
 uint32_t counters_n_amb(const void *dev_copy) {

@@ -97,6 +97,7 @@ class FxCounters(ctypes.Structure):
         ("startup_final_state", ctypes.c_uint32),
         ("startup_attempted", ctypes.c_int64 * 6),
         ("startup_advances", ctypes.c_int64 * 6),
+        ("rng_dependent", ctypes.c_int64),
     ]
 
 
@@ -138,7 +139,11 @@ SIGNATURES = {
     "fx_mem_info": ([_P, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)],
                     ctypes.c_int),
     "fx_frame_bytes": ([ctypes.c_int32, ctypes.c_int32], ctypes.c_int64),
+    "fx_profile_enable": ([_P, ctypes.c_int], ctypes.c_int),
+    "fx_profile_read": ([_P, _P, ctypes.POINTER(ctypes.c_int64), ctypes.c_int], ctypes.c_int),
 }
+
+PROFILE_STAGES = ("producer", "planes", "stencil", "startup", "chain", "walk", "apply")
 
 _LIB = None
 _LIB_LOCK = threading.Lock()

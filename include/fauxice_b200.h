@@ -94,6 +94,8 @@ typedef struct fx_counters {
     uint32_t final_state, startup_final_state;
     int64_t startup_attempted[6];
     int64_t startup_advances[6];
+    int64_t rng_dependent; /* channels whose draw count depends on the state
+                              (walked serially; no reference counterpart) */
 } fx_counters;
 
 /* One frame for fx_process / fx_submit.  Host pointers. */
@@ -171,6 +173,18 @@ FX_API int fx_set_slots(fx_context *ctx, int32_t slots);
 FX_API int fx_submit(fx_context *ctx, const fx_frame *frame, int64_t *ticket);
 FX_API int fx_poll(fx_context *ctx, int64_t ticket);
 FX_API int fx_wait(fx_context *ctx, int64_t ticket, int64_t timeout_ns, fx_counters *counters);
+
+/* Device time per pipeline stage, from CUDA events recorded on the frame's
+ * stream between kernel groups (measurement only; no reference
+ * counterpart).  Stages: 0 producer, 1 auxiliary + history planes,
+ * 2 stencil, 3 hidden startup, 4 chain scan + copy intervals + jumps,
+ * 5 serial walk, 6 apply + emit + counters.  fx_profile_read waits for the
+ * context stream, adds the elapsed times of every profiled pass since the
+ * last reset into ms[FX_PROFILE_STAGES] and reports how many passes were
+ * profiled. */
+#define FX_PROFILE_STAGES 7
+FX_API int fx_profile_enable(fx_context *ctx, int enable);
+FX_API int fx_profile_read(fx_context *ctx, double *ms, int64_t *passes, int reset);
 
 /* Free / total device memory, for admission control. */
 FX_API int fx_mem_info(fx_context *ctx, size_t *free_bytes, size_t *total_bytes);
