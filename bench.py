@@ -380,6 +380,10 @@ def run_b200(args, world, rank, local):
             "clocks": clocks,
             "gpu_launches": 17 * args.steps,
             "rng_dependent_channels": int(counters.rng_dependent),
+            "walk_fallback_segments": int(counters.walk_fallbacks),
+            "walk_candidate_steps": int(counters.walk_candidate_steps),
+            "walk_candidates": int(counters.walk_candidates),
+            "walk_survivors": int(counters.walk_survivors),
         }
         print(json.dumps(line), flush=True)
 

@@ -49,8 +49,11 @@ struct Arena {
     uint8_t *changed = nullptr;
     void *counters = nullptr;
     uint32_t *err = nullptr;
+    void *walk = nullptr;
     int64_t amb_capacity = 0;
 };
+
+static int g_per_wave = 148;  // window blocks per wave: the SM count
 
 static size_t arena_layout(const Geometry &g, int64_t amb_cap, Arena *a) {
     size_t off = 0;
@@ -80,6 +83,7 @@ static size_t arena_layout(const Geometry &g, int64_t amb_cap, Arena *a) {
     const size_t o_chg = take(px);
     const size_t o_ctr = take(dev_counters_bytes());
     const size_t o_err = take(16);
+    const size_t o_walk = take(walk_scratch_bytes(amb_cap, g_per_wave));
     if (a) {
         char *b = reinterpret_cast<char *>(a->base);
         a->rgbi = (uint16_t *)(b + o_rgbi);
@@ -101,6 +105,7 @@ static size_t arena_layout(const Geometry &g, int64_t amb_cap, Arena *a) {
         a->changed = (uint8_t *)(b + o_chg);
         a->counters = (void *)(b + o_ctr);
         a->err = (uint32_t *)(b + o_err);
+        a->walk = (void *)(b + o_walk);
         a->amb_capacity = amb_cap;
     }
     return off;
@@ -132,6 +137,7 @@ struct Slot {
 struct fx_context {
     int device = 0;
     bool profile = false;
+    bool parallel_walk = true;
     std::vector<std::vector<cudaEvent_t>> pending;  // recorded, not yet read
     std::vector<std::vector<cudaEvent_t>> spare;
     double profile_ms[fx::kProfileStages] = {0};
@@ -251,7 +257,10 @@ static int enqueue_pass(fx_context *ctx, Slot &s, const Geometry &g, const fx_pa
     FX_CUDA(ctx, launch_analysis(d_in, g, ctx->lut, a.stages, p, a.aux, a.hs, a.hwa, a.hwr,
                                  (int64_t)g.prow * g.pitch, a.cand, a.meta, a.err, st, marks));
     WriterBuffers wb{a.seg_base, a.seg_amb, a.entries, a.pos, a.extra, a.counters,
-                     a.amb_capacity};
+                     a.amb_capacity,
+                     reinterpret_cast<uint32_t *>(reinterpret_cast<char *>(s.h_ctr) +
+                                                  dev_counters_bytes() + 32),
+                     a.walk, g_per_wave, ctx->parallel_walk};
     FX_CUDA(ctx, launch_writer(g, a.meta, a.cand, d_in, ctx->lut, ctx->high, ctx->low, a.stages,
                                p, rng, wb, d_out, d_changed, a.err, st, marks));
     return FX_OK;
@@ -300,7 +309,7 @@ static int ensure_slots(fx_context *ctx, int n) {
         Slot &s = ctx->slots.back();
         FX_CUDA(ctx, cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking));
         FX_CUDA(ctx, cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming));
-        FX_CUDA(ctx, cudaMallocHost(&s.h_ctr, dev_counters_bytes() + 64));
+        FX_CUDA(ctx, cudaMallocHost(&s.h_ctr, dev_counters_bytes() + 64));  // + err + count
     }
     return FX_OK;
 }
@@ -384,6 +393,10 @@ FX_API int fx_context_create(int device, fx_context **out) {
         delete ctx;
         return fail(nullptr, FX_ERR_CUDA, "cudaSetDevice failed");
     }
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess &&
+        sms > 0)
+        g_per_wave = sms;
     if (analysis_init() != cudaSuccess || ensure_slots(ctx, 1) != FX_OK ||
         cudaMalloc(&ctx->lut, 65536 * 4) != cudaSuccess ||
         cudaMalloc(&ctx->high, 256 * 4) != cudaSuccess ||
@@ -577,6 +590,13 @@ FX_API int fx_sync_counters(fx_context *ctx, fx_counters *counters) {
     const int rc = finish_counters(ctx, s, hc, err, counters, &overflow);
     if (rc) return rc;
     if (overflow) return fail(ctx, FX_ERR_INTERNAL, "amb capacity exceeded; rerun with counters");
+    return FX_OK;
+}
+
+FX_API int fx_set_parallel_walk(fx_context *ctx, int enable) {
+    if (!ctx) return FX_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    ctx->parallel_walk = enable != 0;
     return FX_OK;
 }
 

@@ -160,6 +160,10 @@ struct WriterBuffers {
     uint32_t *extra_after;         // capacity
     void *counters;                // DevCounters
     int64_t capacity;
+    uint32_t *h_n;                 // pinned host word for the channel count
+    void *walk_scratch;            // walk_scratch_bytes(capacity, per_wave)
+    int per_wave;                  // window blocks per wave (SM count)
+    bool parallel_walk;
 };
 
 // Optional CUDA events between kernel groups (measurement only).
@@ -184,6 +188,12 @@ cudaError_t launch_writer(const Geometry &g, const uint8_t *meta, const double *
                           uint8_t *changed_out, uint32_t *err, cudaStream_t stream,
                           const Marks &marks);
 size_t dev_counters_bytes();
+cudaError_t walk_init();
+size_t walk_scratch_bytes(int64_t capacity, int per_wave);
+cudaError_t launch_walk(const AmbEntry *entries, const uint32_t *pos, const uint32_t *n_ptr,
+                        int64_t capacity, uint32_t n, uint32_t s0, void *scratch, int per_wave,
+                        bool parallel, uint32_t *extra_after, uint32_t *fallbacks_out,
+                        unsigned long long *stats_out, cudaStream_t stream);
 void counters_to_host(const void *dev_copy, fx_counters *out);
 uint32_t counters_n_amb(const void *dev_copy);
 size_t producer_bytes(int h, int w);

@@ -1,0 +1,779 @@
+// fx_walk.cu -- the serial RNG walk, parallelised by speculation.
+//
+// The chain of RNG-dependent channels (see fx_writer.cu) is a function of
+// one integer: E_i, the number of extra draws before channel i.  The state
+// at channel i's first draw is T_i = G^(pos_i + 1 + E_i)(T0) (G = one LCG step
+// in T space), the channel draws an extra time iff T_i misses its copy
+// intervals, and E_{i+1} = E_i + extra_i.  So a segment of channels maps an
+// entry count E_in to an exit count E_out, and:
+//   * two candidates E < E' keep their order and merge for good once equal
+//     (E'_k - E_k moves by -1, 0 or +1 per channel), so merges only ever
+//     happen between neighbours in E order;
+//   * candidates merge quickly (the gap is a lazy random walk absorbed at 0).
+//
+// k_window walks one segment for a window of candidate E_in values around
+// the predicted value (expected extras from the exact state-space measure of
+// every copy set), merging candidates as they meet and compacting the
+// survivors, and writes a dense E_in -> E_out table.  k_resolve chains the
+// exact E through a wave of segments with one table read per segment; when
+// E falls outside a window it walks that segment exactly, so correctness
+// never depends on the prediction.  k_rewalk then walks every segment in
+// parallel from its exact E_in and writes the running extra count per
+// channel.  With one segment covering the whole chain, k_rewalk alone is the
+// plain serial walk.
+#include "fx_internal.cuh"
+
+namespace fx {
+
+constexpr int kWinThreads = 512;
+constexpr int kWinSlots = 16;                       // candidates per thread
+constexpr int kWinMax = kWinThreads * kWinSlots;    // 8192 candidates
+constexpr uint32_t kSegLen = 4096;                  // channels per walk segment
+constexpr int kWinChunk = 256;                      // channels staged per chunk
+constexpr uint32_t kNone = 0xFFFFFFFFu;
+constexpr uint32_t kSerialBelow = 4 * kSegLen;      // short chains: one serial walk
+
+struct WalkState {
+    uint32_t e_wave;     // exact E at the start of the current wave
+    uint32_t fallbacks;  // segments resolved by an exact serial walk
+    uint32_t waves;
+    uint32_t pad;
+    unsigned long long candidate_steps;  // window-walk work, for diagnostics
+    unsigned long long window_sum;       // candidates started
+    unsigned long long survivor_sum;     // candidates left at segment ends
+};
+
+struct SegWindow {
+    uint32_t lo, hi;  // candidate E_in range, inclusive
+};
+
+__device__ __forceinline__ uint32_t jump_t(uint32_t t0, uint64_t n) {
+    const Affine f = lcg_power_t(n);
+    return f.a * t0 + f.c;
+}
+
+__device__ __forceinline__ bool copies(const uint4 &lw, uint32_t T) {
+    return (T - lw.x) <= lw.y || (T - lw.z) <= lw.w;
+}
+
+__device__ __forceinline__ uint4 intervals(const AmbEntry &e) {
+    return make_uint4(e.l1, e.w1, e.l2, e.w2);
+}
+
+// Expected extras and their variance per segment, from the exact measure of
+// each copy set (a uniformly random first-draw state misses it with
+// probability p).
+__global__ void k_seg_prob(const AmbEntry *__restrict__ entries, const uint32_t *__restrict__ n_ptr,
+                           int64_t capacity, double *__restrict__ seg_mu,
+                           double *__restrict__ seg_var) {
+    __shared__ double s_mu[8], s_var[8];
+    const uint32_t n = (uint32_t)min((int64_t)*n_ptr, capacity);
+    const uint32_t i0 = blockIdx.x * kSegLen;
+    if (i0 >= n) return;
+    const uint32_t i1 = min(n, i0 + kSegLen);
+    double mu = 0.0, var = 0.0;
+    for (uint32_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+        const AmbEntry e = entries[i];
+        double measure = 0.0;
+        if (e.l1 != 0x80u) measure += (double)((e.w1 >> 8) + 1u);
+        if (e.l2 != 0x80u) measure += (double)((e.w2 >> 8) + 1u);
+        const double p = 1.0 - measure * (1.0 / 16777216.0);
+        mu += p;
+        var += p * (1.0 - p);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mu += __shfl_down_sync(0xFFFFFFFFu, mu, o);
+        var += __shfl_down_sync(0xFFFFFFFFu, var, o);
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+        s_mu[warp] = mu;
+        s_var[warp] = var;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0, b = 0.0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
+            a += s_mu[k];
+            b += s_var[k];
+        }
+        seg_mu[blockIdx.x] = a;
+        seg_var[blockIdx.x] = b;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Block scans over 1024 threads
+// ---------------------------------------------------------------------------
+
+// Exclusive "last valid value" scan in thread order (kNone = no value);
+// `total` receives the inclusive result of the whole block.
+__device__ __forceinline__ uint32_t last_valid_exclusive(uint32_t v, uint32_t *buf,
+                                                         uint32_t &total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        if (lane >= o && x == kNone) x = y;
+    }
+    constexpr int kWarps = kWinThreads / 32;
+    if (lane == 31) buf[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t s = lane < kWarps ? buf[lane] : kNone;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, s, o);
+            if (lane >= o && s == kNone) s = y;
+        }
+        if (lane < kWarps) buf[lane] = s;
+    }
+    __syncthreads();
+    uint32_t before = __shfl_up_sync(0xFFFFFFFFu, x, 1);
+    if (lane == 0) before = kNone;
+    if (before == kNone && warp > 0) before = buf[warp - 1];
+    total = buf[kWarps - 1];
+    __syncthreads();
+    return before;
+}
+
+__device__ __forceinline__ uint32_t add_exclusive(uint32_t v, uint32_t *buf, uint32_t &total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t x = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        if (lane >= o) x += y;
+    }
+    constexpr int kWarps = kWinThreads / 32;
+    if (lane == 31) buf[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t s = lane < kWarps ? buf[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, s, o);
+            if (lane >= o) s += y;
+        }
+        if (lane < kWarps) buf[lane] = s;
+    }
+    __syncthreads();
+    const uint32_t prefix = warp ? buf[warp - 1] : 0u;
+    total = buf[kWarps - 1];
+    __syncthreads();
+    return prefix + x - v;
+}
+
+// ---------------------------------------------------------------------------
+// Window walk
+// ---------------------------------------------------------------------------
+
+constexpr int kListMax = 256;  // survivors kept in the compact per-segment list
+
+// Compact result of one window: survivors in E_in order as 16-bit offsets
+// (E_in - lo, E_out - lo); count == 0xFFFF means "use the dense table".
+struct __align__(16) SegList {
+    uint32_t count;
+    uint32_t pad[3];
+    uint16_t ein[kListMax];
+    uint16_t eout[kListMax];
+};
+static_assert(sizeof(SegList) % 16 == 0, "SegList is staged with 16-byte copies");
+
+struct WindowSmem {
+    AmbEntry ring[2][kWinChunk + 1];
+    uint32_t ein[kWinMax], e[kWinMax], t[kWinMax];  // survivors in E_in order
+    uint32_t buf[32];
+    double pred[2];
+};
+static_assert(kWinSlots <= 32, "live mask is 32 bits");
+
+// One warp steps its live candidates over LEN staged channels.  The entries
+// do not depend on the candidates, so all LEN are loaded first and the
+// dependent chain per channel is compare -> select -> multiply-add.
+template <int SLOTS, int LEN>
+__device__ __forceinline__ void walk_group(const uint4 *r4, uint32_t r, bool tail_next,
+                                           uint32_t (&rE)[kWinSlots], uint32_t (&rT)[kWinSlots],
+                                           uint32_t live_mask, uint32_t &steps) {
+    uint4 lw[LEN], ac[LEN];
+#pragma unroll
+    for (int k = 0; k < LEN; ++k) {
+        lw[k] = r4[2 * (r + k)];
+        const bool next = (k + 1 < LEN) || tail_next;
+        ac[k] = r4[2 * (r + k + (next ? 1 : 0)) + 1];
+    }
+    steps += (uint32_t)__popc(live_mask & ((1u << SLOTS) - 1u)) * LEN;
+#pragma unroll
+    for (int k = 0; k < LEN; ++k) {
+#pragma unroll
+        for (int s = 0; s < SLOTS; ++s) {
+            if (live_mask & (1u << s)) {
+                const uint32_t x = copies(lw[k], rT[s]) ? 0u : 1u;
+                rE[s] += x;
+                rT[s] = x ? ac[k].z * rT[s] + ac[k].w : ac[k].x * rT[s] + ac[k].y;
+            }
+        }
+    }
+}
+
+// Single channels (segment and compaction boundaries).
+template <int SLOTS>
+__device__ __forceinline__ void walk_one(const uint4 *r4, uint32_t r, bool has_next,
+                                         uint32_t (&rE)[kWinSlots], uint32_t (&rT)[kWinSlots],
+                                         uint32_t live_mask, uint32_t &steps) {
+    const uint4 lw = r4[2 * r];
+    const uint4 ac = r4[2 * (r + (has_next ? 1u : 0u)) + 1];
+    steps += (uint32_t)__popc(live_mask & ((1u << SLOTS) - 1u));
+#pragma unroll
+    for (int s = 0; s < SLOTS; ++s) {
+        if (live_mask & (1u << s)) {
+            const uint32_t x = copies(lw, rT[s]) ? 0u : 1u;
+            rE[s] += x;
+            rT[s] = x ? ac.z * rT[s] + ac.w : ac.x * rT[s] + ac.y;
+        }
+    }
+}
+
+// Warp-local merge: lanes of one slot hold consecutive candidates.
+template <int SLOTS>
+__device__ __forceinline__ void warp_merge(const uint32_t (&rE)[kWinSlots], uint32_t &live_mask) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int s = 0; s < SLOTS; ++s) {
+        const bool alive = live_mask & (1u << s);
+        uint32_t x = alive ? rE[s] : kNone;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+            if (lane >= o && x == kNone) x = y;
+        }
+        uint32_t prev = __shfl_up_sync(0xFFFFFFFFu, x, 1);
+        if (lane == 0) prev = kNone;
+        if (alive && rE[s] == prev) live_mask &= ~(1u << s);
+    }
+}
+
+// Walk channels [r, stop) of the staged ring for one warp.
+template <int SLOTS>
+__device__ __forceinline__ void walk_span(const uint4 *r4, uint32_t r, uint32_t stop,
+                                          bool end_next, uint32_t merge_len,
+                                          uint32_t (&rE)[kWinSlots], uint32_t (&rT)[kWinSlots],
+                                          uint32_t &live_mask, uint32_t &steps) {
+    constexpr int kLen = 8;
+    uint32_t since = 0;
+    while (r < stop) {
+        if (r + kLen <= stop) {
+            const bool tail_next = (r + kLen < stop) || end_next;
+            walk_group<SLOTS, kLen>(r4, r, tail_next, rE, rT, live_mask, steps);
+            r += kLen;
+            since += kLen;
+        } else {
+            const bool has_next = (r + 1 < stop) || end_next;
+            walk_one<SLOTS>(r4, r, has_next, rE, rT, live_mask, steps);
+            r += 1;
+            since += 1;
+        }
+        if (since >= merge_len || r == stop) {
+            warp_merge<SLOTS>(rE, live_mask);
+            since = 0;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kWinThreads, 1)
+    k_window(const AmbEntry *__restrict__ entries, const uint32_t *__restrict__ pos,
+             const uint32_t *__restrict__ n_ptr, int64_t capacity,
+             const double *__restrict__ seg_mu, const double *__restrict__ seg_var,
+             const WalkState *__restrict__ st, uint32_t wave, uint32_t per_wave, uint32_t t0,
+             SegWindow *__restrict__ windows, uint32_t *__restrict__ table,
+             SegList *__restrict__ lists, WalkState *stats) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    WindowSmem &S = *reinterpret_cast<WindowSmem *>(smem_raw);
+    const uint32_t n = (uint32_t)min((int64_t)*n_ptr, capacity);
+    const uint32_t seg0 = wave * per_wave;
+    const uint32_t j = seg0 + blockIdx.x;
+    const uint32_t i0 = j * kSegLen;
+    if (i0 >= n) return;
+    const uint32_t i1 = min(n, i0 + kSegLen);
+    const uint32_t tid = threadIdx.x;
+
+    // window of candidate entry counts around the prediction
+    if (tid == 0) {
+        double mu = 0.0, var = 0.0;
+        for (uint32_t k = seg0; k < j; ++k) {
+            mu += seg_mu[k];
+            var += seg_var[k];
+        }
+        S.pred[0] = mu;
+        S.pred[1] = var;
+    }
+    __syncthreads();
+    const uint32_t e0 = st->e_wave;
+    const uint32_t before = i0 - seg0 * kSegLen;  // channels since the wave start
+    const double half = 6.0 * sqrt(S.pred[1]) + 16.0;
+    const double center = S.pred[0];
+    int64_t lo = (int64_t)floor(center - half), hi = (int64_t)ceil(center + half);
+    lo = lo < 0 ? 0 : lo;
+    hi = hi > (int64_t)before ? (int64_t)before : hi;
+    if (hi < lo) hi = lo;
+    if (hi - lo + 1 > kWinMax) {
+        lo = (int64_t)center - kWinMax / 2;
+        lo = lo < 0 ? 0 : lo;
+        hi = lo + kWinMax - 1;
+        if (hi > (int64_t)before) {
+            hi = before;
+            lo = hi - kWinMax + 1;
+        }
+    }
+    const uint32_t wlo = e0 + (uint32_t)lo;
+    const uint32_t count = (uint32_t)(hi - lo + 1);
+
+    // candidates in list order k = slot * kWinThreads + tid; E_in of the
+    // candidate at list position k is S.ein[k] (kept in shared memory)
+    uint32_t rE[kWinSlots], rT[kWinSlots];
+    uint32_t live_mask = 0;
+    uint32_t live = count;
+    {
+        uint32_t t = jump_t(t0, (uint64_t)pos[i0] + 1u + wlo + tid);
+        const Affine stride = lcg_power_t(kWinThreads);
+#pragma unroll
+        for (int s = 0; s < kWinSlots; ++s) {
+            const uint32_t k = s * kWinThreads + tid;
+            rE[s] = wlo + k;
+            rT[s] = t;
+            if (k < live) live_mask |= 1u << s;
+            S.ein[k] = wlo + k;
+            t = stride.a * t + stride.c;
+        }
+    }
+
+    auto stage = [&](uint32_t first, int b) {
+        const uint32_t avail = min((uint32_t)kWinChunk + 1u, n - first);
+        const uint4 *src = reinterpret_cast<const uint4 *>(entries + first);
+        uint4 *dst = reinterpret_cast<uint4 *>(S.ring[b]);
+        for (uint32_t v = tid; v < 2 * avail; v += kWinThreads) {
+            const uint32_t sa = (uint32_t)__cvta_generic_to_shared(dst + v);
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(src + v));
+        }
+        asm volatile("cp.async.commit_group;\n" ::);
+    };
+
+    // block-wide merge across warp and slot boundaries (list order is
+    // slot-major), then compaction of survivors to the front of the list
+    auto merge_and_compact = [&](int slots) {
+        uint32_t carry = kNone;
+#pragma unroll
+        for (int s = 0; s < kWinSlots; ++s) {
+            if (s < slots) {  // block-uniform
+                uint32_t total;
+                const bool alive = live_mask & (1u << s);
+                const uint32_t v = alive ? rE[s] : kNone;
+                uint32_t prev = last_valid_exclusive(v, S.buf, total);
+                if (prev == kNone) prev = carry;
+                if (alive && rE[s] == prev) live_mask &= ~(1u << s);
+                if (total != kNone) carry = total;
+            }
+        }
+        uint32_t base = 0;
+        uint32_t ein[kWinSlots];
+#pragma unroll
+        for (int s = 0; s < kWinSlots; ++s)
+            if (s < slots && (live_mask & (1u << s))) ein[s] = S.ein[s * kWinThreads + tid];
+        __syncthreads();
+#pragma unroll
+        for (int s = 0; s < kWinSlots; ++s) {
+            if (s < slots) {
+                uint32_t total;
+                const bool alive = live_mask & (1u << s);
+                const uint32_t at = base + add_exclusive(alive ? 1u : 0u, S.buf, total);
+                if (alive) {
+                    S.ein[at] = ein[s];
+                    S.e[at] = rE[s];
+                    S.t[at] = rT[s];
+                }
+                base += total;
+            }
+        }
+        __syncthreads();
+        live = base;
+        live_mask = 0;
+#pragma unroll
+        for (int s = 0; s < kWinSlots; ++s) {
+            const uint32_t k = s * kWinThreads + tid;
+            if (k < live) {
+                live_mask |= 1u << s;
+                rE[s] = S.e[k];
+                rT[s] = S.t[k];
+            }
+        }
+        __syncthreads();
+    };
+
+    uint32_t steps = 0;
+    stage(i0, 0);
+    int b = 0;
+    int slots = (int)((live + kWinThreads - 1) / kWinThreads);
+    uint32_t next_compact = 8;  // then 16, 32, ..., every chunk
+    for (uint32_t c0 = i0; c0 < i1; c0 += kWinChunk) {
+        const uint32_t c1 = min(i1, c0 + (uint32_t)kWinChunk);
+        if (c1 < i1) stage(c1, b ^ 1);
+        else asm volatile("cp.async.commit_group;\n" ::);
+        asm volatile("cp.async.wait_group 1;\n" ::);
+        __syncthreads();
+        const uint4 *r4 = reinterpret_cast<const uint4 *>(S.ring[b]);
+        uint32_t r = 0;
+        const uint32_t len = c1 - c0;
+        while (r < len) {
+            const uint32_t done0 = (c0 - i0) + r;
+            const uint32_t stop =
+                min(len, r + (next_compact > done0 ? next_compact - done0 : len));
+            const bool end_next = (c0 + stop) < i1;
+            const uint32_t merge_len = (done0 < 256u) ? 8u : 32u;
+            if (__any_sync(0xFFFFFFFFu, live_mask != 0)) {
+                switch (slots) {
+#define FX_WALK_CASE(K)                                                                         \
+    case K:                                                                                     \
+        walk_span<K>(r4, r, stop, end_next, merge_len, rE, rT, live_mask, steps);               \
+        break;
+                    FX_WALK_CASE(1) FX_WALK_CASE(2) FX_WALK_CASE(3) FX_WALK_CASE(4)
+                    FX_WALK_CASE(5) FX_WALK_CASE(6) FX_WALK_CASE(7) FX_WALK_CASE(8)
+                    FX_WALK_CASE(9) FX_WALK_CASE(10) FX_WALK_CASE(11) FX_WALK_CASE(12)
+                    FX_WALK_CASE(13) FX_WALK_CASE(14) FX_WALK_CASE(15)
+                default:
+                    walk_span<16>(r4, r, stop, end_next, merge_len, rE, rT, live_mask, steps);
+                    break;
+#undef FX_WALK_CASE
+                }
+            }
+            r = stop;
+            const uint32_t done = (c0 - i0) + r;
+            if (done >= next_compact || r == len) {
+                merge_and_compact(slots);
+                slots = (int)((live + kWinThreads - 1) / kWinThreads);
+                if (done >= next_compact)
+                    next_compact = min(2 * next_compact, done + (uint32_t)kWinChunk);
+            }
+        }
+        b ^= 1;
+    }
+    asm volatile("cp.async.wait_group 0;\n" ::);
+
+    // Outputs.  Survivors sit compacted in S.* in E_in order.
+    uint32_t *out = table + (size_t)blockIdx.x * kWinMax;
+    for (uint32_t k = tid; k < live; k += kWinThreads) {
+        const uint32_t from = S.ein[k] - wlo;
+        const uint32_t to = (k + 1 < live) ? S.ein[k + 1] - wlo : count;
+        const uint32_t value = S.e[k];
+        for (uint32_t m = from; m < to; ++m) out[m] = value;
+    }
+    SegList *list = lists + blockIdx.x;
+    if (live <= (uint32_t)kListMax) {
+        for (uint32_t k = tid; k < live; k += kWinThreads) {
+            list->ein[k] = (uint16_t)(S.ein[k] - wlo);
+            list->eout[k] = (uint16_t)(S.e[k] - wlo);
+        }
+    }
+    if (tid == 0) {
+        windows[blockIdx.x] = SegWindow{wlo, wlo + count - 1};
+        list->count = (live <= (uint32_t)kListMax) ? live : 0xFFFFu;
+        atomicAdd(&stats->window_sum, (unsigned long long)count);
+        atomicAdd(&stats->survivor_sum, (unsigned long long)live);
+    }
+    for (int o = 16; o > 0; o >>= 1) steps += __shfl_down_sync(0xFFFFFFFFu, steps, o);
+    if ((tid & 31) == 0 && steps) atomicAdd(&stats->candidate_steps, (unsigned long long)steps);
+}
+
+// Exact serial walk of one segment from a known entry count (the fallback).
+__device__ uint32_t walk_segment_exact(const AmbEntry *entries, const uint32_t *pos, uint32_t i0,
+                                       uint32_t i1, uint32_t e_in, uint32_t t0) {
+    uint32_t T = jump_t(t0, (uint64_t)pos[i0] + 1u + e_in);
+    uint32_t E = e_in;
+    for (uint32_t i = i0; i < i1; ++i) {
+        const uint32_t x = copies(intervals(entries[i]), T) ? 0u : 1u;
+        E += x;
+        if (i + 1 < i1) {
+            const AmbEntry nx = entries[i + 1];
+            T = x ? nx.a1 * T + nx.c1 : nx.a0 * T + nx.c0;
+        }
+    }
+    return E;
+}
+
+// Resolve one wave: chain the exact E through its segments.  The compact
+// survivor lists of the whole wave are staged into shared memory first, so
+// each hop is a short binary search there; a segment whose list overflowed
+// uses its dense table, and E outside a window walks the segment exactly.
+constexpr int kResolveSegs = 160;  // lists held in shared memory
+
+__global__ void __launch_bounds__(1024)
+    k_resolve(const AmbEntry *__restrict__ entries, const uint32_t *__restrict__ pos,
+              const uint32_t *__restrict__ n_ptr, int64_t capacity, WalkState *st,
+              uint32_t wave, uint32_t per_wave, uint32_t t0,
+              const SegWindow *__restrict__ windows, const uint32_t *__restrict__ table,
+              const SegList *__restrict__ lists, uint32_t *__restrict__ e_in_exact) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SegList *s_list = reinterpret_cast<SegList *>(smem_raw);
+    SegWindow *s_win = reinterpret_cast<SegWindow *>(s_list + kResolveSegs);
+    const uint32_t n = (uint32_t)min((int64_t)*n_ptr, capacity);
+    const uint32_t segs = (n + kSegLen - 1) / kSegLen;
+    const uint32_t here = min(per_wave, segs > wave * per_wave ? segs - wave * per_wave : 0u);
+    const uint32_t staged = min(here, (uint32_t)kResolveSegs);
+    {
+        const uint4 *src = reinterpret_cast<const uint4 *>(lists);
+        uint4 *dst = reinterpret_cast<uint4 *>(s_list);
+        const uint32_t vecs = staged * (uint32_t)(sizeof(SegList) / 16);
+        for (uint32_t v = threadIdx.x; v < vecs; v += blockDim.x) {
+            const uint32_t sa = (uint32_t)__cvta_generic_to_shared(dst + v);
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(src + v));
+        }
+        asm volatile("cp.async.commit_group;\n" ::);
+        for (uint32_t b = threadIdx.x; b < staged; b += blockDim.x) s_win[b] = windows[b];
+        asm volatile("cp.async.wait_group 0;\n" ::);
+    }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    uint32_t E = st->e_wave;
+    for (uint32_t b = 0; b < here; ++b) {
+        const uint32_t j = wave * per_wave + b;
+        e_in_exact[j] = E;
+        const bool in_smem = b < staged;
+        const SegWindow win = in_smem ? s_win[b] : windows[b];
+        if (E >= win.lo && E <= win.hi) {
+            const SegList *L = in_smem ? &s_list[b] : &lists[b];
+            const uint32_t cnt = L->count;
+            if (cnt != 0xFFFFu && cnt > 0) {
+                // last survivor with ein <= E - lo
+                const uint32_t q = E - win.lo;
+                uint32_t a = 0, z = cnt;  // invariant: ein[a] <= q, answer in [a, z)
+                while (z - a > 1) {
+                    const uint32_t mid = (a + z) >> 1;
+                    if ((uint32_t)L->ein[mid] <= q) a = mid;
+                    else z = mid;
+                }
+                E = win.lo + L->eout[a];
+            } else {
+                E = table[(size_t)b * kWinMax + (E - win.lo)];
+            }
+        } else {
+            const uint32_t i0 = j * kSegLen, i1 = min(n, i0 + kSegLen);
+            E = walk_segment_exact(entries, pos, i0, i1, E, t0);
+            st->fallbacks += 1;
+        }
+    }
+    st->e_wave = E;
+    st->waves += 1;
+}
+
+// ---------------------------------------------------------------------------
+// Per-channel running counts: one warp per segment; lane 0 walks from the
+// exact entry count while the warp stages the entries with cp.async.
+// ---------------------------------------------------------------------------
+
+constexpr int kRewalkWarps = 4;
+constexpr int kRewalkChunk = 256;
+constexpr int kRewalkRing = 3;
+constexpr int kGroup = 8;
+
+struct RewalkSmem {
+    AmbEntry ring[kRewalkWarps][kRewalkRing][kRewalkChunk];
+    uint32_t out[kRewalkWarps][kRewalkRing][kRewalkChunk];
+};
+
+__device__ __forceinline__ void step(const uint4 &lw, const uint4 &ac, uint32_t &T, uint32_t &extra,
+                                     uint32_t &E) {
+    const uint32_t u0 = ac.x * T + ac.y;
+    const uint32_t u1 = ac.z * T + ac.w;
+    T = extra ? u1 : u0;
+    extra = copies(lw, T) ? 0u : 1u;
+    E += extra;
+}
+
+__global__ void __launch_bounds__(kRewalkWarps * 32)
+    k_rewalk(const AmbEntry *__restrict__ entries, const uint32_t *__restrict__ pos,
+             const uint32_t *__restrict__ n_ptr, int64_t capacity, uint32_t seg_len,
+             const uint32_t *__restrict__ e_in_exact, uint32_t t0,
+             uint32_t *__restrict__ extra_after) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    RewalkSmem &S = *reinterpret_cast<RewalkSmem *>(smem_raw);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t n = (uint32_t)min((int64_t)*n_ptr, capacity);
+    const uint32_t j = blockIdx.x * kRewalkWarps + warp;
+    const uint64_t i0_64 = (uint64_t)j * seg_len;
+    if (i0_64 >= n) return;
+    const uint32_t i0 = (uint32_t)i0_64;
+    const uint32_t i1 = (uint32_t)min((uint64_t)n, i0_64 + seg_len);
+    const uint32_t chunks = (i1 - i0 + kRewalkChunk - 1) / kRewalkChunk;
+    AmbEntry(*ring)[kRewalkChunk] = S.ring[warp];
+    uint32_t(*out)[kRewalkChunk] = S.out[warp];
+    auto issue = [&](uint32_t k) {
+        if (k < chunks) {
+            const uint32_t first = i0 + k * kRewalkChunk;
+            const uint32_t count = min((uint32_t)kRewalkChunk, i1 - first);
+            const uint4 *src = reinterpret_cast<const uint4 *>(entries + first);
+            uint4 *dst = reinterpret_cast<uint4 *>(ring[k % kRewalkRing]);
+            for (uint32_t v = lane; v < 2 * count; v += 32) {
+                const uint32_t s = (uint32_t)__cvta_generic_to_shared(dst + v);
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(src + v));
+            }
+        }
+        asm volatile("cp.async.commit_group;\n" ::);
+    };
+#pragma unroll
+    for (int k = 0; k < kRewalkRing - 1; ++k) issue(k);
+    const uint32_t e_in = e_in_exact[j];
+    uint32_t T = jump_t(t0, (uint64_t)pos[i0] + 1u + e_in);  // state at channel i0's first draw
+    uint32_t E = e_in;
+    uint32_t extra = 0u;
+    for (uint32_t k = 0; k < chunks; ++k) {
+        issue(k + kRewalkRing - 1);
+        asm volatile("cp.async.wait_group %0;\n" ::"n"(kRewalkRing - 1));
+        __syncwarp();
+        const uint32_t first = i0 + k * kRewalkChunk;
+        const uint32_t count = min((uint32_t)kRewalkChunk, i1 - first);
+        if (lane == 0) {
+            const uint4 *__restrict__ e4 = reinterpret_cast<const uint4 *>(ring[k % kRewalkRing]);
+            uint32_t *__restrict__ o = out[k % kRewalkRing];
+            uint32_t i = 0;
+            if (k == 0) {
+                // the first channel needs no transition: its state is the jump
+                extra = copies(e4[0], T) ? 0u : 1u;
+                E += extra;
+                o[0] = E;
+                i = 1;
+            }
+            const uint32_t groups = (count - i) / kGroup;
+            uint4 lw[kGroup], ac[kGroup];
+            if (groups) {
+#pragma unroll
+                for (int q = 0; q < kGroup; ++q) {
+                    lw[q] = e4[2 * (i + q)];
+                    ac[q] = e4[2 * (i + q) + 1];
+                }
+            }
+            for (uint32_t g = 0; g < groups; ++g) {
+                const uint32_t base = i + g * kGroup;
+                const uint32_t next = (g + 1 < groups) ? base + kGroup : base;
+                uint4 nlw[kGroup], nac[kGroup];
+#pragma unroll
+                for (int q = 0; q < kGroup; ++q) {
+                    nlw[q] = e4[2 * (next + q)];
+                    nac[q] = e4[2 * (next + q) + 1];
+                }
+                uint32_t res[kGroup];
+#pragma unroll
+                for (int q = 0; q < kGroup; ++q) {
+                    step(lw[q], ac[q], T, extra, E);
+                    res[q] = E;
+                }
+#pragma unroll
+                for (int q = 0; q < kGroup; ++q) {
+                    o[base + q] = res[q];
+                    lw[q] = nlw[q];
+                    ac[q] = nac[q];
+                }
+            }
+            for (uint32_t r = i + groups * kGroup; r < count; ++r) {
+                step(e4[2 * r], e4[2 * r + 1], T, extra, E);
+                o[r] = E;
+            }
+        }
+        __syncwarp();
+        const uint32_t *o = out[k % kRewalkRing];
+        for (uint32_t r = lane; r < count; r += 32) extra_after[first + r] = o[r];
+        __syncwarp();
+    }
+    asm volatile("cp.async.wait_group 0;\n" ::);
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+
+int64_t walk_max_segments(int64_t capacity) { return (capacity + kSegLen - 1) / kSegLen + 1; }
+
+size_t walk_scratch_bytes(int64_t capacity, int per_wave) {
+    const int64_t segs = walk_max_segments(capacity);
+    size_t b = 0;
+    auto add = [&](size_t n) { b += (n + 255) & ~(size_t)255; };
+    add(segs * sizeof(double));  // mu
+    add(segs * sizeof(double));  // var
+    add(segs * sizeof(uint32_t));  // exact E_in
+    add((size_t)per_wave * sizeof(SegWindow));
+    add((size_t)per_wave * kWinMax * sizeof(uint32_t));
+    add((size_t)per_wave * sizeof(SegList));
+    add(sizeof(WalkState));
+    return b;
+}
+
+static size_t resolve_smem_bytes() {
+    return kResolveSegs * (sizeof(SegList) + sizeof(SegWindow));
+}
+
+cudaError_t walk_init() {
+    cudaError_t e = cudaFuncSetAttribute(k_window, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)sizeof(WindowSmem));
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_resolve, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)resolve_smem_bytes());
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_rewalk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(RewalkSmem));
+}
+
+// Enqueue the walk for `n` RNG-dependent channels (n already known on the
+// host).  `parallel` selects the speculative window walk; otherwise one warp
+// walks the whole chain.
+cudaError_t launch_walk(const AmbEntry *entries, const uint32_t *pos, const uint32_t *n_ptr,
+                        int64_t capacity, uint32_t n, uint32_t s0, void *scratch, int per_wave,
+                        bool parallel, uint32_t *extra_after, uint32_t *fallbacks_out,
+                        unsigned long long *stats_out, cudaStream_t stream) {
+    if (n == 0) return cudaGetLastError();
+    const int64_t segs_max = walk_max_segments(capacity);
+    char *p = reinterpret_cast<char *>(scratch);
+    auto take = [&](size_t bytes) {
+        void *r = p;
+        p += (bytes + 255) & ~(size_t)255;
+        return r;
+    };
+    double *mu = (double *)take(segs_max * sizeof(double));
+    double *var = (double *)take(segs_max * sizeof(double));
+    uint32_t *e_in = (uint32_t *)take(segs_max * sizeof(uint32_t));
+    SegWindow *windows = (SegWindow *)take((size_t)per_wave * sizeof(SegWindow));
+    uint32_t *table = (uint32_t *)take((size_t)per_wave * kWinMax * sizeof(uint32_t));
+    SegList *lists = (SegList *)take((size_t)per_wave * sizeof(SegList));
+    WalkState *st = (WalkState *)take(sizeof(WalkState));
+    const uint32_t t0 = (s0 & kLcgMask) << 8;
+    cudaMemsetAsync(st, 0, sizeof(WalkState), stream);
+    if (!parallel || n < kSerialBelow) {
+        cudaMemsetAsync(e_in, 0, sizeof(uint32_t), stream);
+        k_rewalk<<<1, kRewalkWarps * 32, sizeof(RewalkSmem), stream>>>(
+            entries, pos, n_ptr, capacity, n, e_in, t0, extra_after);
+    } else {
+        const uint32_t segs = (n + kSegLen - 1) / kSegLen;
+        const uint32_t waves = (segs + per_wave - 1) / per_wave;
+        k_seg_prob<<<segs, 256, 0, stream>>>(entries, n_ptr, capacity, mu, var);
+        for (uint32_t w = 0; w < waves; ++w) {
+            const uint32_t blocks = min((uint32_t)per_wave, segs - w * per_wave);
+            k_window<<<blocks, kWinThreads, sizeof(WindowSmem), stream>>>(
+                entries, pos, n_ptr, capacity, mu, var, st, w, per_wave, t0, windows, table,
+                lists, st);
+            k_resolve<<<1, 1024, resolve_smem_bytes(), stream>>>(entries, pos, n_ptr, capacity, st,
+                                                               w, per_wave, t0, windows, table,
+                                                               lists, e_in);
+        }
+        k_rewalk<<<(segs + kRewalkWarps - 1) / kRewalkWarps, kRewalkWarps * 32,
+                   sizeof(RewalkSmem), stream>>>(entries, pos, n_ptr, capacity, kSegLen, e_in, t0,
+                                                 extra_after);
+    }
+    if (fallbacks_out)
+        cudaMemcpyAsync(fallbacks_out, &st->fallbacks, sizeof(uint32_t), cudaMemcpyDeviceToDevice,
+                        stream);
+    if (stats_out)
+        cudaMemcpyAsync(stats_out, &st->candidate_steps, 3 * sizeof(unsigned long long),
+                        cudaMemcpyDeviceToDevice, stream);
+    return cudaGetLastError();
+}
+
+}  // namespace fx

@@ -16,11 +16,14 @@
 //      binary search on the exact binary64 expressions, which are monotone
 //      in the state).
 //   4. k_coef: the affine LCG jump g^gap between consecutive such channels.
-//   5. k_walk: ONE thread walks only the RNG-dependent channels: a jump, an
-//      interval test, a select.  Output: the running count of extra draws.
+//   5. the walk (fx_walk.cu) visits only the RNG-dependent channels: a jump,
+//      an interval test, a select per channel, parallelised over segments by
+//      speculation.  Output: the running count of extra draws.
 //   6. k_apply: every public site recomputes its exact draws and values from
 //      its own start state g^(fixed + extra before it)(s0), in parallel, and
 //      emits public RGB16 with the counters.
+#include <algorithm>
+
 #include "fx_internal.cuh"
 
 namespace fx {
@@ -32,6 +35,8 @@ struct DevCounters {
     uint32_t final_state, su_final_state;
     uint32_t startup_base, startup_amb, startup_extra;
     uint32_t n_amb;
+    uint32_t walk_fallbacks;
+    unsigned long long walk_stats[3];  // candidate steps, window sum, survivor sum
 };
 
 // ---------------------------------------------------------------------------
@@ -328,125 +333,6 @@ __global__ void k_coef(AmbEntry *__restrict__ entries, const uint32_t *__restric
 // The serial walk (one resident warp per frame; lane 0 walks)
 // ---------------------------------------------------------------------------
 
-constexpr int kWalkChunk = 512;  // entries per staged chunk (16 KB)
-constexpr int kWalkRing = 4;
-constexpr int kWalkGroup = 8;    // steps per register batch
-
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
-    const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-    asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
-}
-
-struct WalkSmem {
-    AmbEntry ring[kWalkRing][kWalkChunk];
-    uint32_t out[kWalkRing][kWalkChunk];
-};
-
-// One walk step.  The select on the previous step's outcome is the only
-// serial dependency besides the multiply: both candidate states are formed
-// while the previous interval test resolves.
-__device__ __forceinline__ void walk_step(const uint4 &lw, const uint4 &ac, uint32_t &T,
-                                          uint32_t &extra, uint32_t &total) {
-    const uint32_t u0 = ac.x * T + ac.y;
-    const uint32_t u1 = ac.z * T + ac.w;
-    T = extra ? u1 : u0;
-    const bool hit = (T - lw.x) <= lw.y || (T - lw.z) <= lw.w;
-    extra = hit ? 0u : 1u;
-    total += extra;
-}
-
-__global__ void __launch_bounds__(32)
-    k_walk(const AmbEntry *__restrict__ entries, const uint32_t *__restrict__ n_amb_ptr,
-           uint32_t s0, uint32_t *__restrict__ extra_after, int64_t capacity) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    WalkSmem &S = *reinterpret_cast<WalkSmem *>(smem_raw);
-    const int lane = threadIdx.x;
-    const uint32_t n = (uint32_t)min((int64_t)*n_amb_ptr, capacity);
-    const uint32_t chunks = (n + kWalkChunk - 1) / kWalkChunk;
-    constexpr int kVec = kWalkChunk * (int)sizeof(AmbEntry) / 16;
-
-    auto issue = [&](uint32_t k) {
-        if (k < chunks) {
-            const uint32_t first = k * kWalkChunk;
-            const uint32_t count = min((uint32_t)kWalkChunk, n - first);
-            const int vecs = (int)(count * sizeof(AmbEntry) / 16);
-            const char *src = reinterpret_cast<const char *>(entries + first);
-            char *dst = reinterpret_cast<char *>(S.ring[k % kWalkRing]);
-            for (int v = lane; v < vecs && v < kVec; v += 32) cp_async16(dst + 16 * v, src + 16 * v);
-        }
-        cp_async_commit();
-    };
-#pragma unroll
-    for (int k = 0; k < kWalkRing - 1; ++k) issue(k);
-
-    uint32_t T = s0 << 8;
-    uint32_t extra = 0u;  // whether the previous channel drew twice
-    uint32_t total = 0u;
-    for (uint32_t k = 0; k < chunks; ++k) {
-        issue(k + kWalkRing - 1);
-        cp_async_wait<kWalkRing - 1>();
-        __syncwarp();
-        const uint32_t count = min((uint32_t)kWalkChunk, n - k * kWalkChunk);
-        if (lane == 0) {
-            const uint4 *__restrict__ e4 = reinterpret_cast<const uint4 *>(S.ring[k % kWalkRing]);
-            uint32_t *__restrict__ o = S.out[k % kWalkRing];
-            const uint32_t groups = count / kWalkGroup;
-            uint4 lw[kWalkGroup], ac[kWalkGroup];
-            if (groups) {
-#pragma unroll
-                for (int j = 0; j < kWalkGroup; ++j) {
-                    lw[j] = e4[2 * j];
-                    ac[j] = e4[2 * j + 1];
-                }
-            }
-            for (uint32_t g = 0; g < groups; ++g) {
-                uint4 nlw[kWalkGroup], nac[kWalkGroup];
-                const uint32_t next = (g + 1 < groups) ? (g + 1) * kWalkGroup : g * kWalkGroup;
-#pragma unroll
-                for (int j = 0; j < kWalkGroup; ++j) {
-                    nlw[j] = e4[2 * (next + j)];
-                    nac[j] = e4[2 * (next + j) + 1];
-                }
-                uint32_t tot[kWalkGroup];
-#pragma unroll
-                for (int j = 0; j < kWalkGroup; ++j) {
-                    walk_step(lw[j], ac[j], T, extra, total);
-                    tot[j] = total;
-                }
-                uint4 *o4 = reinterpret_cast<uint4 *>(o + g * kWalkGroup);
-                o4[0] = make_uint4(tot[0], tot[1], tot[2], tot[3]);
-                o4[1] = make_uint4(tot[4], tot[5], tot[6], tot[7]);
-#pragma unroll
-                for (int j = 0; j < kWalkGroup; ++j) {
-                    lw[j] = nlw[j];
-                    ac[j] = nac[j];
-                }
-            }
-            for (uint32_t i = groups * kWalkGroup; i < count; ++i) {
-                walk_step(e4[2 * i], e4[2 * i + 1], T, extra, total);
-                o[i] = total;
-            }
-        }
-        __syncwarp();
-        const uint32_t *o = S.out[k % kWalkRing];
-        for (uint32_t i = lane; i < count; i += 32) extra_after[k * kWalkChunk + i] = o[i];
-        __syncwarp();
-    }
-    cp_async_wait<0>();
-}
-
-size_t walk_smem_bytes() { return sizeof(WalkSmem); }
-
-cudaError_t writer_init() {
-    return cudaFuncSetAttribute(k_walk, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)sizeof(WalkSmem));
-}
-
 // ---------------------------------------------------------------------------
 // Startup counters, apply + emit, final state
 // ---------------------------------------------------------------------------
@@ -632,8 +518,15 @@ cudaError_t launch_writer(const Geometry &g, const uint8_t *meta, const double *
     const uint32_t *n_amb = b.seg_amb + segs;
     k_coef<<<1184, 256, 0, stream>>>(b.entries, b.pos, n_amb, b.capacity);
     marks.mark(5, stream);
-    k_walk<<<1, 32, sizeof(WalkSmem), stream>>>(b.entries, n_amb, s0 & kLcgMask, b.extra_after,
-                                                 b.capacity);
+    // The walk's launch shape depends on the channel count: read it back.
+    cudaMemcpyAsync(b.h_n, n_amb, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream);
+    cudaError_t e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return e;
+    const uint32_t n = (uint32_t)std::min<int64_t>((int64_t)*b.h_n, b.capacity);
+    e = launch_walk(b.entries, b.pos, n_amb, b.capacity, n, s0, b.walk_scratch, b.per_wave,
+                    b.parallel_walk, b.extra_after, &ctr->walk_fallbacks, ctr->walk_stats,
+                    stream);
+    if (e != cudaSuccess) return e;
     marks.mark(6, stream);
     k_startup_counts<<<1, 256, 0, stream>>>(meta, g.w, b.extra_after, s0 & kLcgMask, ctr,
                                             b.capacity);
@@ -661,6 +554,10 @@ void counters_to_host(const void *dev_copy, fx_counters *out) {
         out->startup_advances[k] = (int64_t)c.su_advances[k];
     }
     out->rng_dependent = (int64_t)c.n_amb;
+    out->walk_fallbacks = (int64_t)c.walk_fallbacks;
+    out->walk_candidate_steps = (int64_t)c.walk_stats[0];
+    out->walk_candidates = (int64_t)c.walk_stats[1];
+    out->walk_survivors = (int64_t)c.walk_stats[2];
 }
 
 uint32_t counters_n_amb(const void *dev_copy) {

@@ -98,6 +98,10 @@ class FxCounters(ctypes.Structure):
         ("startup_attempted", ctypes.c_int64 * 6),
         ("startup_advances", ctypes.c_int64 * 6),
         ("rng_dependent", ctypes.c_int64),
+        ("walk_fallbacks", ctypes.c_int64),
+        ("walk_candidate_steps", ctypes.c_int64),
+        ("walk_candidates", ctypes.c_int64),
+        ("walk_survivors", ctypes.c_int64),
     ]
 
 
@@ -133,6 +137,7 @@ SIGNATURES = {
                           ctypes.c_int),
     "fx_sync_counters": ([_P, ctypes.POINTER(FxCounters)], ctypes.c_int),
     "fx_set_slots": ([_P, ctypes.c_int32], ctypes.c_int),
+    "fx_set_parallel_walk": ([_P, ctypes.c_int], ctypes.c_int),
     "fx_submit": ([_P, ctypes.POINTER(FxFrame), ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
     "fx_poll": ([_P, ctypes.c_int64], ctypes.c_int),
     "fx_wait": ([_P, ctypes.c_int64, ctypes.c_int64, ctypes.POINTER(FxCounters)], ctypes.c_int),

@@ -94,8 +94,10 @@ typedef struct fx_counters {
     uint32_t final_state, startup_final_state;
     int64_t startup_attempted[6];
     int64_t startup_advances[6];
-    int64_t rng_dependent; /* channels whose draw count depends on the state
-                              (walked serially; no reference counterpart) */
+    int64_t rng_dependent;  /* channels whose draw count depends on the state
+                               (no reference counterpart) */
+    int64_t walk_fallbacks; /* walk segments resolved by the exact serial path */
+    int64_t walk_candidate_steps, walk_candidates, walk_survivors; /* walk work */
 } fx_counters;
 
 /* One frame for fx_process / fx_submit.  Host pointers. */
@@ -170,6 +172,9 @@ FX_API int fx_sync_counters(fx_context *ctx, fx_counters *counters);
  * the reference processes one job per call).  Up to `slots` frames run
  * concurrently, each on its own stream with its own device buffers. */
 FX_API int fx_set_slots(fx_context *ctx, int32_t slots);
+/* 1 (default): the speculative parallel walk; 0: one warp walks the whole
+ * chain (leaves the rest of the GPU to other frames' kernels). */
+FX_API int fx_set_parallel_walk(fx_context *ctx, int enable);
 FX_API int fx_submit(fx_context *ctx, const fx_frame *frame, int64_t *ticket);
 FX_API int fx_poll(fx_context *ctx, int64_t ticket);
 FX_API int fx_wait(fx_context *ctx, int64_t ticket, int64_t timeout_ns, fx_counters *counters);
