@@ -18,7 +18,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "fauxice_b200", "libfauxice_b200.so")
 BUILD = os.path.join(HERE, "_build")
-SOURCES = ("fx_analysis.cu", "fx_writer.cu", "fx_walk.cu", "fx_prelude.cu", "fx_api.cu")
+SOURCES = ("fx_analysis.cu", "fx_writer.cu", "fx_walk.cu", "fx_prelude.cu", "fx_api.cu",
+           "fx_static.cu")
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -288,6 +288,21 @@ static int error_from_device(fx_context *ctx, uint32_t code) {
     }
 }
 
+// Context accessors for entry points defined in other files.
+int context_device(const fx_context *ctx) { return ctx->device; }
+
+const float *context_lut(const fx_context *ctx) { return ctx->tables ? ctx->lut : nullptr; }
+
+int context_fail(fx_context *ctx, int code, const char *fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(ctx->error, sizeof(ctx->error), fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+int context_device_error(fx_context *ctx, uint32_t code) { return error_from_device(ctx, code); }
+
 // Counters + error word of the slot, after the stream completed.
 static int finish_counters(fx_context *ctx, Slot &s, const void *ctr_copy, uint32_t err,
                            fx_counters *out, bool *overflow) {

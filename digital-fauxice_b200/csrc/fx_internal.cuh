@@ -205,4 +205,10 @@ int host_reduce_prepass(const uint16_t *px, int h, int w, const float *lut, uint
 int host_stage_table(int h, const float *p1, const float *p2, const float *mv, const float *mi,
                      float factor_b, fx_stage *stages);
 
+// fx_api.cu: context accessors for entry points defined in other files
+int context_device(const fx_context *ctx);
+const float *context_lut(const fx_context *ctx);
+int context_fail(fx_context *ctx, int code, const char *fmt, ...);
+int context_device_error(fx_context *ctx, uint32_t code);
+
 }  // namespace fx

@@ -130,6 +130,8 @@ SIGNATURES = {
     "fx_set_tables": ([_P, _P, _P, _P], ctypes.c_int),
     "fx_reduce_prepass": ([_P, ctypes.c_int32, ctypes.c_int32, _P, _P, _P, _P], ctypes.c_int),
     "fx_producer_rows": ([_P, _P, ctypes.c_int32, ctypes.c_int32, _P, _P, _P, _P], ctypes.c_int),
+    "fx_producer_rows_static": ([_P, _P, ctypes.c_int32, ctypes.c_int32, _P, _P, _P],
+                                ctypes.c_int),
     "fx_stage_table": ([ctypes.c_int32, _P, _P, _P, _P, ctypes.c_float, _P], ctypes.c_int),
     "fx_process": ([_P, ctypes.POINTER(FxFrame), ctypes.POINTER(FxCounters)], ctypes.c_int),
     "fx_process_device": ([_P, _P, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(FxParams), _P,

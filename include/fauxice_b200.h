@@ -145,6 +145,23 @@ FX_API int fx_producer_rows(fx_context *ctx, const uint16_t *main_rgbi, int32_t 
                             int32_t width, float *scaled_input, float *input_scale,
                             float *mean_visible, float *mean_infrared);
 
+/* No counterpart in the reference.  fx_producer_rows plus the stage table
+ * (fx_stage_table with auxiliary_factor_b 1) for a frame already in device
+ * memory, for callers that cannot allocate device memory when they need it
+ * (a service whose HBM is claimed by its own pool; acquisition loops that
+ * cannot afford the device-wide synchronization of a cudaFree).  The call
+ * makes no device allocation: its scratch is a fixed 24 MiB device array per
+ * device (frames up to a full 5782x3946 scan); larger frames return
+ * FX_ERR_INVALID_ARGUMENT with the sizes in fx_last_error.  d_rows receives
+ * 4*height floats (scaled_input, input_scale, mean_visible, mean_infrared,
+ * one row after another), d_stages height+6 records.  Work is enqueued on
+ * `stream` (a cudaStream_t, NULL for the legacy default stream) and the call
+ * returns after it finishes.  The scratch is shared by all calls on one
+ * device, so calls are serialized; the first call on a device reserves the
+ * array and should come before any stream capture. */
+FX_API int fx_producer_rows_static(fx_context *ctx, const uint16_t *d_main_rgbi, int32_t height,
+                                   int32_t width, float *d_rows, fx_stage *d_stages, void *stream);
+
 /* producer_parameters.py:498-541 with stage_parameters.py:93-197: the stage
  * table (H+6 entries) built from per-row producer fields; host computation. */
 FX_API int fx_stage_table(int32_t height, const float *scaled_input, const float *input_scale,
