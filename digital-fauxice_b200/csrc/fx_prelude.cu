@@ -163,70 +163,84 @@ __global__ void k_producer_cells(const uint16_t *__restrict__ rgbi, int h, int w
 }
 
 // ---------------------------------------------------------------------------
-// Per-row sums in strict column order, one row per lane.  A warp owns 32
-// rows; 32x32-pixel tiles stream through a cp.async ring in shared memory so
-// each lane reads its own row without uncoalesced global loads.
+// Per-row sums in strict column order.  Only the three binary64 additions
+// per pixel are sequential; the products (IR weight times the response of
+// the visible and infrared samples) are independent.  So a block owns 32
+// rows: seven producer warps compute the products of a 32 x 64 tile into
+// shared memory (zero where the cell's IR test failed first: adding +0.0
+// leaves a non-negative sum unchanged), while warp 0 adds the previous tile,
+// one row per lane, in column order.
 // ---------------------------------------------------------------------------
 
-constexpr int kRowStages = 6;
+constexpr int kRowTile = 64;          // columns per tile
+constexpr int kRowWarps = 8;          // warp 0 adds, warps 1..7 produce
+constexpr int kRowPitch = kRowTile + 1;
 
-__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
-    const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
-}
+struct RowSmem {
+    double p[2][3][32][kRowPitch];  // [buffer][visible, infrared, weight][row][column]
+};
 
-__global__ void __launch_bounds__(32)
+__global__ void __launch_bounds__(kRowWarps * 32)
     k_producer_rows(const uint16_t *__restrict__ rgbi, int h, int w, int active_width, int cells,
                     const float *__restrict__ lut, ProducerBuffers b) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    uint2(*tile)[32][33] = reinterpret_cast<uint2(*)[32][33]>(smem_raw);
-    const int lane = threadIdx.x;
+    RowSmem &S = *reinterpret_cast<RowSmem *>(smem_raw);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int r0 = blockIdx.x * 32;
-    const int row = r0 + lane;
-    const int tiles = (active_width + 31) / 32;
-    auto issue = [&](int t) {
-        if (t < tiles) {
-            const int col = t * 32 + lane;
-            if (col < active_width) {
-                for (int k = 0; k < 32; ++k) {
-                    const int rr = r0 + k;
-                    if (rr < h)
-                        cp_async8(&tile[t % kRowStages][k][lane],
-                                  rgbi + ((int64_t)rr * w + col) * 4);
-                }
-            }
-        }
-        asm volatile("cp.async.commit_group;\n" ::);
-    };
-#pragma unroll
-    for (int t = 0; t < kRowStages - 1; ++t) issue(t);
+    const int tiles = (active_width + kRowTile - 1) / kRowTile;
+    constexpr int kProducers = (kRowWarps - 1) * 32;
     double rv = 0.0, ri = 0.0, rw = 0.0;
-    const int blk = row >> 3, local_row = row & 7;
-    for (int t = 0; t < tiles; ++t) {
-        issue(t + kRowStages - 1);
-        asm volatile("cp.async.wait_group %0;\n" ::"n"(kRowStages - 1));
-        __syncwarp();
-        if (row < h) {
-            const uint2 *tr = tile[t % kRowStages][lane];
-            const int col0 = t * 32;
-            const int n = min(32, active_width - col0);
-            for (int j = 0; j < n; ++j) {
-                const int col = col0 + j;
-                const int fp = b.failpos[(int64_t)blk * cells + (col >> 3)];
-                if (local_row * 8 + (col & 7) < fp) {
-                    const uint2 px = tr[j];
-                    const uint32_t vis = px.x & 0xFFFFu, irv = px.y >> 16;
-                    const double weight = (double)((uint64_t)irv * irv);
-                    rv += weight * (double)__ldg(lut + vis);
-                    ri += weight * (double)__ldg(lut + irv);
-                    rw += weight;
+    for (int t = 0; t <= tiles; ++t) {
+        if (warp > 0 && t < tiles) {
+            const int q0 = threadIdx.x - 32;
+            const int col0 = t * kRowTile;
+#pragma unroll 4
+            for (int q = q0; q < 32 * kRowTile; q += kProducers) {
+                const int k = q / kRowTile, j = q % kRowTile;
+                const int row = r0 + k, col = col0 + j;
+                double pv = 0.0, pi = 0.0, pw = 0.0;
+                if (row < h && col < active_width) {
+                    const int fp = b.failpos[(int64_t)(row >> 3) * cells + (col >> 3)];
+                    if ((row & 7) * 8 + (col & 7) < fp) {
+                        const uint2 px =
+                            __ldg(reinterpret_cast<const uint2 *>(rgbi + ((int64_t)row * w + col) * 4));
+                        const uint32_t vis = px.x & 0xFFFFu, irv = px.y >> 16;
+                        const double weight = (double)((uint64_t)irv * irv);
+                        pv = weight * (double)__ldg(lut + vis);
+                        pi = weight * (double)__ldg(lut + irv);
+                        pw = weight;
+                    }
+                }
+                S.p[t & 1][0][k][j] = pv;
+                S.p[t & 1][1][k][j] = pi;
+                S.p[t & 1][2][k][j] = pw;
+            }
+        }
+        if (warp == 0 && t > 0) {
+            const int u = t - 1;
+            const int n = min(kRowTile, active_width - u * kRowTile);
+            const double *pv = S.p[u & 1][0][lane];
+            const double *pi = S.p[u & 1][1][lane];
+            const double *pw = S.p[u & 1][2][lane];
+            if (n == kRowTile) {
+#pragma unroll 16
+                for (int j = 0; j < kRowTile; ++j) {
+                    rv += pv[j];
+                    ri += pi[j];
+                    rw += pw[j];
+                }
+            } else {
+                for (int j = 0; j < n; ++j) {
+                    rv += pv[j];
+                    ri += pi[j];
+                    rw += pw[j];
                 }
             }
         }
-        __syncwarp();
+        __syncthreads();
     }
-    asm volatile("cp.async.wait_group 0;\n" ::);
-    if (row < h) {
+    const int row = r0 + lane;
+    if (warp == 0 && row < h) {
         b.row_sums[row] = rv;
         b.row_sums[h + row] = ri;
         b.row_sums[2 * h + row] = rw;
@@ -268,49 +282,77 @@ __global__ void __launch_bounds__(32)
     }
 }
 
-// Cumulative row sums (3 binary64 chains) and the epoch p1/p2 chain.
-__global__ void __launch_bounds__(32)
-    k_producer_scan(int h, int ne, ProducerBuffers b) {
-    const int lane = threadIdx.x;
-    double tv = 0.0, ti = 0.0, tw = 0.0;
-    for (int r0 = 0; r0 < h; r0 += 32) {
-        const int r = r0 + lane;
-        const double v = (r < h) ? b.row_sums[r] : 0.0;
-        const double i = (r < h) ? b.row_sums[h + r] : 0.0;
-        const double wv = (r < h) ? b.row_sums[2 * h + r] : 0.0;
-        double mv = 0.0, mi = 0.0, mw = 0.0;
-        const int n = min(32, h - r0);
-        for (int j = 0; j < n; ++j) {
-            tv += __shfl_sync(0xFFFFFFFFu, v, j);
-            ti += __shfl_sync(0xFFFFFFFFu, i, j);
-            tw += __shfl_sync(0xFFFFFFFFu, wv, j);
-            if (lane == j) {
-                mv = tv;
-                mi = ti;
-                mw = tw;
+// Cumulative row sums (3 binary64 chains) and the epoch p1/p2 chain.  Warp
+// 1 walks the epoch chain on its own.  The other warps stream the row sums
+// through shared memory in chunks (synchronising on a named barrier that
+// warp 1 does not take part in), and threads 0..2 each walk one chain.
+constexpr int kScanChunk = 1024;
+constexpr int kScanThreads = 256;
+constexpr int kScanLoaders = kScanThreads - 32;
+
+struct ScanSmem {
+    double v[2][3][kScanChunk];
+};
+
+__device__ __forceinline__ void scan_barrier() {
+    asm volatile("bar.sync 1, %0;\n" ::"n"(kScanLoaders) : "memory");
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_producer_scan(int h, int ne, ProducerBuffers b) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    ScanSmem &S = *reinterpret_cast<ScanSmem *>(smem_raw);
+    const int tid = threadIdx.x;
+    if (tid >= 32 && tid < 64) {
+        if (tid == 32) {
+            float den = 0.0f, num = 0.0f, p1 = kInitialScale, p2 = kInitialScale;
+            for (int e = 0; e < ne; ++e) {
+                const double dw = (double)den + (double)b.add[e];
+                const double nw = (double)num + (double)b.add[ne + e];
+                den = (float)dw;
+                num = (float)nw;
+                if (dw != 0.0) {
+                    const double ratio = nw / dw;
+                    p2 = (float)ratio;
+                    p1 = (float)((double)kScaleMultiplier * ratio);
+                }
+                b.p_epoch[e] = p1;
+                b.p_epoch[ne + e] = p2;
             }
         }
-        if (r < h) {
-            b.cum[r] = mv;
-            b.cum[h + r] = mi;
-            b.cum[2 * h + r] = mw;
-        }
+        return;
     }
-    if (lane == 0) {
-        float den = 0.0f, num = 0.0f, p1 = kInitialScale, p2 = kInitialScale;
-        for (int e = 0; e < ne; ++e) {
-            const double dw = (double)den + (double)b.add[e];
-            const double nw = (double)num + (double)b.add[ne + e];
-            den = (float)dw;
-            num = (float)nw;
-            if (dw != 0.0) {
-                const double ratio = nw / dw;
-                p2 = (float)ratio;
-                p1 = (float)((double)kScaleMultiplier * ratio);
-            }
-            b.p_epoch[e] = p1;
-            b.p_epoch[ne + e] = p2;
+    const int lt = tid < 32 ? tid : tid - 32;  // loader index, 0..kScanLoaders-1
+    const int chunks = (h + kScanChunk - 1) / kScanChunk;
+    auto load = [&](int c) {
+        const int base = c * kScanChunk, n = min(kScanChunk, h - base);
+        for (int i = lt; i < 3 * kScanChunk; i += kScanLoaders) {
+            const int chain = i / kScanChunk, k = i % kScanChunk;
+            if (k < n) S.v[c & 1][chain][k] = b.row_sums[(int64_t)chain * h + base + k];
         }
+    };
+    double acc = 0.0;
+    if (chunks > 0) load(0);
+    scan_barrier();
+    for (int c = 0; c < chunks; ++c) {
+        if (c + 1 < chunks) load(c + 1);
+        if (tid < 3) {
+            const int base = c * kScanChunk, n = min(kScanChunk, h - base);
+            const double *src = S.v[c & 1][tid];
+            double *dst = b.cum + (int64_t)tid * h + base;
+            if (n == kScanChunk) {
+#pragma unroll 8
+                for (int k = 0; k < kScanChunk; ++k) {
+                    acc += src[k];
+                    dst[k] = acc;
+                }
+            } else {
+                for (int k = 0; k < n; ++k) {
+                    acc += src[k];
+                    dst[k] = acc;
+                }
+            }
+        }
+        scan_barrier();
     }
 }
 
@@ -358,8 +400,11 @@ __global__ void k_stage_table(int h, int ne, float factor_b, ProducerBuffers b, 
 }
 
 cudaError_t producer_init() {
-    return cudaFuncSetAttribute(k_producer_rows, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)((size_t)kRowStages * 32 * 33 * sizeof(uint2)));
+    const cudaError_t e = cudaFuncSetAttribute(
+        k_producer_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(RowSmem));
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_producer_scan, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)sizeof(ScanSmem));
 }
 
 size_t producer_bytes(int h, int w) {
@@ -398,12 +443,10 @@ cudaError_t launch_producer(const uint16_t *rgbi, int h, int w, const float *lut
         const int64_t n = (int64_t)nb * cells;
         k_producer_cells<<<(unsigned)((n + 127) / 128), 128, 0, stream>>>(rgbi, h, w, cells, lut, b);
     }
-    {
-        const size_t smem = (size_t)kRowStages * 32 * 33 * sizeof(uint2);
-        k_producer_rows<<<(h + 31) / 32, 32, smem, stream>>>(rgbi, h, w, aw, cells, lut, b);
-    }
+    k_producer_rows<<<(h + 31) / 32, kRowWarps * 32, sizeof(RowSmem), stream>>>(rgbi, h, w, aw,
+                                                                               cells, lut, b);
     if (ne > 0) k_producer_epochs<<<ne, 32, 0, stream>>>(cells, ne, b);
-    k_producer_scan<<<1, 32, 0, stream>>>(h, ne, b);
+    k_producer_scan<<<1, kScanThreads, sizeof(ScanSmem), stream>>>(h, ne, b);
     k_stage_table<<<(h + 6 + 255) / 256, 256, 0, stream>>>(h, ne, 1.0f, b, stages, rows_out, err);
     return cudaGetLastError();
 }
