@@ -30,6 +30,8 @@ constexpr int kWinSlots = 16;                       // candidates per thread
 constexpr int kWinMax = kWinThreads * kWinSlots;    // 8192 candidates
 constexpr uint32_t kSegLen = 4096;                  // channels per walk segment
 constexpr int kWinChunk = 256;                      // channels staged per chunk
+constexpr int kWinRing = 3;                         // staged chunks in flight
+constexpr uint32_t kCompactEvery = 512;             // block compaction period (steady state)
 constexpr uint32_t kNone = 0xFFFFFFFFu;
 constexpr uint32_t kSerialBelow = 4 * kSegLen;      // short chains: one serial walk
 
@@ -53,7 +55,7 @@ __device__ __forceinline__ uint32_t jump_t(uint32_t t0, uint64_t n) {
 }
 
 __device__ __forceinline__ bool copies(const uint4 &lw, uint32_t T) {
-    return (T - lw.x) <= lw.y || (T - lw.z) <= lw.w;
+    return ((T - lw.x) <= lw.y) | ((T - lw.z) <= lw.w);
 }
 
 __device__ __forceinline__ uint4 intervals(const AmbEntry &e) {
@@ -183,16 +185,22 @@ struct __align__(16) SegList {
 static_assert(sizeof(SegList) % 16 == 0, "SegList is staged with 16-byte copies");
 
 struct WindowSmem {
-    AmbEntry ring[2][kWinChunk + 1];
+    AmbEntry ring[kWinRing][kWinChunk + 1];
     uint32_t ein[kWinMax], e[kWinMax], t[kWinMax];  // survivors in E_in order
     uint32_t buf[32];
+    uint32_t wlast[kWinSlots * (kWinThreads / 32)];   // per warp-slot, list order
+    uint32_t wcount[kWinSlots * (kWinThreads / 32)];
     double pred[2];
 };
+static_assert(kWinSlots * (kWinThreads / 32) <= 256, "prefix covers 8 entries per lane");
 static_assert(kWinSlots <= 32, "live mask is 32 bits");
 
-// One warp steps its live candidates over LEN staged channels.  The entries
-// do not depend on the candidates, so all LEN are loaded first and the
-// dependent chain per channel is compare -> select -> multiply-add.
+// One warp steps its candidates over LEN staged channels.  The entries do
+// not depend on the candidates, so all LEN are loaded first and the
+// dependent chain per channel is compare -> select -> multiply-add.  Dead
+// candidates (merged into a neighbour) keep stepping: their values are
+// never read again, and skipping them would put a divergent branch on every
+// step.
 template <int SLOTS, int LEN>
 __device__ __forceinline__ void walk_group(const uint4 *r4, uint32_t r, bool tail_next,
                                            uint32_t (&rE)[kWinSlots], uint32_t (&rT)[kWinSlots],
@@ -209,11 +217,9 @@ __device__ __forceinline__ void walk_group(const uint4 *r4, uint32_t r, bool tai
     for (int k = 0; k < LEN; ++k) {
 #pragma unroll
         for (int s = 0; s < SLOTS; ++s) {
-            if (live_mask & (1u << s)) {
-                const uint32_t x = copies(lw[k], rT[s]) ? 0u : 1u;
-                rE[s] += x;
-                rT[s] = x ? ac[k].z * rT[s] + ac[k].w : ac[k].x * rT[s] + ac[k].y;
-            }
+            const uint32_t x = copies(lw[k], rT[s]) ? 0u : 1u;
+            rE[s] += x;
+            rT[s] = x ? ac[k].z * rT[s] + ac[k].w : ac[k].x * rT[s] + ac[k].y;
         }
     }
 }
@@ -228,11 +234,9 @@ __device__ __forceinline__ void walk_one(const uint4 *r4, uint32_t r, bool has_n
     steps += (uint32_t)__popc(live_mask & ((1u << SLOTS) - 1u));
 #pragma unroll
     for (int s = 0; s < SLOTS; ++s) {
-        if (live_mask & (1u << s)) {
-            const uint32_t x = copies(lw, rT[s]) ? 0u : 1u;
-            rE[s] += x;
-            rT[s] = x ? ac.z * rT[s] + ac.w : ac.x * rT[s] + ac.y;
-        }
+        const uint32_t x = copies(lw, rT[s]) ? 0u : 1u;
+        rE[s] += x;
+        rT[s] = x ? ac.z * rT[s] + ac.w : ac.x * rT[s] + ac.y;
     }
 }
 
@@ -261,7 +265,8 @@ __device__ __forceinline__ void walk_span(const uint4 *r4, uint32_t r, uint32_t 
                                           bool end_next, uint32_t merge_len,
                                           uint32_t (&rE)[kWinSlots], uint32_t (&rT)[kWinSlots],
                                           uint32_t &live_mask, uint32_t &steps) {
-    constexpr int kLen = 8;
+    // many slots give their own parallelism: stage fewer channels at once
+    constexpr int kLen = SLOTS <= 2 ? 8 : (SLOTS <= 8 ? 4 : 2);
     uint32_t since = 0;
     while (r < stop) {
         if (r + kLen <= stop) {
@@ -360,44 +365,86 @@ __global__ void __launch_bounds__(kWinThreads, 1)
         asm volatile("cp.async.commit_group;\n" ::);
     };
 
-    // block-wide merge across warp and slot boundaries (list order is
-    // slot-major), then compaction of survivors to the front of the list
+    // Block-wide merge and compaction.  List order is slot-major
+    // (k = slot * kWinThreads + tid) and E is non-decreasing along it; after
+    // warp_merge the live values of one warp-slot are strictly increasing, so
+    // only its first live lane can equal the last live value before it.
     auto merge_and_compact = [&](int slots) {
-        uint32_t carry = kNone;
+        const int lane = tid & 31, warp = tid >> 5;
+        constexpr int kW = kWinThreads / 32;
+        uint32_t ein[kWinSlots];
+        // 1. last live value of every warp-slot
 #pragma unroll
         for (int s = 0; s < kWinSlots; ++s) {
             if (s < slots) {  // block-uniform
-                uint32_t total;
                 const bool alive = live_mask & (1u << s);
-                const uint32_t v = alive ? rE[s] : kNone;
-                uint32_t prev = last_valid_exclusive(v, S.buf, total);
-                if (prev == kNone) prev = carry;
-                if (alive && rE[s] == prev) live_mask &= ~(1u << s);
-                if (total != kNone) carry = total;
+                const uint32_t bal = __ballot_sync(0xFFFFFFFFu, alive);
+                const uint32_t last = bal ? __shfl_sync(0xFFFFFFFFu, rE[s], 31 - __clz(bal)) : kNone;
+                if (lane == 0) S.wlast[s * kW + warp] = last;
+                if (alive) ein[s] = S.ein[s * kWinThreads + tid];
             }
         }
-        uint32_t base = 0;
-        uint32_t ein[kWinSlots];
-#pragma unroll
-        for (int s = 0; s < kWinSlots; ++s)
-            if (s < slots && (live_mask & (1u << s))) ein[s] = S.ein[s * kWinThreads + tid];
         __syncthreads();
+        // 2. drop a first live lane that repeats the previous warp-slots' last
+        //    value; publish the live counts
 #pragma unroll
         for (int s = 0; s < kWinSlots; ++s) {
             if (s < slots) {
-                uint32_t total;
                 const bool alive = live_mask & (1u << s);
-                const uint32_t at = base + add_exclusive(alive ? 1u : 0u, S.buf, total);
+                const uint32_t bal = __ballot_sync(0xFFFFFFFFu, alive);
+                if (bal && lane == __ffs(bal) - 1) {
+                    uint32_t prev = kNone;
+                    for (int q = s * kW + warp - 1; q >= 0; --q) {
+                        const uint32_t v = S.wlast[q];
+                        if (v != kNone) {
+                            prev = v;
+                            break;
+                        }
+                    }
+                    if (prev == rE[s]) live_mask &= ~(1u << s);
+                }
+                const uint32_t cnt = __popc(__ballot_sync(0xFFFFFFFFu, live_mask & (1u << s)));
+                if (lane == 0) S.wcount[s * kW + warp] = cnt;
+            }
+        }
+        __syncthreads();
+        // 3. exclusive prefix of the counts in list order (every warp computes
+        //    it; lane l covers entries 8l..8l+7), then scatter
+        const int entries = slots * kW;
+        uint32_t lsum = 0;
+#pragma unroll
+        for (int m = 0; m < 8; ++m) {
+            const int q = lane * 8 + m;
+            lsum += (q < entries) ? S.wcount[q] : 0u;
+        }
+        uint32_t incl = lsum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const uint32_t excl = incl - lsum;
+        const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+#pragma unroll
+        for (int s = 0; s < kWinSlots; ++s) {
+            if (s < slots) {
+                const int q = s * kW + warp;
+                uint32_t base = __shfl_sync(0xFFFFFFFFu, excl, q >> 3);
+#pragma unroll
+                for (int m = 0; m < 7; ++m)
+                    if (m < (q & 7)) base += S.wcount[(q & ~7) + m];
+                const bool alive = live_mask & (1u << s);
+                const uint32_t bal = __ballot_sync(0xFFFFFFFFu, alive);
                 if (alive) {
+                    const uint32_t at = base + __popc(bal & ((1u << lane) - 1u));
                     S.ein[at] = ein[s];
                     S.e[at] = rE[s];
                     S.t[at] = rT[s];
                 }
-                base += total;
             }
         }
         __syncthreads();
-        live = base;
+        live = total;
         live_mask = 0;
 #pragma unroll
         for (int s = 0; s < kWinSlots; ++s) {
@@ -408,20 +455,24 @@ __global__ void __launch_bounds__(kWinThreads, 1)
                 rT[s] = S.t[k];
             }
         }
-        __syncthreads();
     };
 
     uint32_t steps = 0;
+    // Three staged chunks: chunk c+2 is fetched into the buffer of chunk c-1
+    // right after the barrier that ends every warp's work on chunk c-1.
     stage(i0, 0);
+    if (i0 + kWinChunk < i1) stage(i0 + kWinChunk, 1);
+    else asm volatile("cp.async.commit_group;\n" ::);
     int b = 0;
     int slots = (int)((live + kWinThreads - 1) / kWinThreads);
-    uint32_t next_compact = 8;  // then 16, 32, ..., every chunk
+    uint32_t next_compact = 8;  // then 16, 32, ..., every kCompactEvery channels
     for (uint32_t c0 = i0; c0 < i1; c0 += kWinChunk) {
         const uint32_t c1 = min(i1, c0 + (uint32_t)kWinChunk);
-        if (c1 < i1) stage(c1, b ^ 1);
-        else asm volatile("cp.async.commit_group;\n" ::);
         asm volatile("cp.async.wait_group 1;\n" ::);
         __syncthreads();
+        const uint32_t c2 = c0 + 2 * kWinChunk;
+        if (c2 < i1) stage(c2, (b + 2) % kWinRing);
+        else asm volatile("cp.async.commit_group;\n" ::);
         const uint4 *r4 = reinterpret_cast<const uint4 *>(S.ring[b]);
         uint32_t r = 0;
         const uint32_t len = c1 - c0;
@@ -449,14 +500,13 @@ __global__ void __launch_bounds__(kWinThreads, 1)
             }
             r = stop;
             const uint32_t done = (c0 - i0) + r;
-            if (done >= next_compact || r == len) {
+            if (done >= next_compact || c0 + r == i1) {
                 merge_and_compact(slots);
                 slots = (int)((live + kWinThreads - 1) / kWinThreads);
-                if (done >= next_compact)
-                    next_compact = min(2 * next_compact, done + (uint32_t)kWinChunk);
+                next_compact = min(2 * next_compact, done + kCompactEvery);
             }
         }
-        b ^= 1;
+        b = (b + 1) % kWinRing;
     }
     asm volatile("cp.async.wait_group 0;\n" ::);
 
