@@ -53,7 +53,7 @@ struct Arena {
     int64_t amb_capacity = 0;
 };
 
-static int g_per_wave = 148;  // window blocks per wave: the SM count
+static int g_per_wave = 296;  // window blocks per wave: walk_per_wave(SM count)
 
 static size_t arena_layout(const Geometry &g, int64_t amb_cap, Arena *a) {
     size_t off = 0;
@@ -411,7 +411,7 @@ FX_API int fx_context_create(int device, fx_context **out) {
     int sms = 0;
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess &&
         sms > 0)
-        g_per_wave = sms;
+        g_per_wave = walk_per_wave(sms);
     if (analysis_init() != cudaSuccess || ensure_slots(ctx, 1) != FX_OK ||
         cudaMalloc(&ctx->lut, 65536 * 4) != cudaSuccess ||
         cudaMalloc(&ctx->high, 256 * 4) != cudaSuccess ||

@@ -162,7 +162,7 @@ struct WriterBuffers {
     int64_t capacity;
     uint32_t *h_n;                 // pinned host word for the channel count
     void *walk_scratch;            // walk_scratch_bytes(capacity, per_wave)
-    int per_wave;                  // window blocks per wave (SM count)
+    int per_wave;                  // window blocks per wave (walk_per_wave of the SM count)
     bool parallel_walk;
 };
 
@@ -190,6 +190,7 @@ cudaError_t launch_writer(const Geometry &g, const uint8_t *meta, const double *
 size_t dev_counters_bytes();
 cudaError_t walk_init();
 size_t walk_scratch_bytes(int64_t capacity, int per_wave);
+int walk_per_wave(int sms);
 cudaError_t launch_walk(const AmbEntry *entries, const uint32_t *pos, const uint32_t *n_ptr,
                         int64_t capacity, uint32_t n, uint32_t s0, void *scratch, int per_wave,
                         bool parallel, uint32_t *extra_after, uint32_t *fallbacks_out,

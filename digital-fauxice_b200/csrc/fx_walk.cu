@@ -25,9 +25,10 @@
 
 namespace fx {
 
-constexpr int kWinThreads = 512;
+constexpr int kWinThreads = 256;
+constexpr int kWinBlocksPerSM = 2;                  // two segments resident per SM
 constexpr int kWinSlots = 16;                       // candidates per thread
-constexpr int kWinMax = kWinThreads * kWinSlots;    // 8192 candidates
+constexpr int kWinMax = kWinThreads * kWinSlots;    // 4096 candidates
 constexpr uint32_t kSegLen = 4096;                  // channels per walk segment
 constexpr int kWinChunk = 256;                      // channels staged per chunk
 constexpr int kWinRing = 3;                         // staged chunks in flight
@@ -287,7 +288,7 @@ __device__ __forceinline__ void walk_span(const uint4 *r4, uint32_t r, uint32_t 
     }
 }
 
-__global__ void __launch_bounds__(kWinThreads, 1)
+__global__ void __launch_bounds__(kWinThreads, kWinBlocksPerSM)
     k_window(const AmbEntry *__restrict__ entries, const uint32_t *__restrict__ pos,
              const uint32_t *__restrict__ n_ptr, int64_t capacity,
              const double *__restrict__ seg_mu, const double *__restrict__ seg_var,
@@ -305,14 +306,21 @@ __global__ void __launch_bounds__(kWinThreads, 1)
     const uint32_t tid = threadIdx.x;
 
     // window of candidate entry counts around the prediction
-    if (tid == 0) {
+    if (tid < 32) {  // the prediction only centres the window: any summation order
         double mu = 0.0, var = 0.0;
-        for (uint32_t k = seg0; k < j; ++k) {
+        for (uint32_t k = seg0 + tid; k < j; k += 32) {
             mu += seg_mu[k];
             var += seg_var[k];
         }
-        S.pred[0] = mu;
-        S.pred[1] = var;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            mu += __shfl_down_sync(0xFFFFFFFFu, mu, o);
+            var += __shfl_down_sync(0xFFFFFFFFu, var, o);
+        }
+        if (tid == 0) {
+            S.pred[0] = mu;
+            S.pred[1] = var;
+        }
     }
     __syncthreads();
     const uint32_t e0 = st->e_wave;
@@ -552,68 +560,93 @@ __device__ uint32_t walk_segment_exact(const AmbEntry *entries, const uint32_t *
 }
 
 // Resolve one wave: chain the exact E through its segments.  The compact
-// survivor lists of the whole wave are staged into shared memory first, so
-// each hop is a short binary search there; a segment whose list overflowed
-// uses its dense table, and E outside a window walks the segment exactly.
-constexpr int kResolveSegs = 160;  // lists held in shared memory
+// survivor lists stream through shared memory in chunks (warps 1.. stage
+// chunk c+1 while warp 0 chains chunk c), so each hop is a ballot count in
+// shared memory; a segment whose list overflowed uses its dense table, and
+// E outside a window walks the segment exactly.
+constexpr int kResolveChunk = 96;  // lists per staged chunk
+constexpr int kResolveThreads = 512;
 
-__global__ void __launch_bounds__(1024)
+struct ResolveSmem {
+    SegList list[2][kResolveChunk];
+    SegWindow win[2][kResolveChunk];
+};
+
+__global__ void __launch_bounds__(kResolveThreads)
     k_resolve(const AmbEntry *__restrict__ entries, const uint32_t *__restrict__ pos,
               const uint32_t *__restrict__ n_ptr, int64_t capacity, WalkState *st,
               uint32_t wave, uint32_t per_wave, uint32_t t0,
               const SegWindow *__restrict__ windows, const uint32_t *__restrict__ table,
               const SegList *__restrict__ lists, uint32_t *__restrict__ e_in_exact) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    SegList *s_list = reinterpret_cast<SegList *>(smem_raw);
-    SegWindow *s_win = reinterpret_cast<SegWindow *>(s_list + kResolveSegs);
+    ResolveSmem &S = *reinterpret_cast<ResolveSmem *>(smem_raw);
     const uint32_t n = (uint32_t)min((int64_t)*n_ptr, capacity);
     const uint32_t segs = (n + kSegLen - 1) / kSegLen;
     const uint32_t here = min(per_wave, segs > wave * per_wave ? segs - wave * per_wave : 0u);
-    const uint32_t staged = min(here, (uint32_t)kResolveSegs);
-    {
-        const uint4 *src = reinterpret_cast<const uint4 *>(lists);
-        uint4 *dst = reinterpret_cast<uint4 *>(s_list);
-        const uint32_t vecs = staged * (uint32_t)(sizeof(SegList) / 16);
-        for (uint32_t v = threadIdx.x; v < vecs; v += blockDim.x) {
+    const uint32_t chunks = (here + kResolveChunk - 1) / kResolveChunk;
+    const int tid = threadIdx.x, lane = tid & 31;
+    auto stage = [&](uint32_t c) {
+        const uint32_t first = c * kResolveChunk;
+        const uint32_t cnt = min((uint32_t)kResolveChunk, here - first);
+        const uint4 *src = reinterpret_cast<const uint4 *>(lists + first);
+        uint4 *dst = reinterpret_cast<uint4 *>(S.list[c & 1]);
+        const uint32_t vecs = cnt * (uint32_t)(sizeof(SegList) / 16);
+        for (uint32_t v = tid - 32; v < vecs; v += kResolveThreads - 32) {
             const uint32_t sa = (uint32_t)__cvta_generic_to_shared(dst + v);
             asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(src + v));
         }
         asm volatile("cp.async.commit_group;\n" ::);
-        for (uint32_t b = threadIdx.x; b < staged; b += blockDim.x) s_win[b] = windows[b];
-        asm volatile("cp.async.wait_group 0;\n" ::);
-    }
-    __syncthreads();
-    if (threadIdx.x != 0) return;
+        for (uint32_t b = tid - 32; b < cnt; b += kResolveThreads - 32)
+            S.win[c & 1][b] = windows[first + b];
+    };
+    if (tid >= 32 && chunks > 0) stage(0);
     uint32_t E = st->e_wave;
-    for (uint32_t b = 0; b < here; ++b) {
-        const uint32_t j = wave * per_wave + b;
-        e_in_exact[j] = E;
-        const bool in_smem = b < staged;
-        const SegWindow win = in_smem ? s_win[b] : windows[b];
-        if (E >= win.lo && E <= win.hi) {
-            const SegList *L = in_smem ? &s_list[b] : &lists[b];
-            const uint32_t cnt = L->count;
-            if (cnt != 0xFFFFu && cnt > 0) {
-                // last survivor with ein <= E - lo
-                const uint32_t q = E - win.lo;
-                uint32_t a = 0, z = cnt;  // invariant: ein[a] <= q, answer in [a, z)
-                while (z - a > 1) {
-                    const uint32_t mid = (a + z) >> 1;
-                    if ((uint32_t)L->ein[mid] <= q) a = mid;
-                    else z = mid;
+    uint32_t fallbacks = 0;
+    for (uint32_t c = 0; c < chunks; ++c) {
+        if (tid >= 32) asm volatile("cp.async.wait_group 0;\n" ::);
+        __syncthreads();  // chunk c visible; warp 0 is done with chunk c-1
+        if (tid >= 32) {
+            if (c + 1 < chunks) stage(c + 1);
+            continue;
+        }
+        // warp 0: one hop per segment; survivor E_in values are increasing
+        // and the first is the window's lowest candidate
+        const uint32_t first = c * kResolveChunk;
+        const uint32_t cnt_c = min((uint32_t)kResolveChunk, here - first);
+        for (uint32_t bb = 0; bb < cnt_c; ++bb) {
+            const uint32_t b = first + bb;
+            const uint32_t j = wave * per_wave + b;
+            if (lane == 0) e_in_exact[j] = E;
+            const SegWindow win = S.win[c & 1][bb];
+            if (E >= win.lo && E <= win.hi) {
+                const SegList *L = &S.list[c & 1][bb];
+                const uint32_t cnt = L->count;
+                if (cnt != 0xFFFFu && cnt > 0) {
+                    const uint32_t q = E - win.lo;
+                    uint32_t below = 0;
+                    for (uint32_t k0 = 0; k0 < cnt; k0 += 32) {
+                        const uint32_t k = k0 + lane;
+                        const bool le = k < cnt && (uint32_t)L->ein[k] <= q;
+                        below += __popc(__ballot_sync(0xFFFFFFFFu, le));
+                    }
+                    E = win.lo + L->eout[below - 1];
+                } else {
+                    E = table[(size_t)b * kWinMax + (E - win.lo)];
                 }
-                E = win.lo + L->eout[a];
             } else {
-                E = table[(size_t)b * kWinMax + (E - win.lo)];
+                const uint32_t i0 = j * kSegLen, i1 = min(n, i0 + kSegLen);
+                uint32_t e_exact = 0;
+                if (lane == 0) e_exact = walk_segment_exact(entries, pos, i0, i1, E, t0);
+                E = __shfl_sync(0xFFFFFFFFu, e_exact, 0);
+                fallbacks += 1;
             }
-        } else {
-            const uint32_t i0 = j * kSegLen, i1 = min(n, i0 + kSegLen);
-            E = walk_segment_exact(entries, pos, i0, i1, E, t0);
-            st->fallbacks += 1;
         }
     }
-    st->e_wave = E;
-    st->waves += 1;
+    if (tid == 0) {
+        st->e_wave = E;
+        st->waves += 1;
+        st->fallbacks += fallbacks;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -757,9 +790,9 @@ size_t walk_scratch_bytes(int64_t capacity, int per_wave) {
     return b;
 }
 
-static size_t resolve_smem_bytes() {
-    return kResolveSegs * (sizeof(SegList) + sizeof(SegWindow));
-}
+static size_t resolve_smem_bytes() { return sizeof(ResolveSmem); }
+
+int walk_per_wave(int sms) { return kWinBlocksPerSM * sms; }
 
 cudaError_t walk_init() {
     cudaError_t e = cudaFuncSetAttribute(k_window, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -809,7 +842,7 @@ cudaError_t launch_walk(const AmbEntry *entries, const uint32_t *pos, const uint
             k_window<<<blocks, kWinThreads, sizeof(WindowSmem), stream>>>(
                 entries, pos, n_ptr, capacity, mu, var, st, w, per_wave, t0, windows, table,
                 lists, st);
-            k_resolve<<<1, 1024, resolve_smem_bytes(), stream>>>(entries, pos, n_ptr, capacity, st,
+            k_resolve<<<1, kResolveThreads, resolve_smem_bytes(), stream>>>(entries, pos, n_ptr, capacity, st,
                                                                w, per_wave, t0, windows, table,
                                                                lists, e_in);
         }
