@@ -212,12 +212,48 @@ struct ChannelView {
 };
 
 // First state where a monotone predicate differs from its value at 0
-// (2^24 when it never does).
+// (2^24 when it never does).  `guess` estimates that state; the search
+// gallops from it to a bracket checked on the exact predicate and bisects
+// inside, so the estimate changes only the cost, never the result.
 template <class F>
-__device__ __forceinline__ uint32_t switch_point(F pred) {
+__device__ __forceinline__ uint32_t switch_point(F pred, double guess) {
     const bool p0 = pred(0u);
     if (pred(kLcgMask) == p0) return kLcgMask + 1u;
+    // invariant: pred(lo) == p0, pred(hi) != p0, lo < hi
     uint32_t lo = 0u, hi = kLcgMask;
+    uint32_t x = kLcgMask / 2u;
+    if (guess == guess) {  // not NaN
+        const double top = (double)(kLcgMask - 1u);
+        x = (uint32_t)(guess < 1.0 ? 1.0 : (guess > top ? top : guess));
+    }
+    uint32_t step = 1u;
+    if (pred(x) == p0) {
+        lo = x;
+        while (hi - lo > 1u) {
+            if (hi - lo <= step) break;
+            const uint32_t y = lo + step;
+            if (pred(y) == p0) {
+                lo = y;
+                step <<= 1;
+            } else {
+                hi = y;
+                break;
+            }
+        }
+    } else {
+        hi = x;
+        while (hi - lo > 1u) {
+            if (hi - lo <= step) break;
+            const uint32_t y = hi - step;
+            if (pred(y) != p0) {
+                hi = y;
+                step <<= 1;
+            } else {
+                lo = y;
+                break;
+            }
+        }
+    }
     while (hi - lo > 1u) {
         const uint32_t mid = lo + ((hi - lo) >> 1);
         if (pred(mid) == p0) lo = mid;
@@ -226,10 +262,19 @@ __device__ __forceinline__ uint32_t switch_point(F pred) {
     return hi;
 }
 
+// The state s1 at which base + raw(s1) would reach `target` if the delta
+// were computed exactly (it is affine in s1): a starting point for
+// switch_point.
+__device__ __forceinline__ double crossing(const ChannelView &cv, double base, double target) {
+    const double scale = cv.env * (double)cv.span;
+    return ((target - base) / scale + 0.5) / kNormalization - 1.0;
+}
+
 __device__ void copy_intervals(const ChannelView &cv, AmbEntry &e, uint32_t *err) {
-    uint32_t b[3] = {switch_point([&](uint32_t s) { return cv.low_ok(s); }),
-                     switch_point([&](uint32_t s) { return cv.high_ok(s); }),
-                     switch_point([&](uint32_t s) { return cv.floor_test(s); })};
+    uint32_t b[3] = {
+        switch_point([&](uint32_t s) { return cv.low_ok(s); }, crossing(cv, cv.cd, cv.dc.low)),
+        switch_point([&](uint32_t s) { return cv.high_ok(s); }, crossing(cv, cv.cd, cv.dc.high)),
+        switch_point([&](uint32_t s) { return cv.floor_test(s); }, crossing(cv, cv.cand, cv.od))};
     // sort the three breakpoints
     if (b[0] > b[1]) { const uint32_t t = b[0]; b[0] = b[1]; b[1] = t; }
     if (b[1] > b[2]) { const uint32_t t = b[1]; b[1] = b[2]; b[2] = t; }
@@ -266,41 +311,29 @@ __device__ void copy_intervals(const ChannelView &cv, AmbEntry &e, uint32_t *err
     if (intervals == 2) { e.l2 = lo[1] << 8; e.w2 = (hi[1] - lo[1]) << 8; }
 }
 
+// Lists every RNG-dependent channel in chain order: entry a gets its site
+// (l1), channel (w1) and draw position; k_coef fills in the rest.
 __global__ void __launch_bounds__(kSegThreads)
-    k_amb(const uint8_t *__restrict__ meta, const double *__restrict__ cand, int64_t sites, int w,
-          const uint16_t *__restrict__ rgbi, const float *__restrict__ lut,
-          const fx_stage *__restrict__ stages, fx_params p, const uint32_t *__restrict__ seg_base,
+    k_amb(const uint8_t *__restrict__ meta, int64_t sites, const uint32_t *__restrict__ seg_base,
           const uint32_t *__restrict__ seg_amb, AmbEntry *__restrict__ entries,
-          uint32_t *__restrict__ pos_out, int64_t capacity, uint32_t *err) {
+          uint32_t *__restrict__ pos_out, int64_t capacity) {
     __shared__ uint32_t ws[kSegThreads / 32];
     const int64_t first = (int64_t)blockIdx.x * kSegment + threadIdx.x * kPer;
     uint8_t m[kPer];
     load_meta(meta, first, sites, m);
     uint32_t P, A;
     site_offsets(m, seg_base, seg_amb, ws, P, A);
-    const DitherConst dc = dither_const(p);
-#pragma unroll 1
+#pragma unroll
     for (int i = 0; i < kPer; ++i) {
-        const int64_t site = first + i;
         if (meta_amb(m[i])) {
-            const SiteInfo si = site_info(site, w, rgbi, lut, stages, p);
-            uint32_t pos = P;
-            uint32_t a = A;
+            uint32_t pos = P, a = A;
+#pragma unroll
             for (int c = 0; c < 3; ++c) {
                 const int code = meta_code(m[i], c);
                 if (code == 3) {
-                    ChannelView cv;
-                    cv.cand = cand[3 * site + c];
-                    cv.cd = (double)(float)cv.cand;
-                    cv.dc = dc;
-                    cv.env = ((dc.high - cv.cd) * (cv.cd - dc.low)) * dc.coefficient;
-                    cv.span = (float)((double)p.dither_scales[c] * cv.cd);
-                    cv.od = (double)si.orig[c];
-                    AmbEntry e;
-                    copy_intervals(cv, e, err);
-                    e.a0 = e.c0 = e.a1 = e.c1 = 0u;
                     if ((int64_t)a < capacity) {
-                        entries[a] = e;
+                        entries[a].l1 = (uint32_t)(first + i);
+                        entries[a].w1 = (uint32_t)c;
                         pos_out[a] = pos;
                     }
                     ++a;
@@ -315,17 +348,38 @@ __global__ void __launch_bounds__(kSegThreads)
     }
 }
 
+// One thread per listed channel: its copy intervals (from the exact binary64
+// predicates) and the affine jumps from the previous listed channel.
 __global__ void k_coef(AmbEntry *__restrict__ entries, const uint32_t *__restrict__ pos,
-                       const uint32_t *__restrict__ n_amb_ptr, int64_t capacity) {
+                       const uint32_t *__restrict__ n_amb_ptr, int64_t capacity,
+                       const double *__restrict__ cand, int w, const uint16_t *__restrict__ rgbi,
+                       const float *__restrict__ lut, fx_params p, uint32_t *err) {
     const uint32_t n = (uint32_t)min((int64_t)*n_amb_ptr, capacity);
+    const DitherConst dc = dither_const(p);
+    const int64_t su = 6 * (int64_t)w;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int64_t site = entries[i].l1;
+        const int c = (int)entries[i].w1;
+        const int64_t pixel = site < su ? site % w : site - su;
+        const uint2 raw = reinterpret_cast<const uint2 *>(rgbi)[pixel];
+        const uint32_t lane = c == 0 ? (raw.x & 0xFFFFu) : (c == 1 ? (raw.x >> 16) : (raw.y & 0xFFFFu));
+        ChannelView cv;
+        cv.cand = cand[3 * site + c];
+        cv.cd = (double)(float)cv.cand;
+        cv.dc = dc;
+        cv.env = ((dc.high - cv.cd) * (cv.cd - dc.low)) * dc.coefficient;
+        cv.span = (float)((double)p.dither_scales[c] * cv.cd);
+        cv.od = (double)__ldg(lut + lane);
+        AmbEntry e;
+        copy_intervals(cv, e, err);
         const uint64_t gap = (i == 0) ? (uint64_t)pos[0] + 1u : (uint64_t)(pos[i] - pos[i - 1]);
         const Affine f = lcg_power_t(gap);
         const Affine f1 = affine_compose(Affine{125u, 256u}, f);  // one more draw
-        entries[i].a0 = f.a;
-        entries[i].c0 = f.c;
-        entries[i].a1 = (i == 0) ? f.a : f1.a;  // no previous channel before the first
-        entries[i].c1 = (i == 0) ? f.c : f1.c;
+        e.a0 = f.a;
+        e.c0 = f.c;
+        e.a1 = (i == 0) ? f.a : f1.a;  // no previous channel before the first
+        e.c1 = (i == 0) ? f.c : f1.c;
+        entries[i] = e;
     }
 }
 
@@ -512,11 +566,11 @@ cudaError_t launch_writer(const Geometry &g, const uint8_t *meta, const double *
     cudaMemsetAsync(ctr, 0, sizeof(DevCounters), stream);
     k_seg_sums<<<(unsigned)segs, kSegThreads, 0, stream>>>(meta, g.sites, b.seg_base, b.seg_amb);
     k_seg_scan<<<1, 1024, 0, stream>>>(b.seg_base, b.seg_amb, segs);
-    k_amb<<<(unsigned)segs, kSegThreads, 0, stream>>>(meta, cand, g.sites, g.w, rgbi, lut, stages,
-                                                      p, b.seg_base, b.seg_amb, b.entries, b.pos,
-                                                      b.capacity, err);
+    k_amb<<<(unsigned)segs, kSegThreads, 0, stream>>>(meta, g.sites, b.seg_base, b.seg_amb,
+                                                      b.entries, b.pos, b.capacity);
     const uint32_t *n_amb = b.seg_amb + segs;
-    k_coef<<<1184, 256, 0, stream>>>(b.entries, b.pos, n_amb, b.capacity);
+    k_coef<<<1184, 256, 0, stream>>>(b.entries, b.pos, n_amb, b.capacity, cand, g.w, rgbi, lut, p,
+                                     err);
     marks.mark(5, stream);
     // The walk's launch shape depends on the channel count: read it back.
     cudaMemcpyAsync(b.h_n, n_amb, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream);
