@@ -613,23 +613,37 @@ __global__ void __launch_bounds__(kResolveThreads)
         // and the first is the window's lowest candidate
         const uint32_t first = c * kResolveChunk;
         const uint32_t cnt_c = min((uint32_t)kResolveChunk, here - first);
+        // software-pipelined: hop bb+1's window and list (independent of E)
+        // are loaded while hop bb resolves
+        constexpr int kM = kListMax / 32;
+        auto load_hop = [&](uint32_t bb, SegWindow &w, uint32_t &cnt, uint32_t (&e)[kM]) {
+            w = S.win[c & 1][bb];
+            const SegList *L = &S.list[c & 1][bb];
+            cnt = L->count;
+#pragma unroll
+            for (int m = 0; m < kM; ++m) {
+                const uint32_t k = m * 32 + lane;
+                e[m] = (cnt != 0xFFFFu && k < cnt) ? (uint32_t)L->ein[k] : 0xFFFFFFFFu;
+            }
+        };
+        SegWindow win{};
+        uint32_t cnt = 0, ein[kM];
+        if (cnt_c) load_hop(0, win, cnt, ein);
         for (uint32_t bb = 0; bb < cnt_c; ++bb) {
+            SegWindow nwin{};
+            uint32_t ncnt = 0, nein[kM];
+            if (bb + 1 < cnt_c) load_hop(bb + 1, nwin, ncnt, nein);
             const uint32_t b = first + bb;
             const uint32_t j = wave * per_wave + b;
             if (lane == 0) e_in_exact[j] = E;
-            const SegWindow win = S.win[c & 1][bb];
             if (E >= win.lo && E <= win.hi) {
-                const SegList *L = &S.list[c & 1][bb];
-                const uint32_t cnt = L->count;
                 if (cnt != 0xFFFFu && cnt > 0) {
                     const uint32_t q = E - win.lo;
                     uint32_t below = 0;
-                    for (uint32_t k0 = 0; k0 < cnt; k0 += 32) {
-                        const uint32_t k = k0 + lane;
-                        const bool le = k < cnt && (uint32_t)L->ein[k] <= q;
-                        below += __popc(__ballot_sync(0xFFFFFFFFu, le));
-                    }
-                    E = win.lo + L->eout[below - 1];
+#pragma unroll
+                    for (int m = 0; m < kM; ++m)
+                        below += __popc(__ballot_sync(0xFFFFFFFFu, ein[m] <= q));
+                    E = win.lo + S.list[c & 1][bb].eout[below - 1];
                 } else {
                     E = table[(size_t)b * kWinMax + (E - win.lo)];
                 }
@@ -640,6 +654,10 @@ __global__ void __launch_bounds__(kResolveThreads)
                 E = __shfl_sync(0xFFFFFFFFu, e_exact, 0);
                 fallbacks += 1;
             }
+            win = nwin;
+            cnt = ncnt;
+#pragma unroll
+            for (int m = 0; m < kM; ++m) ein[m] = nein[m];
         }
     }
     if (tid == 0) {
