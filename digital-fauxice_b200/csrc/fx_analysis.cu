@@ -719,6 +719,7 @@ cudaError_t launch_analysis(const uint16_t *rgbi, const Geometry &g, const float
 size_t stencil_smem_bytes() { return sizeof(StencilSmem); }
 
 cudaError_t producer_init();
+cudaError_t writer_init();
 
 // Opt in to the dynamic shared memory the tiled kernels use (once per
 // device, with the device current).
@@ -727,6 +728,8 @@ cudaError_t analysis_init() {
                                          (int)sizeof(StencilSmem));
     if (e != cudaSuccess) return e;
     e = walk_init();
+    if (e != cudaSuccess) return e;
+    e = writer_init();
     if (e != cudaSuccess) return e;
     return producer_init();
 }

@@ -438,6 +438,38 @@ __device__ __forceinline__ bool emit_one(float v, const uint32_t *hi, const uint
     return true;
 }
 
+// Affine jump tables: g_jump[j][d] = g^(d * 64^j) in T space, so any jump
+// below 2^36 draws is six table lookups and compositions.
+constexpr int kJumpDigits = 6;
+__device__ Affine g_jump[kJumpDigits][64];
+
+cudaError_t writer_init() {
+    Affine tab[kJumpDigits][64];
+    Affine step{125u, 256u};  // g^(64^j)
+    for (int j = 0; j < kJumpDigits; ++j) {
+        Affine acc{1u, 0u};
+        for (int d = 0; d < 64; ++d) {
+            tab[j][d] = acc;
+            acc = affine_compose(step, acc);
+        }
+        step = acc;
+    }
+    return cudaMemcpyToSymbol(g_jump, tab, sizeof(tab));
+}
+
+__device__ __forceinline__ uint32_t jump_by_table(const Affine (*tab)[64], uint32_t s,
+                                                  uint64_t n) {
+    Affine r{1u, 0u};
+#pragma unroll
+    for (int j = 0; j < kJumpDigits; ++j) r = affine_compose(tab[j][(n >> (6 * j)) & 63u], r);
+    return ((r.a * (s << 8) + r.c) >> 8) & kLcgMask;
+}
+
+// Public sites: exact draws and values, emit, counters.  Phase 1 emits every
+// site that was not attempted (its output is the identity emit) and lists
+// the attempted ones in shared memory; phase 2 processes that list densely,
+// each entry from its own start state g^(fixed + extra before it)(s0), and
+// checks the draws it makes against the classification and the walk.
 __global__ void __launch_bounds__(kSegThreads)
     k_apply(const uint8_t *__restrict__ meta, const double *__restrict__ cand, int64_t sites,
             int w, const uint16_t *__restrict__ rgbi, const float *__restrict__ lut,
@@ -450,81 +482,134 @@ __global__ void __launch_bounds__(kSegThreads)
     __shared__ uint32_t ws[kSegThreads / 32];
     __shared__ uint32_t hi[256], lo[256];
     __shared__ unsigned long long scratch[8];
+    __shared__ Affine s_jump[kJumpDigits][64];
+    __shared__ uint32_t s_ref[kSegment], s_p[kSegment], s_a[kSegment];
     for (int i = threadIdx.x; i < 256; i += kSegThreads) {
         hi[i] = g_high[i];
         lo[i] = g_low[i];
     }
+    for (int i = threadIdx.x; i < kJumpDigits * 64; i += kSegThreads)
+        s_jump[i / 64][i % 64] = g_jump[i / 64][i % 64];
     const int64_t su = 6 * (int64_t)w;
-    const int64_t first = (int64_t)blockIdx.x * kSegment + threadIdx.x * kPer;
+    const int64_t seg0 = (int64_t)blockIdx.x * kSegment;
+    const int64_t first = seg0 + threadIdx.x * kPer;
     uint8_t m[kPer];
     load_meta(meta, first, sites, m);
     uint32_t P, A;
     site_offsets(m, seg_base, seg_amb, ws, P, A);  // contains __syncthreads
-    const DitherConst dc = dither_const(p);
-    unsigned long long att = 0, written = 0, changed = 0, draws_total = 0;
-#pragma unroll 1
+
+    // ---- phase 1: identity emits; list the attempted sites ---------------
+    uint32_t mine = 0, pp[kPer], aa[kPer];
+    bool listed_here[kPer];
+    bool ok = true;
+#pragma unroll
     for (int i = 0; i < kPer; ++i) {
         const int64_t site = first + i;
         const uint8_t mi = m[i];
+        listed_here[i] = false;
+        pp[i] = P;
+        aa[i] = A;
         if (site >= su && site < sites) {
-            const int64_t pixel = site - su;
-            const SiteInfo si = site_info(site, w, rgbi, lut, stages, p);
-            float values[3] = {si.orig[0], si.orig[1], si.orig[2]};
             if (mi & 0x80u) {
-                const int amb = meta_amb(mi);
-                const uint32_t e_before = extra_before(extra_after, A, capacity);
-                const uint32_t extra = extra_before(extra_after, A + amb, capacity) - e_before;
-                uint32_t state = lcg_jump(s0, (uint64_t)P + e_before);
-                const double *cd = cand + 3 * site;
-                const double c3[3] = {cd[0], cd[1], cd[2]};
-                bool valid = true;
-#pragma unroll
-                for (int c = 0; c < 3; ++c) valid &= isfinite(c3[c]) && c3[c] > 0.0;
-                uint32_t draws = 0;
-                if (valid) {
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) {
-                        int drew;
-                        const double firstd = dither_delta(c3[c], p.dither_scales[c], dc, state, drew);
-                        draws += drew;
-                        if (si.floor_enabled && c3[c] + firstd <= (double)si.orig[c]) {
-                            values[c] = si.orig[c];
-                        } else {
-                            double d = firstd;
-                            if (si.floor_enabled) {
-                                d = dither_delta(c3[c], p.dither_scales[c], dc, state, drew);
-                                draws += drew;
-                            }
-                            values[c] = (float)(c3[c] + d);
-                        }
-                    }
-                }
-                if ((int64_t)(A + amb) <= capacity && draws != (uint32_t)meta_base(mi) + extra)
-                    raise_error(err, FX_ERR_INTERNAL);
-                att += 1;
-                draws_total += draws;
-                written += (values[0] != si.orig[0] || values[1] != si.orig[1] ||
-                            values[2] != si.orig[2]);
+                listed_here[i] = true;
+                ++mine;
+            } else {
+                const int64_t pixel = site - su;
+                const uint2 raw = reinterpret_cast<const uint2 *>(rgbi)[pixel];
+                uint16_t e0[3];
+                ok &= emit_one(__ldg(lut + (raw.x & 0xFFFFu)), hi, lo, e0[0]);
+                ok &= emit_one(__ldg(lut + (raw.x >> 16)), hi, lo, e0[1]);
+                ok &= emit_one(__ldg(lut + (raw.y & 0xFFFFu)), hi, lo, e0[2]);
+                uint16_t *o = rgb_out + 3 * pixel;
+                o[0] = e0[0];
+                o[1] = e0[1];
+                o[2] = e0[2];
+                if (changed_out) changed_out[pixel] = 0;
             }
-            uint16_t e[3], e0[3];
-            bool ok = true;
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                ok &= emit_one(values[c], hi, lo, e[c]);
-                ok &= emit_one(si.orig[c], hi, lo, e0[c]);
-            }
-            if (!ok) raise_error(err, FX_ERR_NONFINITE_WORK);
-            const bool ch = (e[0] != e0[0]) || (e[1] != e0[1]) || (e[2] != e0[2]);
-            changed += ch;
-            uint16_t *o = rgb_out + 3 * pixel;
-            o[0] = e[0];
-            o[1] = e[1];
-            o[2] = e[2];
-            if (changed_out) changed_out[pixel] = ch ? 1 : 0;
         }
         P += meta_base(mi);
         A += meta_amb(mi);
     }
+    uint32_t listed;
+    const uint32_t at = block_exclusive_scan<kSegThreads>(mine, listed, ws);
+    {
+        uint32_t slot = at;
+#pragma unroll
+        for (int i = 0; i < kPer; ++i) {
+            if (listed_here[i]) {
+                s_ref[slot] = ((uint32_t)m[i] << 16) | (uint32_t)(threadIdx.x * kPer + i);
+                s_p[slot] = pp[i];
+                s_a[slot] = aa[i];
+                ++slot;
+            }
+        }
+    }
+    __syncthreads();
+
+    // ---- phase 2: attempted sites, densely ----------------------------------
+    const DitherConst dc = dither_const(p);
+    unsigned long long att = 0, written = 0, changed = 0, draws_total = 0;
+    for (uint32_t k = threadIdx.x; k < listed; k += kSegThreads) {
+        const uint32_t r = s_ref[k];
+        const uint8_t mi = (uint8_t)(r >> 16);
+        const int64_t site = seg0 + (r & 0xFFFFu);
+        const uint32_t pixel = (uint32_t)(site - su);  // H*W < 2^31
+        const uint32_t y = pixel / (uint32_t)w;
+        const uint2 raw = reinterpret_cast<const uint2 *>(rgbi)[pixel];
+        const float orig[3] = {__ldg(lut + (raw.x & 0xFFFFu)), __ldg(lut + (raw.x >> 16)),
+                               __ldg(lut + (raw.y & 0xFFFFu))};
+        const bool floor_enabled = p.driver_gate_primary || stages[y + 6].gate_secondary;
+        float values[3] = {orig[0], orig[1], orig[2]};
+        const uint32_t Ak = s_a[k];
+        const int amb = meta_amb(mi);
+        const uint32_t e_before = extra_before(extra_after, Ak, capacity);
+        const uint32_t extra = extra_before(extra_after, Ak + amb, capacity) - e_before;
+        uint32_t state = jump_by_table(s_jump, s0, (uint64_t)s_p[k] + e_before);
+        const double *cd = cand + 3 * site;
+        const double c3[3] = {cd[0], cd[1], cd[2]};
+        bool valid = true;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) valid &= isfinite(c3[c]) && c3[c] > 0.0;
+        uint32_t draws = 0;
+        if (valid) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                int drew;
+                const double firstd = dither_delta(c3[c], p.dither_scales[c], dc, state, drew);
+                draws += drew;
+                if (floor_enabled && c3[c] + firstd <= (double)orig[c]) {
+                    values[c] = orig[c];
+                } else {
+                    double d = firstd;
+                    if (floor_enabled) {
+                        d = dither_delta(c3[c], p.dither_scales[c], dc, state, drew);
+                        draws += drew;
+                    }
+                    values[c] = (float)(c3[c] + d);
+                }
+            }
+        }
+        if ((int64_t)(Ak + amb) <= capacity && draws != (uint32_t)meta_base(mi) + extra)
+            raise_error(err, FX_ERR_INTERNAL);
+        att += 1;
+        draws_total += draws;
+        written += (values[0] != orig[0] || values[1] != orig[1] || values[2] != orig[2]);
+        uint16_t e[3], e0[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            ok &= emit_one(orig[c], hi, lo, e0[c]);
+            e[c] = e0[c];
+            if (!(values[c] == orig[c])) ok &= emit_one(values[c], hi, lo, e[c]);
+        }
+        const bool ch = (e[0] != e0[0]) || (e[1] != e0[1]) || (e[2] != e0[2]);
+        changed += ch;
+        uint16_t *o = rgb_out + 3 * (int64_t)pixel;
+        o[0] = e[0];
+        o[1] = e[1];
+        o[2] = e[2];
+        if (changed_out) changed_out[pixel] = ch ? 1 : 0;
+    }
+    if (!ok) raise_error(err, FX_ERR_NONFINITE_WORK);
     att = block_sum<kSegThreads, unsigned long long>(att, scratch);
     written = block_sum<kSegThreads, unsigned long long>(written, scratch);
     changed = block_sum<kSegThreads, unsigned long long>(changed, scratch);
