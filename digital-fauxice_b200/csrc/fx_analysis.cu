@@ -175,10 +175,32 @@ __device__ __forceinline__ float rgb_candidate(double avg, float weight) {
     return (float)avg;
 }
 
+// The combiner's and writer's float32 profile constants, widened once on the
+// host (the widening is exact).
+struct CombineConst {
+    double band_scale[3], factor_a[9], factor_b[9], coarse_slope[3], strength[3];
+    double dither_scale[3];
+};
+
+static CombineConst combine_const(const fx_params &p) {
+    CombineConst c;
+    for (int i = 0; i < 3; ++i) {
+        c.band_scale[i] = (double)p.band_scales[i];
+        c.coarse_slope[i] = (double)p.coarse_slopes[i];
+        c.strength[i] = (double)p.configured_strengths[i];
+        c.dither_scale[i] = (double)p.dither_scales[i];
+    }
+    for (int i = 0; i < 9; ++i) {
+        c.factor_a[i] = (double)p.factors_a[i];
+        c.factor_b[i] = (double)p.factors_b[i];
+    }
+    return c;
+}
+
 // combine_recovered_candidate (reconstruction.py:807-887).  feats[r][l].
 __device__ bool combine(const float cand[3][3], const float source[3], const float weights[4],
                         const float feats[5][4], int records, float coarse_reference,
-                        const fx_params &p, double out[3]) {
+                        const fx_params &p, const CombineConst &cc, double out[3]) {
     bool finite = true;
 #pragma unroll
     for (int k = 0; k < 3; ++k)
@@ -193,18 +215,31 @@ __device__ bool combine(const float cand[3][3], const float source[3], const flo
         for (int l = 0; l < 4; ++l) finite &= isfinite(feats[r][l]);
     if (!finite) return false;
 
+    // band ranges: each record's four values widened once
     double rmin[3], rmax[3];
+    double f00;
+    {
+        const double a0 = (double)feats[0][0], a1 = (double)feats[0][1];
+        const double a2 = (double)feats[0][2], a3 = (double)feats[0][3];
+        f00 = a0;
+        rmin[0] = rmax[0] = a1 - a0;
+        rmin[1] = rmax[1] = a2 - a1;
+        rmin[2] = rmax[2] = a3 - a2;
+    }
+    for (int r = 1; r < records; ++r) {
+        const double a0 = (double)feats[r][0], a1 = (double)feats[r][1];
+        const double a2 = (double)feats[r][2], a3 = (double)feats[r][3];
+        const double d[3] = {a1 - a0, a2 - a1, a3 - a2};
+#pragma unroll
+        for (int t = 0; t < 3; ++t) {
+            rmin[t] = (d[t] < rmin[t]) ? d[t] : rmin[t];
+            rmax[t] = (d[t] > rmax[t]) ? d[t] : rmax[t];
+        }
+    }
 #pragma unroll
     for (int t = 0; t < 3; ++t) {
-        double mn = (double)feats[0][t + 1] - (double)feats[0][t];
-        double mx = mn;
-        for (int r = 1; r < records; ++r) {
-            const double d = (double)feats[r][t + 1] - (double)feats[r][t];
-            mn = (d < mn) ? d : mn;
-            mx = (d > mx) ? d : mx;
-        }
-        rmin[t] = (double)(float)mn;
-        rmax[t] = (double)(float)mx;
+        rmin[t] = (double)(float)rmin[t];
+        rmax[t] = (double)(float)rmax[t];
     }
     double strengths[3];
     if (p.configured_strengths[0] == 0.0f) {
@@ -213,42 +248,42 @@ __device__ bool combine(const float cand[3][3], const float source[3], const flo
         const double clamped = (lower < 1.0) ? lower : 1.0;
         strengths[0] = (double)(float)clamped;
     } else {
-        strengths[0] = (double)p.configured_strengths[0];
+        strengths[0] = cc.strength[0];
     }
     if (p.configured_strengths[1] == 0.0f) {
         const float m2 = (weights[2] < 0.0f) ? 0.0f : weights[2];
         strengths[1] = (double)m2;
     } else {
-        strengths[1] = (double)p.configured_strengths[1];
+        strengths[1] = cc.strength[1];
     }
-    strengths[2] = (p.configured_strengths[2] == 0.0f)
-                       ? (double)weights[3] * (double)weights[3]
-                       : (double)p.configured_strengths[2];
+    if (p.configured_strengths[2] == 0.0f) {
+        const double w3 = (double)weights[3];
+        strengths[2] = w3 * w3;
+    } else {
+        strengths[2] = cc.strength[2];
+    }
 
     double candidate[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) candidate[c] = (double)cand[0][c];
     if (p.coarse_enabled) {
-        const double delta = (double)coarse_reference - (double)feats[0][0];
+        const double delta = (double)coarse_reference - f00;
 #pragma unroll
-        for (int c = 0; c < 3; ++c)
-            candidate[c] = candidate[c] + (double)p.coarse_slopes[c] * delta;
+        for (int c = 0; c < 3; ++c) candidate[c] = candidate[c] + cc.coarse_slope[c] * delta;
     }
 #pragma unroll
     for (int b = 0; b < 3; ++b) {
         if (!p.band_enabled[b]) continue;
-        const double scale = (double)p.band_scales[b];
+        const double scale = cc.band_scale[b];
         const double emin = rmin[b], emax = rmax[b];
         const bool negative = emin < 0.0 && emax < 0.0;
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            const double coarse_v = (b == 0) ? (double)cand[0][c] : (b == 1) ? (double)cand[1][c]
-                                                                              : (double)cand[2][c];
-            const double fine_v = (b == 0) ? (double)cand[1][c] : (b == 1) ? (double)cand[2][c]
-                                                                            : (double)source[c];
+            const double coarse_v = (double)cand[b][c];
+            const double fine_v = (b < 2) ? (double)cand[b + 1][c] : (double)source[c];
             const double diff = scale * (fine_v - coarse_v);
-            const double fa = (double)p.factors_a[b * 3 + c];
-            const double fb = (double)p.factors_b[b * 3 + c];
+            const double fa = cc.factor_a[b * 3 + c];
+            const double fb = cc.factor_b[b * 3 + c];
             const double upper = negative ? fb * emax : fa * emax;
             const double lower = negative ? fa * emin : fb * emin;
             double residual;
@@ -268,7 +303,7 @@ __device__ bool combine(const float cand[3][3], const float source[3], const flo
 // reconstruction.py:916-982).  Per channel: 0 = no draw, 1 = one draw,
 // 2 = two draws, 3 = one or two draws depending on the state.
 __device__ uint8_t classify_site(const double cand[3], const float orig[3], bool floor_enabled,
-                                 const fx_params &p, const DitherConst &dc, uint32_t *err) {
+                                 const CombineConst &cc, const DitherConst &dc, uint32_t *err) {
     uint8_t meta = 0x80;
     bool valid = true;
 #pragma unroll
@@ -286,7 +321,7 @@ __device__ uint8_t classify_site(const double cand[3], const float orig[3], bool
             code = 1;
         } else {
             const double env = ((dc.high - cd) * (cd - dc.low)) * dc.coefficient;
-            const float span = (float)((double)p.dither_scales[c] * cd);
+            const float span = (float)(cc.dither_scale[c] * cd);
             const double da = dither_raw_delta(cd, env, span, 0u);
             const double db = dither_raw_delta(cd, env, span, kLcgMask);
             double lo = (da < db) ? da : db, hi = (da < db) ? db : da;
@@ -319,20 +354,19 @@ struct StencilSmem {
     float hs[PR][PC];
     float hwa[PR][PC];
     float hwr[3][RR][RC];
-    float paux[CR][RECC];
-    float cs[2][5][CR][CC];       // [score|waux][S3,S5,S7,S9,B16]
+    double cs[2][5][CR][CC];      // [score|waux][S3,S5,S7,S9,B16], float-rounded
     float rcs[3][4][kTileH][RC];  // [channel][S3,S5,S7,S9]
     Record rec[CR][RECC];
     float cw[kTileH][kTileW][4];
-    uint8_t low[RR][RC];
+    float auxt[RR][RC];  // aux at clamped (y0-4+r, x0-4+c): decision bars and point aux
 };
 
 __global__ void __launch_bounds__(kStencilThreads)
     k_stencil(const uint16_t *__restrict__ rgbi, Geometry g, const float *__restrict__ lut,
-              const fx_stage *__restrict__ stages, fx_params p, const float *__restrict__ aux,
-              const float *__restrict__ hs, const float *__restrict__ hwa,
-              const float *__restrict__ hwr, int64_t plane, double *__restrict__ cand_out,
-              uint8_t *__restrict__ meta_out, uint32_t *err) {
+              const fx_stage *__restrict__ stages, fx_params p, CombineConst cc,
+              const float *__restrict__ aux, const float *__restrict__ hs,
+              const float *__restrict__ hwa, const float *__restrict__ hwr, int64_t plane,
+              double *__restrict__ cand_out, uint8_t *__restrict__ meta_out, uint32_t *err) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     StencilSmem &S = *reinterpret_cast<StencilSmem *>(smem_raw);
     const int tid = threadIdx.x;
@@ -340,32 +374,33 @@ __global__ void __launch_bounds__(kStencilThreads)
     const int h = g.h, w = g.w;
 
     // ---- stage the tile ---------------------------------------------------
+    // Every element goes through cp.async, so all of a thread's requests
+    // are in flight at once; one wait then covers the whole tile.
+    auto cp4 = [](void *dst, const void *src) {
+        const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src));
+    };
     for (int i = tid; i < PR * PC; i += kStencilThreads) {
         const int r = i / PC, c = i % PC;
         const int64_t o = (int64_t)(y0 + r) * g.pitch + (x0 + c);  // padded (y0-5+r, x0-5+c)
-        S.hs[r][c] = hs[o];
-        S.hwa[r][c] = hwa[o];
+        cp4(&S.hs[r][c], hs + o);
+        cp4(&S.hwa[r][c], hwa + o);
     }
     for (int i = tid; i < 3 * RR * RC; i += kStencilThreads) {
         const int ch = i / (RR * RC), rem = i % (RR * RC);
         const int r = rem / RC, c = rem % RC;
-        S.hwr[ch][r][c] = hwr[ch * plane + (int64_t)(y0 + 1 + r) * g.pitch + (x0 + 1 + c)];
+        cp4(&S.hwr[ch][r][c], hwr + ch * plane + (int64_t)(y0 + 1 + r) * g.pitch + (x0 + 1 + c));
     }
-    const float thr = p.decision_threshold;
     for (int i = tid; i < RR * RC; i += kStencilThreads) {
         const int r = i / RC, c = i % RC;
         int yy = y0 - 4 + r, xx = x0 - 4 + c;
         yy = yy < 0 ? 0 : (yy > h - 1 ? h - 1 : yy);
         xx = xx < 0 ? 0 : (xx > w - 1 ? w - 1 : xx);
-        S.low[r][c] = aux[(int64_t)yy * w + xx] < thr;
+        cp4(&S.auxt[r][c], aux + (int64_t)yy * w + xx);
     }
-    for (int i = tid; i < CR * RECC; i += kStencilThreads) {
-        const int r = i / RECC, c = i % RECC;
-        int yy = y0 - 1 + r;
-        const int xx = x0 - 1 + c;
-        yy = yy < 0 ? 0 : (yy > h - 1 ? h - 1 : yy);
-        S.paux[r][c] = (xx >= 0 && xx < w) ? aux[(int64_t)yy * w + xx] : 0.0f;
-    }
+    asm volatile("cp.async.commit_group;\n" ::);
+    asm volatile("cp.async.wait_group 0;\n" ::);
+    const float thr = p.decision_threshold;
     __syncthreads();
 
     // ---- vertical column sums, shared by every record of the tile ---------
@@ -410,11 +445,11 @@ __global__ void __launch_bounds__(kStencilThreads)
             double wq[3], nq[3];
 #pragma unroll
             for (int src = 0; src < 2; ++src) {
-                const float(*s3)[CC] = S.cs[src][0];
-                const float(*s5)[CC] = S.cs[src][1];
-                const float(*s7)[CC] = S.cs[src][2];
-                const float(*s9)[CC] = S.cs[src][3];
-                const float(*bb)[CC] = S.cs[src][4];
+                const double(*s3)[CC] = S.cs[src][0];
+                const double(*s5)[CC] = S.cs[src][1];
+                const double(*s7)[CC] = S.cs[src][2];
+                const double(*s9)[CC] = S.cs[src][3];
+                const double(*bb)[CC] = S.cs[src][4];
                 double q69, q21;
                 q69_q21([&](int k) { return s3[r][c + k]; }, [&](int k) { return s5[r][c + k]; },
                         [&](int k) { return s7[r][c + k]; }, [&](int k) { return s9[r][c + k]; },
@@ -437,7 +472,7 @@ __global__ void __launch_bounds__(kStencilThreads)
                 }
             }
             if (point_score > 0.0f) {
-                rec.a[3] = S.paux[r][c];
+                rec.a[3] = S.auxt[r + 3][c + 3];  // xx is inside the row here
             } else {
                 rec.a[3] = 0.0f;
                 rec.fb |= 8u;
@@ -459,6 +494,9 @@ __global__ void __launch_bounds__(kStencilThreads)
     const int y = y0 + ty, x = x0 + tx;
     if (y >= h || x >= w) return;
     const int64_t site = 6 * (int64_t)w + (int64_t)y * w + x;
+    // the original's samples: issued first so their latency overlaps the
+    // decision and candidate arithmetic
+    const uint2 raw = reinterpret_cast<const uint2 *>(rgbi)[(int64_t)y * w + x];
     const fx_stage ws = stages[y + 6];  // writer stage y+7
     const bool floor_enabled = p.driver_gate_primary || ws.gate_secondary;
 
@@ -467,10 +505,10 @@ __global__ void __launch_bounds__(kStencilThreads)
     int vl = 0, vr = 0, ha = 0, hb = 0;
 #pragma unroll
     for (int d = -4; d <= 4; ++d) {
-        vl += S.low[ty + 4 + d][tx + 4 - rad];
-        vr += S.low[ty + 4 + d][tx + 4 + rad];
-        ha += S.low[ty + 4 - rad][tx + 4 + d];
-        hb += S.low[ty + 4 + rad][tx + 4 + d];
+        vl += S.auxt[ty + 4 + d][tx + 4 - rad] < thr;
+        vr += S.auxt[ty + 4 + d][tx + 4 + rad] < thr;
+        ha += S.auxt[ty + 4 - rad][tx + 4 + d] < thr;
+        hb += S.auxt[ty + 4 + rad][tx + 4 + d] < thr;
     }
     const int lim = p.count_limit;
     bool eligible = !(vl > lim || ha > lim || vr > lim || hb > lim);
@@ -483,6 +521,8 @@ __global__ void __launch_bounds__(kStencilThreads)
         meta_out[site] = 0;
         return;
     }
+    const float orig[3] = {__ldg(lut + (raw.x & 0xFFFFu)), __ldg(lut + (raw.x >> 16)),
+                           __ldg(lut + (raw.y & 0xFFFFu))};
 
     const float fallback = ws.coarse;
     const int records = p.cross_neighbor ? 5 : 1;
@@ -516,17 +556,14 @@ __global__ void __launch_bounds__(kStencilThreads)
         cand[1][ch] = rgb_candidate(q21, weights[1]);
         cand[2][ch] = rgb_candidate(q16, weights[2]);
     }
-    const uint2 raw = reinterpret_cast<const uint2 *>(rgbi)[(int64_t)y * w + x];
-    const float orig[3] = {__ldg(lut + (raw.x & 0xFFFFu)), __ldg(lut + (raw.x >> 16)),
-                           __ldg(lut + (raw.y & 0xFFFFu))};
     double combined[3];
-    if (!combine(cand, orig, weights, feats, records, ws.coarse, p, combined)) {
+    if (!combine(cand, orig, weights, feats, records, ws.coarse, p, cc, combined)) {
         raise_error(err, FX_ERR_COMBINER_INPUT);
         meta_out[site] = 0;
         return;
     }
     const DitherConst dc = dither_const(p);
-    meta_out[site] = classify_site(combined, orig, floor_enabled, p, dc, err);
+    meta_out[site] = classify_site(combined, orig, floor_enabled, cc, dc, err);
     double *dst = cand_out + 3 * site;
     dst[0] = combined[0];
     dst[1] = combined[1];
@@ -601,8 +638,8 @@ __device__ __forceinline__ int max1(int v) { return v < 1 ? 1 : v; }
 
 __global__ void k_startup(const uint16_t *__restrict__ rgbi, StartupView v,
                           const float *__restrict__ lut, const fx_stage *__restrict__ stages,
-                          fx_params p, double *__restrict__ cand_out, uint8_t *__restrict__ meta_out,
-                          uint32_t *err) {
+                          fx_params p, CombineConst cc, double *__restrict__ cand_out,
+                          uint8_t *__restrict__ meta_out, uint32_t *err) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int k = blockIdx.y;  // stage hit k+1, centre k-6
     const int w = v.g.w;
@@ -670,13 +707,13 @@ __global__ void k_startup(const uint16_t *__restrict__ rgbi, StartupView v,
     const float orig[3] = {__ldg(lut + (raw.x & 0xFFFFu)), __ldg(lut + (raw.x >> 16)),
                            __ldg(lut + (raw.y & 0xFFFFu))};
     double combined[3];
-    if (!combine(cand, orig, weights, feats, records, act.coarse, p, combined)) {
+    if (!combine(cand, orig, weights, feats, records, act.coarse, p, cc, combined)) {
         raise_error(err, FX_ERR_COMBINER_INPUT);
         meta_out[site] = 0;
         return;
     }
     const DitherConst dc = dither_const(p);
-    meta_out[site] = classify_site(combined, orig, floor_enabled, p, dc, err);
+    meta_out[site] = classify_site(combined, orig, floor_enabled, cc, dc, err);
     double *dst = cand_out + 3 * site;
     dst[0] = combined[0];
     dst[1] = combined[1];
@@ -691,6 +728,7 @@ cudaError_t launch_analysis(const uint16_t *rgbi, const Geometry &g, const float
                             const fx_stage *stages, const fx_params &p, float *aux, float *hs,
                             float *hwa, float *hwr, int64_t plane, double *cand, uint8_t *meta,
                             uint32_t *err, cudaStream_t stream, const Marks &marks) {
+    const CombineConst cc = combine_const(p);
     {
         dim3 block(256), grid((g.w + 255) / 256, g.h);
         k_auxiliary<<<grid, block, 0, stream>>>(rgbi, g.h, g.w, lut, stages, p.visible_channel,
@@ -704,13 +742,13 @@ cudaError_t launch_analysis(const uint16_t *rgbi, const Geometry &g, const float
     {
         dim3 grid(g.tw, g.th);
         k_stencil<<<grid, kStencilThreads, sizeof(StencilSmem), stream>>>(
-            rgbi, g, lut, stages, p, aux, hs, hwa, hwr, plane, cand, meta, err);
+            rgbi, g, lut, stages, p, cc, aux, hs, hwa, hwr, plane, cand, meta, err);
     }
     marks.mark(3, stream);
     {
         StartupView v{g, aux, hs, hwa, hwr, plane, p.cross_neighbor ? 5 : 4};
         dim3 block(128), grid((g.w + 127) / 128, 6);
-        k_startup<<<grid, block, 0, stream>>>(rgbi, v, lut, stages, p, cand, meta, err);
+        k_startup<<<grid, block, 0, stream>>>(rgbi, v, lut, stages, p, cc, cand, meta, err);
     }
     marks.mark(4, stream);
     return cudaGetLastError();
