@@ -123,6 +123,30 @@ __device__ __forceinline__ ColumnSums column_sums(const float v[9]) {
     return o;
 }
 
+// column_sums on samples already widened to binary64 (the widening is
+// exact, so the chains and roundings are the same).
+__device__ __forceinline__ ColumnSums column_sums_wide(const double *v) {
+    ColumnSums o;
+    double acc = v[3] + v[4];
+    acc += v[5];
+    o.s3 = (float)acc;
+    acc += v[2];
+    acc += v[6];
+    o.s5 = (float)acc;
+    acc += v[1];
+    acc += v[7];
+    o.s7 = (float)acc;
+    acc += v[0];
+    acc += v[8];
+    o.s9 = (float)acc;
+    const double center = v[4];
+    double b = v[3] + center;
+    b += v[5];
+    b += center;
+    o.b16 = (float)(b * (double)(float)(1.0 / 16.0));
+    return o;
+}
+
 // Horizontal combination (reconstruction.py:240-268).  S(k) gives the
 // column sums of patch column k (0..8).
 template <class S3, class S5, class S7, class S9>
@@ -359,6 +383,8 @@ struct StencilSmem {
     Record rec[CR][RECC];
     float cw[kTileH][kTileW][4];
     float auxt[RR][RC];  // aux at clamped (y0-4+r, x0-4+c): decision bars and point aux
+    unsigned long long rowlow[RR];  // bit c: auxt[r][c] below the decision threshold
+    uint32_t collow[RC];            // bit r: the same, by column
 };
 
 __global__ void __launch_bounds__(kStencilThreads)
@@ -403,32 +429,55 @@ __global__ void __launch_bounds__(kStencilThreads)
     const float thr = p.decision_threshold;
     __syncthreads();
 
-    // ---- vertical column sums, shared by every record of the tile ---------
-    for (int i = tid; i < 2 * CR * CC; i += kStencilThreads) {
-        const int src = i / (CR * CC), rem = i % (CR * CC);
-        const int r = rem / CC, c = rem % CC;
-        const float(*pl)[PC] = src ? S.hwa : S.hs;
-        float v[9];
-#pragma unroll
-        for (int k = 0; k < 9; ++k) v[k] = pl[r + k][c];
-        const ColumnSums cs = column_sums(v);
-        S.cs[src][0][r][c] = cs.s3;
-        S.cs[src][1][r][c] = cs.s5;
-        S.cs[src][2][r][c] = cs.s7;
-        S.cs[src][3][r][c] = cs.s9;
-        S.cs[src][4][r][c] = cs.b16;
+    // ---- decision masks and vertical column sums ---------------------------
+    if (tid < RR) {
+        unsigned long long m = 0;
+        for (int c = 0; c < RC; ++c) m |= (unsigned long long)(S.auxt[tid][c] < thr) << c;
+        S.rowlow[tid] = m;
+    } else if (tid >= 32 && tid < 32 + RC) {
+        const int c = tid - 32;
+        uint32_t m = 0;
+        for (int r = 0; r < RR; ++r) m |= (uint32_t)(S.auxt[r][c] < thr) << r;
+        S.collow[c] = m;
     }
-    for (int i = tid; i < 3 * kTileH * RC; i += kStencilThreads) {
-        const int ch = i / (kTileH * RC), rem = i % (kTileH * RC);
-        const int r = rem / RC, c = rem % RC;
-        float v[9];
+    // One work item is a vertical run of column sums in one column: the
+    // samples are loaded and widened once and shared by the run's chains.
+    // Items 0..167: score / waux planes, runs of 5 record rows; items
+    // 168..407: the three RGB planes, runs of 4 pixel rows.
+    constexpr int kWaItems = 2 * CC * 2, kRgbItems = 3 * RC * 2;
+    for (int it = tid; it < kWaItems + kRgbItems; it += kStencilThreads) {
+        if (it < kWaItems) {
+            const int src = it / (2 * CC), rem = it % (2 * CC);
+            const int c = rem >> 1, r0 = (rem & 1) * 5;
+            const float(*pl)[PC] = src ? S.hwa : S.hs;
+            double v[13];
 #pragma unroll
-        for (int k = 0; k < 9; ++k) v[k] = S.hwr[ch][r + k][c];
-        const ColumnSums cs = column_sums(v);
-        S.rcs[ch][0][r][c] = cs.s3;
-        S.rcs[ch][1][r][c] = cs.s5;
-        S.rcs[ch][2][r][c] = cs.s7;
-        S.rcs[ch][3][r][c] = cs.s9;
+            for (int k = 0; k < 13; ++k) v[k] = (double)pl[r0 + k][c];
+#pragma unroll
+            for (int j = 0; j < 5; ++j) {
+                const ColumnSums cs = column_sums_wide(v + j);
+                S.cs[src][0][r0 + j][c] = (double)cs.s3;
+                S.cs[src][1][r0 + j][c] = (double)cs.s5;
+                S.cs[src][2][r0 + j][c] = (double)cs.s7;
+                S.cs[src][3][r0 + j][c] = (double)cs.s9;
+                S.cs[src][4][r0 + j][c] = (double)cs.b16;
+            }
+        } else {
+            const int q = it - kWaItems;
+            const int ch = q / (2 * RC), rem = q % (2 * RC);
+            const int c = rem >> 1, r0 = (rem & 1) * 4;
+            double v[12];
+#pragma unroll
+            for (int k = 0; k < 12; ++k) v[k] = (double)S.hwr[ch][r0 + k][c];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const ColumnSums cs = column_sums_wide(v + j);
+                S.rcs[ch][0][r0 + j][c] = cs.s3;
+                S.rcs[ch][1][r0 + j][c] = cs.s5;
+                S.rcs[ch][2][r0 + j][c] = cs.s7;
+                S.rcs[ch][3][r0 + j][c] = cs.s9;
+            }
+        }
     }
     __syncthreads();
 
@@ -502,14 +551,11 @@ __global__ void __launch_bounds__(kStencilThreads)
 
     // decision bars (streaming.py:157-198), edge-replicated via the tile
     const int rad = p.radius;
-    int vl = 0, vr = 0, ha = 0, hb = 0;
-#pragma unroll
-    for (int d = -4; d <= 4; ++d) {
-        vl += S.auxt[ty + 4 + d][tx + 4 - rad] < thr;
-        vr += S.auxt[ty + 4 + d][tx + 4 + rad] < thr;
-        ha += S.auxt[ty + 4 - rad][tx + 4 + d] < thr;
-        hb += S.auxt[ty + 4 + rad][tx + 4 + d] < thr;
-    }
+    // bars of nine: rows ty..ty+8 of a column, columns tx..tx+8 of a row
+    const int vl = __popc((S.collow[tx + 4 - rad] >> ty) & 0x1FFu);
+    const int vr = __popc((S.collow[tx + 4 + rad] >> ty) & 0x1FFu);
+    const int ha = __popcll((S.rowlow[ty + 4 - rad] >> tx) & 0x1FFull);
+    const int hb = __popcll((S.rowlow[ty + 4 + rad] >> tx) & 0x1FFull);
     const int lim = p.count_limit;
     bool eligible = !(vl > lim || ha > lim || vr > lim || hb > lim);
     const float point_score = S.cw[ty][tx][3];
