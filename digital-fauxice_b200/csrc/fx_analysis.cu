@@ -448,7 +448,7 @@ __global__ void __launch_bounds__(kStencilThreads)
     for (int it = tid; it < kWaItems + kRgbItems; it += kStencilThreads) {
         if (it < kWaItems) {
             const int src = it / (2 * CC), rem = it % (2 * CC);
-            const int c = rem >> 1, r0 = (rem & 1) * 5;
+            const int c = rem % CC, r0 = (rem / CC) * 5;  // lanes on consecutive columns
             const float(*pl)[PC] = src ? S.hwa : S.hs;
             double v[13];
 #pragma unroll
@@ -465,7 +465,7 @@ __global__ void __launch_bounds__(kStencilThreads)
         } else {
             const int q = it - kWaItems;
             const int ch = q / (2 * RC), rem = q % (2 * RC);
-            const int c = rem >> 1, r0 = (rem & 1) * 4;
+            const int c = rem % RC, r0 = (rem / RC) * 4;
             double v[12];
 #pragma unroll
             for (int k = 0; k < 12; ++k) v[k] = (double)S.hwr[ch][r0 + k][c];
