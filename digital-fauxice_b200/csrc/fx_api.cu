@@ -257,10 +257,7 @@ static int enqueue_pass(fx_context *ctx, Slot &s, const Geometry &g, const fx_pa
     FX_CUDA(ctx, launch_analysis(d_in, g, ctx->lut, a.stages, p, a.aux, a.hs, a.hwa, a.hwr,
                                  (int64_t)g.prow * g.pitch, a.cand, a.meta, a.err, st, marks));
     WriterBuffers wb{a.seg_base, a.seg_amb, a.entries, a.pos, a.extra, a.counters,
-                     a.amb_capacity,
-                     reinterpret_cast<uint32_t *>(reinterpret_cast<char *>(s.h_ctr) +
-                                                  dev_counters_bytes() + 32),
-                     a.walk, g_per_wave, ctx->parallel_walk};
+                     a.amb_capacity, a.walk, g_per_wave, ctx->parallel_walk};
     FX_CUDA(ctx, launch_writer(g, a.meta, a.cand, d_in, ctx->lut, ctx->high, ctx->low, a.stages,
                                p, rng, wb, d_out, d_changed, a.err, st, marks));
     return FX_OK;

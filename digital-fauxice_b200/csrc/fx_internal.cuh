@@ -160,7 +160,6 @@ struct WriterBuffers {
     uint32_t *extra_after;         // capacity
     void *counters;                // DevCounters
     int64_t capacity;
-    uint32_t *h_n;                 // pinned host word for the channel count
     void *walk_scratch;            // walk_scratch_bytes(capacity, per_wave)
     int per_wave;                  // window blocks per wave (walk_per_wave of the SM count)
     bool parallel_walk;
@@ -192,7 +191,7 @@ cudaError_t walk_init();
 size_t walk_scratch_bytes(int64_t capacity, int per_wave);
 int walk_per_wave(int sms);
 cudaError_t launch_walk(const AmbEntry *entries, const uint32_t *pos, const uint32_t *n_ptr,
-                        int64_t capacity, uint32_t n, uint32_t s0, void *scratch, int per_wave,
+                        int64_t capacity, uint32_t s0, void *scratch, int per_wave,
                         bool parallel, uint32_t *extra_after, uint32_t *fallbacks_out,
                         unsigned long long *stats_out, cudaStream_t stream);
 void counters_to_host(const void *dev_copy, fx_counters *out);

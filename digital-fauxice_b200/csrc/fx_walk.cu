@@ -294,10 +294,11 @@ __global__ void __launch_bounds__(kWinThreads, kWinBlocksPerSM)
              const double *__restrict__ seg_mu, const double *__restrict__ seg_var,
              const WalkState *__restrict__ st, uint32_t wave, uint32_t per_wave, uint32_t t0,
              SegWindow *__restrict__ windows, uint32_t *__restrict__ table,
-             SegList *__restrict__ lists, WalkState *stats) {
+             SegList *__restrict__ lists, WalkState *stats, uint32_t serial_below) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     WindowSmem &S = *reinterpret_cast<WindowSmem *>(smem_raw);
     const uint32_t n = (uint32_t)min((int64_t)*n_ptr, capacity);
+    if (n < serial_below) return;  // the chain is walked serially instead
     const uint32_t seg0 = wave * per_wave;
     const uint32_t j = seg0 + blockIdx.x;
     const uint32_t i0 = j * kSegLen;
@@ -577,10 +578,12 @@ __global__ void __launch_bounds__(kResolveThreads)
               const uint32_t *__restrict__ n_ptr, int64_t capacity, WalkState *st,
               uint32_t wave, uint32_t per_wave, uint32_t t0,
               const SegWindow *__restrict__ windows, const uint32_t *__restrict__ table,
-              const SegList *__restrict__ lists, uint32_t *__restrict__ e_in_exact) {
+              const SegList *__restrict__ lists, uint32_t *__restrict__ e_in_exact,
+              uint32_t serial_below) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ResolveSmem &S = *reinterpret_cast<ResolveSmem *>(smem_raw);
     const uint32_t n = (uint32_t)min((int64_t)*n_ptr, capacity);
+    if (n < serial_below) return;
     const uint32_t segs = (n + kSegLen - 1) / kSegLen;
     const uint32_t here = min(per_wave, segs > wave * per_wave ? segs - wave * per_wave : 0u);
     const uint32_t chunks = (here + kResolveChunk - 1) / kResolveChunk;
@@ -673,7 +676,7 @@ __global__ void __launch_bounds__(kResolveThreads)
 // ---------------------------------------------------------------------------
 
 constexpr int kRewalkWarps = 4;
-constexpr int kRewalkChunk = 256;
+constexpr int kRewalkChunk = 128;  // 13.8 KB of staging per warp: every segment resident at once
 constexpr int kRewalkRing = 3;
 constexpr int kGroup = 8;
 
@@ -693,13 +696,16 @@ __device__ __forceinline__ void step(const uint4 &lw, const uint4 &ac, uint32_t 
 
 __global__ void __launch_bounds__(kRewalkWarps * 32)
     k_rewalk(const AmbEntry *__restrict__ entries, const uint32_t *__restrict__ pos,
-             const uint32_t *__restrict__ n_ptr, int64_t capacity, uint32_t seg_len,
+             const uint32_t *__restrict__ n_ptr, int64_t capacity, uint32_t parallel_seg_len,
              const uint32_t *__restrict__ e_in_exact, uint32_t t0,
-             uint32_t *__restrict__ extra_after) {
+             uint32_t *__restrict__ extra_after, uint32_t serial_below) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     RewalkSmem &S = *reinterpret_cast<RewalkSmem *>(smem_raw);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t n = (uint32_t)min((int64_t)*n_ptr, capacity);
+    // a short chain (or the serial mode) is one segment walked from E = 0
+    const bool serial = n < serial_below;
+    const uint32_t seg_len = serial ? (n > 0 ? n : 1u) : parallel_seg_len;
     const uint32_t j = blockIdx.x * kRewalkWarps + warp;
     const uint64_t i0_64 = (uint64_t)j * seg_len;
     if (i0_64 >= n) return;
@@ -723,7 +729,7 @@ __global__ void __launch_bounds__(kRewalkWarps * 32)
     };
 #pragma unroll
     for (int k = 0; k < kRewalkRing - 1; ++k) issue(k);
-    const uint32_t e_in = e_in_exact[j];
+    const uint32_t e_in = serial ? 0u : e_in_exact[j];
     uint32_t T = jump_t(t0, (uint64_t)pos[i0] + 1u + e_in);  // state at channel i0's first draw
     uint32_t E = e_in;
     uint32_t extra = 0u;
@@ -823,14 +829,15 @@ cudaError_t walk_init() {
                                 (int)sizeof(RewalkSmem));
 }
 
-// Enqueue the walk for `n` RNG-dependent channels (n already known on the
-// host).  `parallel` selects the speculative window walk; otherwise one warp
-// walks the whole chain.
+// Enqueue the walk.  The channel count stays on the device (n_ptr): the
+// launch shape is sized from the list capacity and every kernel exits early
+// beyond the count, so nothing waits for the host.  Chains shorter than
+// kSerialBelow (or every chain, when `parallel` is off) are walked by one
+// warp instead of the speculative windows.
 cudaError_t launch_walk(const AmbEntry *entries, const uint32_t *pos, const uint32_t *n_ptr,
-                        int64_t capacity, uint32_t n, uint32_t s0, void *scratch, int per_wave,
+                        int64_t capacity, uint32_t s0, void *scratch, int per_wave,
                         bool parallel, uint32_t *extra_after, uint32_t *fallbacks_out,
                         unsigned long long *stats_out, cudaStream_t stream) {
-    if (n == 0) return cudaGetLastError();
     const int64_t segs_max = walk_max_segments(capacity);
     char *p = reinterpret_cast<char *>(scratch);
     auto take = [&](size_t bytes) {
@@ -846,28 +853,25 @@ cudaError_t launch_walk(const AmbEntry *entries, const uint32_t *pos, const uint
     SegList *lists = (SegList *)take((size_t)per_wave * sizeof(SegList));
     WalkState *st = (WalkState *)take(sizeof(WalkState));
     const uint32_t t0 = (s0 & kLcgMask) << 8;
+    const uint32_t serial_below = parallel ? kSerialBelow : 0xFFFFFFFFu;
     cudaMemsetAsync(st, 0, sizeof(WalkState), stream);
-    if (!parallel || n < kSerialBelow) {
-        cudaMemsetAsync(e_in, 0, sizeof(uint32_t), stream);
-        k_rewalk<<<1, kRewalkWarps * 32, sizeof(RewalkSmem), stream>>>(
-            entries, pos, n_ptr, capacity, n, e_in, t0, extra_after);
-    } else {
-        const uint32_t segs = (n + kSegLen - 1) / kSegLen;
+    const uint32_t segs = (uint32_t)segs_max;
+    if (parallel) {
         const uint32_t waves = (segs + per_wave - 1) / per_wave;
         k_seg_prob<<<segs, 256, 0, stream>>>(entries, n_ptr, capacity, mu, var);
         for (uint32_t w = 0; w < waves; ++w) {
             const uint32_t blocks = min((uint32_t)per_wave, segs - w * per_wave);
             k_window<<<blocks, kWinThreads, sizeof(WindowSmem), stream>>>(
                 entries, pos, n_ptr, capacity, mu, var, st, w, per_wave, t0, windows, table,
-                lists, st);
-            k_resolve<<<1, kResolveThreads, resolve_smem_bytes(), stream>>>(entries, pos, n_ptr, capacity, st,
-                                                               w, per_wave, t0, windows, table,
-                                                               lists, e_in);
+                lists, st, serial_below);
+            k_resolve<<<1, kResolveThreads, resolve_smem_bytes(), stream>>>(
+                entries, pos, n_ptr, capacity, st, w, per_wave, t0, windows, table, lists, e_in,
+                serial_below);
         }
-        k_rewalk<<<(segs + kRewalkWarps - 1) / kRewalkWarps, kRewalkWarps * 32,
-                   sizeof(RewalkSmem), stream>>>(entries, pos, n_ptr, capacity, kSegLen, e_in, t0,
-                                                 extra_after);
     }
+    k_rewalk<<<(segs + kRewalkWarps - 1) / kRewalkWarps, kRewalkWarps * 32, sizeof(RewalkSmem),
+               stream>>>(entries, pos, n_ptr, capacity, kSegLen, e_in, t0, extra_after,
+                         serial_below);
     if (fallbacks_out)
         cudaMemcpyAsync(fallbacks_out, &st->fallbacks, sizeof(uint32_t), cudaMemcpyDeviceToDevice,
                         stream);

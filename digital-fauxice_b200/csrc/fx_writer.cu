@@ -657,14 +657,9 @@ cudaError_t launch_writer(const Geometry &g, const uint8_t *meta, const double *
     k_coef<<<1184, 256, 0, stream>>>(b.entries, b.pos, n_amb, b.capacity, cand, g.w, rgbi, lut, p,
                                      err);
     marks.mark(5, stream);
-    // The walk's launch shape depends on the channel count: read it back.
-    cudaMemcpyAsync(b.h_n, n_amb, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream);
-    cudaError_t e = cudaStreamSynchronize(stream);
-    if (e != cudaSuccess) return e;
-    const uint32_t n = (uint32_t)std::min<int64_t>((int64_t)*b.h_n, b.capacity);
-    e = launch_walk(b.entries, b.pos, n_amb, b.capacity, n, s0, b.walk_scratch, b.per_wave,
-                    b.parallel_walk, b.extra_after, &ctr->walk_fallbacks, ctr->walk_stats,
-                    stream);
+    cudaError_t e = launch_walk(b.entries, b.pos, n_amb, b.capacity, s0, b.walk_scratch,
+                                b.per_wave, b.parallel_walk, b.extra_after, &ctr->walk_fallbacks,
+                                ctr->walk_stats, stream);
     if (e != cudaSuccess) return e;
     marks.mark(6, stream);
     k_startup_counts<<<1, 256, 0, stream>>>(meta, g.w, b.extra_after, s0 & kLcgMask, ctr,
