@@ -130,6 +130,12 @@ struct Slot {
     std::vector<fx_stage> stages;
     bool has_stages = false;
     Geometry g{};
+    // device-buffer request (fx_submit_device): caller-owned device memory
+    bool device = false;
+    const uint16_t *d_in = nullptr;
+    uint16_t *d_out = nullptr;
+    float *d_score = nullptr;
+    uint8_t *d_changed = nullptr;
 };
 
 }  // namespace fx
@@ -138,6 +144,7 @@ struct fx_context {
     int device = 0;
     bool profile = false;
     bool parallel_walk = true;
+    int walk_wave = 0;  // window segments per wave; 0: g_per_wave (two per SM)
     std::vector<std::vector<cudaEvent_t>> pending;  // recorded, not yet read
     std::vector<std::vector<cudaEvent_t>> spare;
     double profile_ms[fx::kProfileStages] = {0};
@@ -256,8 +263,11 @@ static int enqueue_pass(fx_context *ctx, Slot &s, const Geometry &g, const fx_pa
     marks.mark(1, st);
     FX_CUDA(ctx, launch_analysis(d_in, g, ctx->lut, a.stages, p, a.aux, a.hs, a.hwa, a.hwr,
                                  (int64_t)g.prow * g.pitch, a.cand, a.meta, a.err, st, marks));
+    // the walk scratch is sized for g_per_wave; a narrower wave uses part of it
+    const int wave = (ctx->walk_wave > 0 && ctx->walk_wave < g_per_wave) ? ctx->walk_wave
+                                                                         : g_per_wave;
     WriterBuffers wb{a.seg_base, a.seg_amb, a.entries, a.pos, a.extra, a.counters,
-                     a.amb_capacity, a.walk, g_per_wave, ctx->parallel_walk};
+                     a.amb_capacity, a.walk, wave, ctx->parallel_walk};
     FX_CUDA(ctx, launch_writer(g, a.meta, a.cand, d_in, ctx->lut, ctx->high, ctx->low, a.stages,
                                p, rng, wb, d_out, d_changed, a.err, st, marks));
     return FX_OK;
@@ -612,6 +622,13 @@ FX_API int fx_set_parallel_walk(fx_context *ctx, int enable) {
     return FX_OK;
 }
 
+FX_API int fx_set_walk_wave(fx_context *ctx, int32_t segments) {
+    if (!ctx || segments < 0) return FX_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    ctx->walk_wave = segments;
+    return FX_OK;
+}
+
 FX_API int fx_set_slots(fx_context *ctx, int32_t slots) {
     if (!ctx || slots < 1 || slots > 64) return FX_ERR_INVALID_ARGUMENT;
     std::lock_guard<std::mutex> lock(ctx->mu);
@@ -656,6 +673,7 @@ FX_API int fx_submit(fx_context *ctx, const fx_frame *f, int64_t *ticket) {
         s.h_out_bytes = out_bytes;
     }
     std::memcpy(s.h_in, f->main_rgbi, in_bytes);
+    s.device = false;
     s.frame = *f;
     s.params = *f->params;
     s.frame.params = &s.params;
@@ -680,6 +698,70 @@ FX_API int fx_submit(fx_context *ctx, const fx_frame *f, int64_t *ticket) {
                                  cudaMemcpyDeviceToHost, s.stream));
     FX_CUDA(ctx, cudaMemcpyAsync(hc + dev_counters_bytes(), s.arena.err, 4,
                                  cudaMemcpyDeviceToHost, s.stream));
+    FX_CUDA(ctx, cudaEventRecord(s.done, s.stream));
+    s.busy = true;
+    s.ticket = ctx->next_ticket++;
+    *ticket = s.ticket;
+    return FX_OK;
+}
+
+// Score plane and counters of a device-buffer request, enqueued on the
+// slot's stream after its pass.
+static int copy_device_results(fx_context *ctx, Slot &s) {
+    const Geometry &g = s.g;
+    if (s.d_score)
+        FX_CUDA(ctx, cudaMemcpy2DAsync(s.d_score, (size_t)g.w * 4, s.arena.hs + g.padded_index(0, 0),
+                                       (size_t)g.pitch * 4, (size_t)g.w * 4, g.h,
+                                       cudaMemcpyDeviceToDevice, s.stream));
+    char *hc = reinterpret_cast<char *>(s.h_ctr);
+    FX_CUDA(ctx, cudaMemcpyAsync(hc, s.arena.counters, dev_counters_bytes(),
+                                 cudaMemcpyDeviceToHost, s.stream));
+    FX_CUDA(ctx, cudaMemcpyAsync(hc + dev_counters_bytes(), s.arena.err, 4,
+                                 cudaMemcpyDeviceToHost, s.stream));
+    return FX_OK;
+}
+
+FX_API int fx_submit_device(fx_context *ctx, const uint16_t *d_rgbi, int32_t h, int32_t w,
+                            const fx_params *params, const fx_stage *stages, uint32_t rng,
+                            uint16_t *d_out, float *d_score, uint8_t *d_changed,
+                            int64_t *ticket) {
+    if (!ctx || !d_rgbi || !d_out || !ticket) return FX_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    cudaSetDevice(ctx->device);
+    int rc = check_frame(ctx, params, h, w);
+    if (rc) return rc;
+    if (!stages && w < 8)
+        return fail(ctx, FX_ERR_GEOMETRY, "main RGBI frame has no complete producer cell");
+    Slot *slot = nullptr;
+    for (Slot &s : ctx->slots)
+        if (!s.busy) {
+            slot = &s;
+            break;
+        }
+    if (!slot) return fail(ctx, FX_PENDING, "no free slot");
+    Slot &s = *slot;
+    const Geometry g = make_geometry(h, w);
+    rc = ensure_arena(ctx, s, g, default_amb_capacity(g));
+    if (rc) return rc;
+    s.frame = fx_frame{};
+    s.frame.height = h;
+    s.frame.width = w;
+    s.frame.rng_state = rng;
+    s.params = *params;
+    s.frame.params = &s.params;
+    s.has_stages = stages != nullptr;
+    if (s.has_stages) s.stages.assign(stages, stages + (g.h + 6));
+    s.g = g;
+    s.device = true;
+    s.d_in = d_rgbi;
+    s.d_out = d_out;
+    s.d_score = d_score;
+    s.d_changed = d_changed;
+    rc = enqueue_pass(ctx, s, g, s.params, s.has_stages ? s.stages.data() : nullptr, rng, d_rgbi,
+                      d_out, d_changed, false);
+    if (rc) return rc;
+    rc = copy_device_results(ctx, s);
+    if (rc) return rc;
     FX_CUDA(ctx, cudaEventRecord(s.done, s.stream));
     s.busy = true;
     s.ticket = ctx->next_ticket++;
@@ -723,7 +805,22 @@ FX_API int fx_wait(fx_context *ctx, int64_t ticket, int64_t timeout_ns, fx_count
                 std::memcpy(&err, hc + dev_counters_bytes(), 4);
                 bool overflow;
                 int rc = finish_counters(ctx, s, hc, err, counters, &overflow);
-                if (!rc && overflow) {
+                if (!rc && overflow && s.device) {
+                    // rare: more RNG-dependent channels than the default
+                    // capacity; rerun synchronously with room for all
+                    const int64_t cap = (int64_t)counters_n_amb(hc) + 1024;
+                    rc = ensure_arena(ctx, s, s.g, cap);
+                    if (!rc)
+                        rc = enqueue_pass(ctx, s, s.g, s.params,
+                                          s.has_stages ? s.stages.data() : nullptr,
+                                          s.frame.rng_state, s.d_in, s.d_out, s.d_changed, false);
+                    if (!rc) rc = copy_device_results(ctx, s);
+                    if (!rc && cudaStreamSynchronize(s.stream) != cudaSuccess)
+                        rc = fail(ctx, FX_ERR_CUDA, "retry failed");
+                    std::memcpy(&err, hc + dev_counters_bytes(), 4);
+                    if (!rc) rc = finish_counters(ctx, s, hc, err, counters, &overflow);
+                    if (!rc && overflow) rc = fail(ctx, FX_ERR_INTERNAL, "capacity retry");
+                } else if (!rc && overflow) {
                     // rare: more RNG-dependent channels than the default
                     // capacity; rerun synchronously with room for all
                     fx_frame f = s.frame;
@@ -759,7 +856,7 @@ FX_API int fx_wait(fx_context *ctx, int64_t ticket, int64_t timeout_ns, fx_count
                         if (!rc && overflow) rc = fail(ctx, FX_ERR_INTERNAL, "capacity retry");
                     }
                 }
-                if (!rc) {
+                if (!rc && !s.device) {
                     const char *ho = reinterpret_cast<const char *>(s.h_out);
                     std::memcpy(s.frame.rgb_out, ho, px * 6);
                     if (s.frame.score_out) std::memcpy(s.frame.score_out, ho + px * 6, px * 4);

@@ -1,0 +1,208 @@
+"""Batched processing: many frames of uneven sizes in flight on one B200.
+
+No counterpart in the reference, which processes one job per call.  Each
+frame is an independent job (its own prelude and its own RNG chain from the
+job's initial state), so frames can run concurrently without changing any
+result: up to ``slots`` frames are in flight, each in its own context slot
+with its own CUDA stream and device buffers, and the kernels of different
+frames overlap on the device (one frame's latency-bound walk and one-block
+scans leave most SMs to the others).
+
+* :func:`run_device_batch` -- frames already in device memory (pointers),
+  outputs written to device memory; the measurement path.
+* :func:`process_batch` -- :class:`ProcessingJob` objects in, reference-shaped
+  :class:`ProcessingResult` objects out (host buffers), same validation and
+  fail-closed behaviour as :func:`fauxice_b200.engine.process_b200`.
+* :func:`tune_slots` -- picks the slot count that maximises throughput on a
+  sample of the workload (the batching autotuner).
+"""
+
+from __future__ import annotations
+
+import ctypes
+import time
+from collections import deque
+from dataclasses import dataclass
+from typing import Iterable, Sequence
+
+import numpy as np
+
+from . import _lib
+from .engine import (
+    NIKON_PE_INITIAL_STATE,
+    FrameOutcome,
+    ProcessingResult,
+    context,
+    make_diagnostics,
+    raise_library_error,
+    reduce_prepass,
+    replay_result,
+)
+from .profile import DEFAULT_PROFILE
+
+FX_PENDING = 18
+
+
+@dataclass
+class DeviceFrame:
+    """One device-resident frame: RGBI input and RGB16 output (device
+    pointers as integers), optional score plane and changed mask."""
+
+    rgbi: int
+    height: int
+    width: int
+    rgb_out: int
+    score_out: int = 0
+    changed_out: int = 0
+    rng_state: int = NIKON_PE_INITIAL_STATE
+
+
+def _check(ctx: _lib.Context, status: int) -> None:
+    if status:
+        try:
+            ctx.check(status)
+        except _lib.LibraryError as error:
+            raise_library_error(error)
+
+
+def set_slots(ctx: _lib.Context, slots: int) -> None:
+    with ctx.lock:
+        _check(ctx, _lib.load().fx_set_slots(ctx.handle, int(slots)))
+
+
+def set_walk_wave(ctx: _lib.Context, segments: int) -> None:
+    """Segments per speculative walk wave (0: the default, two per SM)."""
+
+    with ctx.lock:
+        _check(ctx, _lib.load().fx_set_walk_wave(ctx.handle, int(segments)))
+
+
+def run_device_batch(ctx: _lib.Context, frames: Sequence[DeviceFrame], *, slots: int = 4,
+                     params: _lib.FxParams | None = None) -> list[_lib.FxCounters]:
+    """Process device-resident frames with up to ``slots`` in flight.
+
+    Frames are submitted in order; when every slot is busy the oldest
+    request is waited for.  Returns the counters of every frame, in order.
+    """
+
+    lib = _lib.load()
+    set_slots(ctx, slots)
+    if params is None:
+        params = DEFAULT_PROFILE.hot_path_parameters().to_c()
+    pending: deque[tuple[int, int]] = deque()  # (frame index, ticket)
+    results: list[_lib.FxCounters | None] = [None] * len(frames)
+
+    def wait_oldest() -> None:
+        index, ticket = pending.popleft()
+        counters = _lib.FxCounters()
+        status = lib.fx_wait(ctx.handle, ticket, -1, ctypes.byref(counters))
+        _check(ctx, status)
+        results[index] = counters
+
+    for index, f in enumerate(frames):
+        if len(pending) >= slots:  # the context may hold more slots than asked for
+            wait_oldest()
+        while True:
+            ticket = ctypes.c_int64()
+            with ctx.lock:
+                status = lib.fx_submit_device(
+                    ctx.handle, ctypes.c_void_p(f.rgbi), f.height, f.width, ctypes.byref(params),
+                    None, int(f.rng_state) & 0xFFFFFF, ctypes.c_void_p(f.rgb_out),
+                    ctypes.c_void_p(f.score_out or None), ctypes.c_void_p(f.changed_out or None),
+                    ctypes.byref(ticket))
+            if status == FX_PENDING and pending:
+                wait_oldest()
+                continue
+            _check(ctx, status)
+            pending.append((index, ticket.value))
+            break
+    while pending:
+        wait_oldest()
+    return results  # type: ignore[return-value]
+
+
+def tune_slots(ctx: _lib.Context, frames: Sequence[DeviceFrame],
+               candidates: Iterable[int] = (1, 2, 4, 8), waves: Iterable[int] = (0,),
+               repeats: int = 1) -> tuple[tuple[int, int], dict]:
+    """Time the sample batch at each (slots, walk wave) pair; leave the best
+    walk wave set and return it with the measured seconds of every pair
+    (after one warm-up run that allocates the slots' buffers)."""
+
+    candidates, waves = tuple(candidates), tuple(waves)
+    timings: dict[tuple[int, int], float] = {}
+    run_device_batch(ctx, frames, slots=max(candidates))
+    for wave in waves:
+        set_walk_wave(ctx, wave)
+        for slots in candidates:
+            best = float("inf")
+            for _ in range(repeats):
+                t0 = time.perf_counter()
+                run_device_batch(ctx, frames, slots=slots)
+                best = min(best, time.perf_counter() - t0)
+            timings[(slots, wave)] = best
+    choice = min(timings, key=timings.get)
+    set_walk_wave(ctx, choice[1])
+    return choice, timings
+
+
+def process_batch(jobs: Sequence, *, slots: int = 4, export_diagnostics: bool = False,
+                  device: int = 0) -> list[ProcessingResult]:
+    """Process many jobs with up to ``slots`` frames in flight.
+
+    Every job is validated (and its prepass record checked) before any is
+    submitted, so a bad job fails the call before device work starts.  Each
+    result equals :func:`fauxice_b200.engine.process_b200` on the same job.
+    """
+
+    for job in jobs:
+        DEFAULT_PROFILE.validate_job(job)
+    ctx = context(device)
+    for job in jobs:
+        payload, _, _ = reduce_prepass(ctx, job.acquisition.prepass.pixels)
+        DEFAULT_PROFILE.check_prepass_record(payload)
+    lib = _lib.load()
+    set_slots(ctx, slots)
+    params = DEFAULT_PROFILE.hot_path_parameters().to_c()
+    floor = DEFAULT_PROFILE.score_floor()
+
+    inflight: deque[tuple[int, int, object]] = deque()
+    results: list[ProcessingResult | None] = [None] * len(jobs)
+
+    def finish_oldest() -> None:
+        index, ticket, keep = inflight.popleft()
+        counters = _lib.FxCounters()
+        status = lib.fx_wait(ctx.handle, ticket, -1, ctypes.byref(counters))
+        _check(ctx, status)
+        _, out, score, changed = keep
+        outcome = FrameOutcome(out, counters, score, changed)
+        diagnostics = make_diagnostics(outcome, floor) if export_diagnostics else None
+        results[index] = ProcessingResult(output_rgb16=out, replay=replay_result(outcome),
+                                          profile_id=DEFAULT_PROFILE.profile_id,
+                                          diagnostics=diagnostics)
+
+    for index, job in enumerate(jobs):
+        px = np.ascontiguousarray(job.acquisition.main.pixels, dtype=np.uint16)
+        h, w = px.shape[:2]
+        out = np.empty((h, w, 3), np.uint16)
+        score = np.empty((h, w), np.float32) if export_diagnostics else None
+        changed = np.empty((h, w), np.uint8) if export_diagnostics else None
+        frame = _lib.FxFrame(
+            main_rgbi=px.ctypes.data, height=h, width=w, params=ctypes.pointer(params),
+            stages=None, rng_state=NIKON_PE_INITIAL_STATE, rgb_out=out.ctypes.data,
+            score_out=score.ctypes.data if score is not None else None,
+            changed_out=changed.ctypes.data if changed is not None else None)
+        if len(inflight) >= slots:
+            finish_oldest()
+        while True:
+            ticket = ctypes.c_int64()
+            with ctx.lock:
+                status = lib.fx_submit(ctx.handle, ctypes.byref(frame), ctypes.byref(ticket))
+            if status == FX_PENDING and inflight:
+                finish_oldest()
+                continue
+            _check(ctx, status)
+            inflight.append((index, ticket.value, (px, out, score, changed)))
+            break
+    while inflight:
+        finish_oldest()
+    return results  # type: ignore[return-value]

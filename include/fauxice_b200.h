@@ -192,7 +192,21 @@ FX_API int fx_set_slots(fx_context *ctx, int32_t slots);
 /* 1 (default): the speculative parallel walk; 0: one warp walks the whole
  * chain (leaves the rest of the GPU to other frames' kernels). */
 FX_API int fx_set_parallel_walk(fx_context *ctx, int enable);
+/* Segments of 4096 RNG-dependent channels walked speculatively per wave
+ * (0, the default: two per SM).  Fewer segments per wave mean narrower
+ * candidate windows (less total work, for throughput when several frames
+ * are in flight) and more waves (longer latency for one frame). */
+FX_API int fx_set_walk_wave(fx_context *ctx, int32_t segments);
 FX_API int fx_submit(fx_context *ctx, const fx_frame *frame, int64_t *ticket);
+/* fx_submit for a frame already in device memory: the pass is enqueued on
+ * a free slot's stream and writes d_rgb_out / d_score_out / d_changed_out
+ * (device pointers, NULL for the optional planes) directly.  The caller
+ * keeps every buffer valid until fx_wait returns for the ticket.
+ * FX_PENDING when every slot is busy. */
+FX_API int fx_submit_device(fx_context *ctx, const uint16_t *d_rgbi, int32_t height,
+                            int32_t width, const fx_params *params, const fx_stage *stages,
+                            uint32_t rng_state, uint16_t *d_rgb_out, float *d_score_out,
+                            uint8_t *d_changed_out, int64_t *ticket);
 FX_API int fx_poll(fx_context *ctx, int64_t ticket);
 FX_API int fx_wait(fx_context *ctx, int64_t ticket, int64_t timeout_ns, fx_counters *counters);
 
