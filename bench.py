@@ -47,6 +47,52 @@ SEED = 2
 # per RNG-dependent channel.
 STENCIL_BYTES_PER_PIXEL = 33
 WALK_BYTES_PER_CHANNEL = 36
+BATCH_FRAMES = 16          # uneven sizes, seeds 100..115
+SERVE_RATES = (2.0, 8.0, 32.0)
+STENCIL_PROFILE = os.path.join(ROOT, "profiles", "k_stencil_native_frame.md")
+
+
+def launches_per_frame(h: int, w: int, per_wave: int) -> int:
+    """Kernel launches of one plain pass (the library's launch sequence):
+    producer 5, planes 2, stencil 1, startup 1, chain 4, walk 1 + 2 per wave
+    + 1, apply 3.  Waves are sized from the RNG-dependent list capacity."""
+
+    sites = 6 * w + h * w
+    capacity = max(65536, sites // 2)
+    segments = (capacity + 4095) // 4096 + 1
+    waves = (segments + per_wave - 1) // per_wave
+    return 18 + 2 * waves
+
+
+def stencil_traffic():
+    """DRAM bytes per k_stencil launch from the committed ncu summary."""
+
+    try:
+        for line in open(STENCIL_PROFILE):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return int(line.split(":")[1].strip())
+    except OSError:
+        pass
+    return None
+
+
+def generate_batch(count: int):
+    """Frames of the batched workload, generated in spawn workers (before
+    any CUDA call in this process)."""
+
+    import multiprocessing as mp
+
+    with mp.get_context("spawn").Pool(min(count, os.cpu_count() or 1)) as pool:
+        return pool.map(_batch_frame, range(count))
+
+
+def _batch_frame(index: int):
+    for _p in (ROOT, os.path.join(ROOT, "digital-fauxice_b200")):
+        if _p not in sys.path:
+            sys.path.insert(0, _p)
+    from fauxice_b200 import synthetic
+
+    return synthetic.batch_frame(index)[0]
 
 
 def parse():
@@ -57,6 +103,10 @@ def parse():
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched and serving runs")
+    ap.add_argument("--batch-steps", type=int, default=3)
+    ap.add_argument("--serve-seconds", type=float, default=6.0,
+                    help="arrival window per request rate (the workload's 120 s, shortened)")
     return ap.parse_args()
 
 
@@ -234,7 +284,7 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
-def run_b200(args, world, rank, local):
+def run_b200(args, world, rank, local, frames=None):
     import torch
 
     from fauxice_b200 import _lib, engine, synthetic
@@ -307,24 +357,26 @@ def run_b200(args, world, rank, local):
     mp = h * w / 1e6
     value = world * args.steps * mp / (elapsed_ms / 1000.0)
 
-    # roofline of the dominant stage (HBM-bound kinds)
+    # roofline of the largest single kernel launch (k_stencil): algorithmic
+    # bytes of the a1-a10 stage, 33 B per pixel, over its CUDA-event time
     peak, peak_kind = load_peaks()
-    dominant = max(("stencil", "walk"), key=lambda k: stages[k])
-    if dominant == "stencil":
-        bytes_per_launch = STENCIL_BYTES_PER_PIXEL * h * w
-    else:
-        bytes_per_launch = WALK_BYTES_PER_CHANNEL * counters.rng_dependent
-    achieved = bytes_per_launch / (stages[dominant] / 1000.0) / 1e9
+    bytes_per_launch = STENCIL_BYTES_PER_PIXEL * h * w
+    achieved = bytes_per_launch / (stages["stencil"] / 1000.0) / 1e9
     roofline = {
-        "kernel": {"stencil": "k_stencil", "walk": "k_walk"}[dominant],
+        "kernel": "k_stencil",
         "bound": "hbm",
         "achieved": round(achieved, 2),
         "peak": peak,
         "unit": "GB/s",
         "frac": round(achieved / peak, 5),
         "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
-        "traffic": None,
+        "traffic": stencil_traffic(),
+        "algorithmic_bytes_per_launch": bytes_per_launch,
         "stage_ms": {k: round(v, 4) for k, v in stages.items()},
+        "walk": {"bytes_per_channel": WALK_BYTES_PER_CHANNEL,
+                 "achieved_gbs": round(WALK_BYTES_PER_CHANNEL * counters.rng_dependent
+                                       / (stages["walk"] / 1000.0) / 1e9, 2),
+                 "note": "dependent integer chain (latency-bound), not HBM-bound"},
     }
 
     # end to end through the public API, host buffers in and out
@@ -378,14 +430,120 @@ def run_b200(args, world, rank, local):
             "cpu_baseline": cpu,
             "e2e": e2e,
             "clocks": clocks,
-            "gpu_launches": 17 * args.steps,
+            "gpu_launches": launches_per_frame(h, w, 2 * torch.cuda.get_device_properties(
+                local).multi_processor_count) * args.steps,
             "rng_dependent_channels": int(counters.rng_dependent),
             "walk_fallback_segments": int(counters.walk_fallbacks),
             "walk_candidate_steps": int(counters.walk_candidate_steps),
             "walk_candidates": int(counters.walk_candidates),
             "walk_survivors": int(counters.walk_survivors),
         }
+        if frames is not None:
+            line["batched"] = run_batched(ctx, frames, args, golden)
+            line["serving"] = run_serving(ctx, frames, args)
         print(json.dumps(line), flush=True)
+
+
+def run_batched(ctx, frames, args, golden):
+    """The batched workload: 16 frames of uneven sizes, device-resident.
+
+    Timed once with one frame in flight (the plain path on this mix) and once
+    with the autotuned number of slots; every batched output is compared
+    with its one-at-a-time output, and frames 0-4 (seeds 100-104) with the
+    reference's recorded results.
+    """
+
+    import hashlib
+
+    import torch
+
+    from fauxice_b200 import batch
+
+    d_in = [torch.from_numpy(np.ascontiguousarray(f).view(np.int16)).to("cuda") for f in frames]
+    plain_out = [torch.empty((f.shape[0], f.shape[1], 3), dtype=torch.int16, device="cuda")
+                 for f in frames]
+    outs = [torch.empty_like(o) for o in plain_out]
+    mp = sum(f.shape[0] * f.shape[1] for f in frames) / 1e6
+    as_jobs = lambda dst: [batch.DeviceFrame(d.data_ptr(), f.shape[0], f.shape[1], o.data_ptr())
+                           for f, d, o in zip(frames, d_in, dst)]
+
+    def timed(jobs, slots):
+        times = []
+        for _ in range(args.batch_steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            batch.run_device_batch(ctx, jobs, slots=slots)
+            torch.cuda.synchronize()
+            times.append(time.perf_counter() - t0)
+        return min(times), sorted(times)[len(times) // 2]
+
+    batch.set_walk_wave(ctx, 0)
+    batch.run_device_batch(ctx, as_jobs(plain_out), slots=1)  # warm
+    plain_best, plain_med = timed(as_jobs(plain_out), 1)
+    (slots, wave), tuning = batch.tune_slots(ctx, as_jobs(outs), candidates=(2, 4, 8),
+                                             waves=(0, 148))
+    best, med = timed(as_jobs(outs), slots)
+    same = all(torch.equal(a, b) for a, b in zip(outs, plain_out))
+    ref_ok = []
+    for i in range(5):
+        host = outs[i].cpu().numpy().view(np.uint16)
+        digest = hashlib.sha256(host.astype("<u2").tobytes()).hexdigest()
+        ref_ok.append(digest == golden["jobs"][f"batch_{i}"]["output_sha256"])
+    batch.set_walk_wave(ctx, 0)
+    return {
+        "workload": f"{len(frames)} frames cycling 5782x3946, 3946x5782, 2892x1973, 1024x768, "
+                    "4000x2700 (seeds 100-115, ~0.5% defects), device-resident",
+        "value": round(mp / med, 1), "unit": "MP/s", "megapixels": round(mp, 2),
+        "ms_per_step": round(1000 * med, 2), "steps": args.batch_steps,
+        "plain_same_mix": {"value": round(mp / plain_med, 1), "unit": "MP/s",
+                           "ms_per_step": round(1000 * plain_med, 2), "slots": 1},
+        "slots": slots, "walk_wave": wave or "default (2 per SM)",
+        "tuning_ms": {f"slots={k[0]},wave={k[1] or 'default'}": round(1000 * v, 1)
+                      for k, v in tuning.items()},
+        "timing": "host clock around the whole batch, synchronize on both sides (frames run on "
+                  "several library streams)",
+        "bit_exact_vs_single_frame": bool(same),
+        "bit_exact_vs_reference_frames_0_4": bool(all(ref_ok)),
+    }
+
+
+def run_serving(ctx, frames, args):
+    """Requests at Poisson rates 2, 8 and 32 per second over a shortened
+    window; sizes 50% 5782x3946, 30% 2892x1973, 20% seeded crops of
+    U[256, 2048]^2 from the batch frames; inputs in pinned host memory."""
+
+    import torch
+
+    from fauxice_b200 import serve
+
+    full = [f for f in frames if f.shape[:2] == (5782, 3946)]
+    half = [f for f in frames if f.shape[:2] == (2892, 1973)]
+    rng = np.random.default_rng(500)
+    crops = []
+    for k in range(6):
+        src = frames[k % len(frames)]
+        ch, cw = (int(v) for v in rng.integers(256, 2049, size=2))
+        ch, cw = min(ch, src.shape[0]), min(cw, src.shape[1])
+        y = int(rng.integers(0, src.shape[0] - ch + 1))
+        x = int(rng.integers(0, src.shape[1] - cw + 1))
+        crops.append(np.ascontiguousarray(src[y:y + ch, x:x + cw]))
+    pinned = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.int16)).pin_memory()
+    pools = [[pinned(f) for f in full], [pinned(f) for f in half], [pinned(f) for f in crops]]
+    out = {"workload": "Poisson arrivals, 50% 5782x3946 / 30% 2892x1973 / 20% crops "
+                       f"U[256,2048]^2, {args.serve_seconds:g} s per rate (of the 120 s "
+                       "workload), latency from arrival to device completion, 4 slots",
+           "rates": {}}
+    for r_i, rate in enumerate(SERVE_RATES):
+        arrivals = serve.poisson_arrivals(rate, args.serve_seconds, seed=600 + r_i)
+        pick = np.random.default_rng(700 + r_i)
+        requests = []
+        for t in arrivals:
+            u = pick.random()
+            pool = pools[0] if u < 0.5 else (pools[1] if u < 0.8 else pools[2])
+            requests.append(serve.Request(float(t), pool[int(pick.integers(0, len(pool)))]))
+        report = serve.serve(ctx, requests, slots=4)
+        out["rates"][f"{rate:g}/s"] = report.summary()
+    return out
 
 
 def main():
@@ -394,7 +552,10 @@ def main():
     if args.impl == "reference":
         run_reference(args, world, rank)
     else:
-        run_b200(args, world, rank, local)
+        frames = None
+        if world == 1 and not args.no_batch:
+            frames = generate_batch(BATCH_FRAMES)
+        run_b200(args, world, rank, local, frames)
     if world > 1:
         import torch.distributed as dist
 
