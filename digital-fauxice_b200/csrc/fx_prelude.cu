@@ -56,7 +56,6 @@ __host__ __device__ inline int setter_stage(float p1, float p2, float p3, float 
 // ---------------------------------------------------------------------------
 
 struct ProducerBuffers {
-    uint8_t *failpos;      // [nb][cells]
     uint8_t *cell_ok;      // [ne][cells]
     double2 *terms;        // [ne][cells][4]  (term, ratio * term)
     double *row_sums;      // [3][h]  visible, infrared, weight
@@ -95,45 +94,28 @@ __device__ __forceinline__ void center_quadrants(const float q[4], float out[4])
     for (int i = 0; i < 4; ++i) out[i] = (float)((double)q[i] - (double)mean);
 }
 
-__global__ void k_producer_cells(const uint16_t *__restrict__ rgbi, int h, int w, int cells,
-                                 const float *__restrict__ lut, ProducerBuffers b) {
-    const int nb = (h + 7) / 8;
-    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= (int64_t)nb * cells) return;
-    const int blk = (int)(idx / cells), cell = (int)(idx % cells);
-    const int r0 = blk * 8, rows = min(8, h - r0);
-    const double thr = (double)kIrThreshold;
-    int failpos = 64;
-    for (int i = 0; i < rows && failpos == 64; ++i) {
-        for (int j = 0; j < 8; ++j) {
-            const uint32_t ir = (uint32_t)rgbi[((int64_t)(r0 + i) * w + cell * 8 + j) * 4 + 3];
-            if (!(thr < (double)ir)) {
-                failpos = i * 8 + j;
-                break;
-            }
-        }
-    }
-    b.failpos[idx] = (uint8_t)failpos;
-    if (rows < 8) return;  // no complete epoch in a partial final block
-    const int64_t e_idx = (int64_t)blk * cells + cell;
-    if (failpos != 64) {
-        b.cell_ok[e_idx] = 0;
-        return;
-    }
-    b.cell_ok[e_idx] = 1;
-    float vr[8][8], ir[8][8];
+// The four quadrant terms of one complete cell whose eight rows all pass the
+// IR test (_scale_epoch_additions, producer_parameters.py:183-263).
+// raw(i, j) gives the cell's RGBI sample at row i, column j (uint2).
+template <class Raw>
+__device__ void cell_terms(Raw raw, const float *__restrict__ lut, double2 out[4]) {
     float raw_sum = 0.0f;
-    for (int i = 0; i < 8; ++i)
-        for (int j = 0; j < 8; ++j) {
-            const uint16_t *px = rgbi + ((int64_t)(r0 + i) * w + cell * 8 + j) * 4;
-            vr[i][j] = __ldg(lut + px[0]);
-            ir[i][j] = __ldg(lut + px[3]);
-            raw_sum = (float)((double)raw_sum + (double)px[3]);
-        }
+#pragma unroll 8
+    for (int i = 0; i < 64; ++i)
+        raw_sum = (float)((double)raw_sum + (double)(raw(i >> 3, i & 7).y >> 16));
     const int qy[4] = {0, 0, 4, 4}, qx[4] = {0, 4, 0, 4};
     float vq[4], iq[4], vd[4], id[4];
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
+        float vr[8][8], ir[8][8];  // only the quadrant's 4x4 entries are touched
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const uint2 px = raw(qy[q] + i, qx[q] + j);
+                vr[qy[q] + i][qx[q] + j] = __ldg(lut + (px.x & 0xFFFFu));
+                ir[qy[q] + i][qx[q] + j] = __ldg(lut + (px.y >> 16));
+            }
         vq[q] = quadrant_tree(vr, qy[q], qx[q]);
         iq[q] = quadrant_tree(ir, qy[q], qx[q]);
     }
@@ -158,65 +140,129 @@ __global__ void k_producer_cells(const uint16_t *__restrict__ rgbi, int h, int w
         double term = weight * weight;
         term *= rs;
         term *= rs;
-        b.terms[e_idx * 4 + q] = make_double2(term, ratio * term);
+        out[q] = make_double2(term, ratio * term);
     }
 }
 
 // ---------------------------------------------------------------------------
-// Per-row sums in strict column order.  Only the three binary64 additions
-// per pixel are sequential; the products (IR weight times the response of
-// the visible and infrared samples) are independent.  So a block owns 32
-// rows: seven producer warps compute the products of a 32 x 64 tile into
-// shared memory (zero where the cell's IR test failed first: adding +0.0
-// leaves a non-negative sum unchanged), while warp 0 adds the previous tile,
-// one row per lane, in column order.
+// Cells and per-row sums in one pass over the frame.  A block owns 32 rows
+// (four 8-row blocks) and walks 32 x 64 tiles, the next tile's samples
+// arriving by cp.async while the current one is worked on:
+//   * every warp but the first finds, by ballot, the first IR position in
+//     each 8x8 cell that fails the threshold (cells of the tile);
+//   * warp 7 computes the quadrant terms of complete passing cells of
+//     complete 8-row blocks (the scale epochs);
+//   * warps 1..6 compute the per-pixel products of the row sums (zero where
+//     the cell failed earlier: adding +0.0 leaves a non-negative sum
+//     unchanged) into shared memory;
+//   * warp 0 adds the previous tile's products, one row per lane, in strict
+//     column order -- the only sequential part.
 // ---------------------------------------------------------------------------
 
-constexpr int kRowTile = 64;          // columns per tile
-constexpr int kRowWarps = 8;          // warp 0 adds, warps 1..7 produce
+constexpr int kRowTile = 64;          // columns per tile (8 cells)
+constexpr int kRowWarps = 8;
 constexpr int kRowPitch = kRowTile + 1;
+constexpr int kProductWarps = 6;      // warps 1..6
 
 struct RowSmem {
+    uint2 raw[2][32][kRowTile];     // staged RGBI samples
     double p[2][3][32][kRowPitch];  // [buffer][visible, infrared, weight][row][column]
+    int fp[4][8];                   // first failing position per (8-row block, cell)
 };
 
-__global__ void __launch_bounds__(kRowWarps * 32)
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
+    const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem));
+}
+
+__global__ void __launch_bounds__(kRowWarps * 32, 1)
     k_producer_rows(const uint16_t *__restrict__ rgbi, int h, int w, int active_width, int cells,
                     const float *__restrict__ lut, ProducerBuffers b) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     RowSmem &S = *reinterpret_cast<RowSmem *>(smem_raw);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int r0 = blockIdx.x * 32;
     const int tiles = (active_width + kRowTile - 1) / kRowTile;
-    constexpr int kProducers = (kRowWarps - 1) * 32;
+    const int ne = h / 8;  // complete 8-row blocks
+    const double thr = (double)kIrThreshold;
+    auto stage = [&](int t) {
+        if (t < tiles) {
+            const int col0 = t * kRowTile;
+            for (int q = tid; q < 32 * kRowTile; q += kRowWarps * 32) {
+                const int k = q / kRowTile, j = q % kRowTile;
+                const int row = r0 + k, col = col0 + j;
+                if (row < h && col < active_width)
+                    cp_async8(&S.raw[t & 1][k][j], rgbi + ((int64_t)row * w + col) * 4);
+            }
+        }
+        asm volatile("cp.async.commit_group;\n" ::);
+    };
+    stage(0);
     double rv = 0.0, ri = 0.0, rw = 0.0;
     for (int t = 0; t <= tiles; ++t) {
-        if (warp > 0 && t < tiles) {
-            const int q0 = threadIdx.x - 32;
-            const int col0 = t * kRowTile;
-#pragma unroll 4
-            for (int q = q0; q < 32 * kRowTile; q += kProducers) {
+        asm volatile("cp.async.wait_group 0;\n" ::);
+        __syncthreads();  // tile t staged; tile t-1's products complete
+        stage(t + 1);
+        const int col0 = t * kRowTile;
+        const int bt = t & 1;
+        if (t < tiles && warp >= 1) {
+            // first failing IR position of each cell (row-major inside the cell)
+            for (int ci = warp - 1; ci < 32; ci += kRowWarps - 1) {
+                const int rb = ci >> 3, cc = ci & 7;
+                const int cell = t * 8 + cc;
+                if (cell >= cells) continue;  // warp-uniform
+                bool fail[2];
+#pragma unroll
+                for (int hlf = 0; hlf < 2; ++hlf) {
+                    const int pidx = lane + 32 * hlf, i = pidx >> 3, j = pidx & 7;
+                    const int row = r0 + rb * 8 + i;
+                    fail[hlf] = row < h &&
+                                !(thr < (double)(S.raw[bt][rb * 8 + i][cc * 8 + j].y >> 16));
+                }
+                const uint32_t b0 = __ballot_sync(0xFFFFFFFFu, fail[0]);
+                const uint32_t b1 = __ballot_sync(0xFFFFFFFFu, fail[1]);
+                if (lane == 0)
+                    S.fp[rb][cc] = b0 ? __ffs(b0) - 1 : (b1 ? 32 + __ffs(b1) - 1 : 64);
+            }
+        }
+        __syncthreads();  // fail positions of tile t visible
+        if (t < tiles && warp >= 1 && warp <= kProductWarps) {
+            const int q0 = tid - 32;
+            for (int q = q0; q < 32 * kRowTile; q += kProductWarps * 32) {
                 const int k = q / kRowTile, j = q % kRowTile;
                 const int row = r0 + k, col = col0 + j;
                 double pv = 0.0, pi = 0.0, pw = 0.0;
-                if (row < h && col < active_width) {
-                    const int fp = b.failpos[(int64_t)(row >> 3) * cells + (col >> 3)];
-                    if ((row & 7) * 8 + (col & 7) < fp) {
-                        const uint2 px =
-                            __ldg(reinterpret_cast<const uint2 *>(rgbi + ((int64_t)row * w + col) * 4));
-                        const uint32_t vis = px.x & 0xFFFFu, irv = px.y >> 16;
-                        const double weight = (double)((uint64_t)irv * irv);
-                        pv = weight * (double)__ldg(lut + vis);
-                        pi = weight * (double)__ldg(lut + irv);
-                        pw = weight;
-                    }
+                if (row < h && col < active_width &&
+                    (row & 7) * 8 + (col & 7) < S.fp[k >> 3][j >> 3]) {
+                    const uint2 px = S.raw[bt][k][j];
+                    const uint32_t vis = px.x & 0xFFFFu, irv = px.y >> 16;
+                    const double weight = (double)((uint64_t)irv * irv);
+                    pv = weight * (double)__ldg(lut + vis);
+                    pi = weight * (double)__ldg(lut + irv);
+                    pw = weight;
                 }
-                S.p[t & 1][0][k][j] = pv;
-                S.p[t & 1][1][k][j] = pi;
-                S.p[t & 1][2][k][j] = pw;
+                S.p[bt][0][k][j] = pv;
+                S.p[bt][1][k][j] = pi;
+                S.p[bt][2][k][j] = pw;
             }
-        }
-        if (warp == 0 && t > 0) {
+        } else if (t < tiles && warp == kRowWarps - 1) {
+            // scale-epoch terms: complete 8-row blocks, cells that pass
+            const int rb = lane >> 3, cc = lane & 7;
+            const int blk = (r0 >> 3) + rb, cell = t * 8 + cc;
+            if (blk < ne && cell < cells) {
+                const int64_t e_idx = (int64_t)blk * cells + cell;
+                if (S.fp[rb][cc] != 64) {
+                    b.cell_ok[e_idx] = 0;
+                } else {
+                    b.cell_ok[e_idx] = 1;
+                    double2 terms[4];
+                    cell_terms([&](int i, int j) { return S.raw[bt][rb * 8 + i][cc * 8 + j]; },
+                               lut, terms);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) b.terms[e_idx * 4 + q] = terms[q];
+                }
+            }
+        } else if (warp == 0 && t > 0) {
             const int u = t - 1;
             const int n = min(kRowTile, active_width - u * kRowTile);
             const double *pv = S.p[u & 1][0][lane];
@@ -237,8 +283,8 @@ __global__ void __launch_bounds__(kRowWarps * 32)
                 }
             }
         }
-        __syncthreads();
     }
+    asm volatile("cp.async.wait_group 0;\n" ::);
     const int row = r0 + lane;
     if (warp == 0 && row < h) {
         b.row_sums[row] = rv;
@@ -408,10 +454,9 @@ cudaError_t producer_init() {
 }
 
 size_t producer_bytes(int h, int w) {
-    const int64_t aw = (w / 8) * 8, cells = aw / 8, nb = (h + 7) / 8, ne = h / 8;
+    const int64_t aw = (w / 8) * 8, cells = aw / 8, ne = h / 8;
     size_t b = 0;
     auto add = [&](size_t n) { b += (n + 255) & ~(size_t)255; };
-    add(nb * cells);
     add(ne * cells);
     add(ne * cells * 4 * sizeof(double2));
     add(3 * (size_t)h * sizeof(double));
@@ -424,7 +469,7 @@ size_t producer_bytes(int h, int w) {
 cudaError_t launch_producer(const uint16_t *rgbi, int h, int w, const float *lut, void *scratch,
                             fx_stage *stages, float *rows_out, uint32_t *err,
                             cudaStream_t stream) {
-    const int aw = (w / 8) * 8, cells = aw / 8, nb = (h + 7) / 8, ne = h / 8;
+    const int aw = (w / 8) * 8, cells = aw / 8, ne = h / 8;
     ProducerBuffers b;
     char *p = reinterpret_cast<char *>(scratch);
     auto take = [&](size_t n) {
@@ -432,17 +477,12 @@ cudaError_t launch_producer(const uint16_t *rgbi, int h, int w, const float *lut
         p += (n + 255) & ~(size_t)255;
         return r;
     };
-    b.failpos = (uint8_t *)take((size_t)nb * cells);
     b.cell_ok = (uint8_t *)take((size_t)ne * cells);
     b.terms = (double2 *)take((size_t)ne * cells * 4 * sizeof(double2));
     b.row_sums = (double *)take(3 * (size_t)h * sizeof(double));
     b.cum = (double *)take(3 * (size_t)h * sizeof(double));
     b.add = (float *)take(2 * (size_t)ne * sizeof(float));
     b.p_epoch = (float *)take(2 * (size_t)ne * sizeof(float));
-    {
-        const int64_t n = (int64_t)nb * cells;
-        k_producer_cells<<<(unsigned)((n + 127) / 128), 128, 0, stream>>>(rgbi, h, w, cells, lut, b);
-    }
     k_producer_rows<<<(h + 31) / 32, kRowWarps * 32, sizeof(RowSmem), stream>>>(rgbi, h, w, aw,
                                                                                cells, lut, b);
     if (ne > 0) k_producer_epochs<<<ne, 32, 0, stream>>>(cells, ne, b);
