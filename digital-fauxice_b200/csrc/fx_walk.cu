@@ -567,15 +567,29 @@ __device__ uint32_t walk_segment_exact(const AmbEntry *entries, const uint32_t *
 
 // Resolve one wave: chain the exact E through its segments.  The compact
 // survivor lists stream through shared memory in chunks (warps 1.. stage
-// chunk c+1 while warp 0 chains chunk c), so each hop is a ballot count in
-// shared memory; a segment whose list overflowed uses its dense table, and
+// chunk c+1 while warp 0 chains chunk c), so each hop is a warp-reduced count
+// of survivors at or below E, from registers loaded ahead; a segment whose list overflowed uses its dense table, and
 // E outside a window walks the segment exactly.
+// A hop the survivor list cannot answer: a list that overflowed (dense
+// table) or E outside the window (exact walk of the segment).  Kept out of
+// line so the resolve loop stays short.
+__device__ __noinline__ uint32_t resolve_off_list(const AmbEntry *entries, const uint32_t *pos,
+                                                  uint32_t n, uint32_t t0, const uint32_t *table,
+                                                  SegWindow win, uint32_t E, uint32_t j,
+                                                  uint32_t b, uint32_t &fallbacks) {
+    if (E >= win.lo && E <= win.hi) return table[(size_t)b * kWinMax + (E - win.lo)];
+    const uint32_t i0 = j * kSegLen, i1 = min(n, i0 + kSegLen);
+    fallbacks += 1;
+    return walk_segment_exact(entries, pos, i0, i1, E, t0);
+}
+
 constexpr int kResolveChunk = 96;  // lists per staged chunk
 constexpr int kResolveThreads = 512;
 
 struct ResolveSmem {
     SegList list[2][kResolveChunk];
     SegWindow win[2][kResolveChunk];
+    uint32_t e_in[2][kResolveChunk];  // exact entry counts found by warp 0
 };
 
 __global__ void __launch_bounds__(kResolveThreads)
@@ -628,10 +642,12 @@ __global__ void __launch_bounds__(kResolveThreads)
             w = S.win[c & 1][bb];
             const SegList *L = &S.list[c & 1][bb];
             cnt = L->count;
+            const uint32_t valid = cnt != 0xFFFFu ? cnt : 0u;
 #pragma unroll
-            for (int m = 0; m < kM; ++m) {
+            for (int m = 0; m < kM; ++m) {  // in bounds for any count: no branch
                 const uint32_t k = m * 32 + lane;
-                e[m] = (cnt != 0xFFFFu && k < cnt) ? (uint32_t)L->ein[k] : 0xFFFFFFFFu;
+                const uint32_t v = L->ein[k];
+                e[m] = k < valid ? v : 0xFFFFFFFFu;
             }
         };
         SegWindow win{};
@@ -641,32 +657,30 @@ __global__ void __launch_bounds__(kResolveThreads)
             SegWindow nwin{};
             uint32_t ncnt = 0, nein[kM];
             if (bb + 1 < cnt_c) load_hop(bb + 1, nwin, ncnt, nein);
-            const uint32_t b = first + bb;
-            const uint32_t j = wave * per_wave + b;
-            if (lane == 0) e_in_exact[j] = E;
-            if (E >= win.lo && E <= win.hi) {
-                if (cnt != 0xFFFFu && cnt > 0) {
-                    const uint32_t q = E - win.lo;
-                    uint32_t below = 0;
+            S.e_in[c & 1][bb] = E;  // every lane writes the same value
+            // the list lookup runs unconditionally (an E outside the window
+            // reads an in-bounds but meaningless entry, discarded below), so
+            // the rare-case test is off the dependent path
+            const uint32_t q = E - win.lo;
+            uint32_t mine = 0;  // this lane's entries at or below q
 #pragma unroll
-                    for (int m = 0; m < kM; ++m)
-                        below += __popc(__ballot_sync(0xFFFFFFFFu, ein[m] <= q));
-                    E = win.lo + S.list[c & 1][bb].eout[below - 1];
-                } else {
-                    E = table[(size_t)b * kWinMax + (E - win.lo)];
-                }
-            } else {
-                const uint32_t i0 = j * kSegLen, i1 = min(n, i0 + kSegLen);
-                uint32_t e_exact = 0;
-                if (lane == 0) e_exact = walk_segment_exact(entries, pos, i0, i1, E, t0);
-                E = __shfl_sync(0xFFFFFFFFu, e_exact, 0);
-                fallbacks += 1;
-            }
+            for (int m = 0; m < kM; ++m) mine += ein[m] <= q;
+            const uint32_t below = __reduce_add_sync(0xFFFFFFFFu, mine);
+            const uint32_t fast = win.lo + S.list[c & 1][bb].eout[(below - 1) & (kListMax - 1)];
+            const bool listed = E >= win.lo && E <= win.hi && cnt != 0xFFFFu && cnt > 0;
+            if (!listed)  // rare: every lane computes the same value, out of line
+                E = resolve_off_list(entries, pos, n, t0, table, win, E,
+                                     wave * per_wave + first + bb, first + bb, fallbacks);
+            else
+                E = fast;
             win = nwin;
             cnt = ncnt;
 #pragma unroll
             for (int m = 0; m < kM; ++m) ein[m] = nein[m];
         }
+        __syncwarp();
+        for (uint32_t bb = lane; bb < cnt_c; bb += 32)
+            e_in_exact[wave * per_wave + first + bb] = S.e_in[c & 1][bb];
     }
     if (tid == 0) {
         st->e_wave = E;
