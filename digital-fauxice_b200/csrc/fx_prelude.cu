@@ -99,10 +99,13 @@ __device__ __forceinline__ void center_quadrants(const float q[4], float out[4])
 // raw(i, j) gives the cell's RGBI sample at row i, column j (uint2).
 template <class Raw>
 __device__ void cell_terms(Raw raw, const float *__restrict__ lut, double2 out[4]) {
-    float raw_sum = 0.0f;
+    // The reference accumulates the raw IR samples in float32, one at a
+    // time.  Every partial sum is an integer below 64 * 65535 < 2^24, so each
+    // float32 rounding is exact and the integer sum is the same value.
+    uint32_t raw_total = 0;
 #pragma unroll 8
-    for (int i = 0; i < 64; ++i)
-        raw_sum = (float)((double)raw_sum + (double)(raw(i >> 3, i & 7).y >> 16));
+    for (int i = 0; i < 64; ++i) raw_total += raw(i >> 3, i & 7).y >> 16;
+    const float raw_sum = (float)raw_total;
     const int qy[4] = {0, 0, 4, 4}, qx[4] = {0, 4, 0, 4};
     float vq[4], iq[4], vd[4], id[4];
 #pragma unroll
@@ -185,14 +188,19 @@ __global__ void __launch_bounds__(kRowWarps * 32, 1)
     const int tiles = (active_width + kRowTile - 1) / kRowTile;
     const int ne = h / 8;  // complete 8-row blocks
     const double thr = (double)kIrThreshold;
+    // staging: thread tid copies column tid % 64 of rows tid / 64 + 4 m
+    const int sj = tid % kRowTile, sk0 = tid / kRowTile;
+    const uint16_t *srow = rgbi + ((int64_t)(r0 + sk0) * w + sj) * 4;
+    const int64_t srow_step = (int64_t)4 * w * 4;  // four rows of samples
     auto stage = [&](int t) {
         if (t < tiles) {
-            const int col0 = t * kRowTile;
-            for (int q = tid; q < 32 * kRowTile; q += kRowWarps * 32) {
-                const int k = q / kRowTile, j = q % kRowTile;
-                const int row = r0 + k, col = col0 + j;
-                if (row < h && col < active_width)
-                    cp_async8(&S.raw[t & 1][k][j], rgbi + ((int64_t)row * w + col) * 4);
+            const int col = t * kRowTile + sj;
+            const uint16_t *src = srow + (int64_t)t * kRowTile * 4;
+#pragma unroll
+            for (int m = 0; m < 32 / (kRowWarps * 32 / kRowTile); ++m) {
+                const int k = sk0 + 4 * m;
+                if (r0 + k < h && col < active_width) cp_async8(&S.raw[t & 1][k][sj], src);
+                src += srow_step;
             }
         }
         asm volatile("cp.async.commit_group;\n" ::);
@@ -227,23 +235,42 @@ __global__ void __launch_bounds__(kRowWarps * 32, 1)
         }
         __syncthreads();  // fail positions of tile t visible
         if (t < tiles && warp >= 1 && warp <= kProductWarps) {
+            // fixed trip count, fully unrolled: every LUT gather of the
+            // thread's pixels is in flight before the first product
+            constexpr int kStride = kProductWarps * 32;
+            constexpr int kPerThread = (32 * kRowTile + kStride - 1) / kStride;
             const int q0 = tid - 32;
-            for (int q = q0; q < 32 * kRowTile; q += kProductWarps * 32) {
+            float lv[kPerThread], li[kPerThread];
+            uint32_t wir[kPerThread];
+            bool use[kPerThread];
+#pragma unroll
+            for (int m = 0; m < kPerThread; ++m) {
+                const int q = q0 + m * kStride;
                 const int k = q / kRowTile, j = q % kRowTile;
                 const int row = r0 + k, col = col0 + j;
-                double pv = 0.0, pi = 0.0, pw = 0.0;
-                if (row < h && col < active_width &&
-                    (row & 7) * 8 + (col & 7) < S.fp[k >> 3][j >> 3]) {
-                    const uint2 px = S.raw[bt][k][j];
-                    const uint32_t vis = px.x & 0xFFFFu, irv = px.y >> 16;
-                    const double weight = (double)((uint64_t)irv * irv);
-                    pv = weight * (double)__ldg(lut + vis);
-                    pi = weight * (double)__ldg(lut + irv);
-                    pw = weight;
+                use[m] = q < 32 * kRowTile && row < h && col < active_width &&
+                         (row & 7) * 8 + (col & 7) < S.fp[k >> 3][j >> 3];
+                const uint2 px = use[m] ? S.raw[bt][k][j] : make_uint2(0u, 0u);
+                wir[m] = px.y >> 16;
+                lv[m] = __ldg(lut + (px.x & 0xFFFFu));
+                li[m] = __ldg(lut + wir[m]);
+            }
+#pragma unroll
+            for (int m = 0; m < kPerThread; ++m) {
+                const int q = q0 + m * kStride;
+                if (q < 32 * kRowTile) {
+                    const int k = q / kRowTile, j = q % kRowTile;
+                    double pv = 0.0, pi = 0.0, pw = 0.0;
+                    if (use[m]) {
+                        const double weight = (double)((uint64_t)wir[m] * wir[m]);
+                        pv = weight * (double)lv[m];
+                        pi = weight * (double)li[m];
+                        pw = weight;
+                    }
+                    S.p[bt][0][k][j] = pv;
+                    S.p[bt][1][k][j] = pi;
+                    S.p[bt][2][k][j] = pw;
                 }
-                S.p[bt][0][k][j] = pv;
-                S.p[bt][1][k][j] = pi;
-                S.p[bt][2][k][j] = pw;
             }
         } else if (t < tiles && warp == kRowWarps - 1) {
             // scale-epoch terms: complete 8-row blocks, cells that pass
