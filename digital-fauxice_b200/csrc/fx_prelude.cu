@@ -94,37 +94,39 @@ __device__ __forceinline__ void center_quadrants(const float q[4], float out[4])
     for (int i = 0; i < 4; ++i) out[i] = (float)((double)q[i] - (double)mean);
 }
 
-// The four quadrant terms of one complete cell whose eight rows all pass the
-// IR test (_scale_epoch_additions, producer_parameters.py:183-263).
+// Scale-epoch terms of one complete cell whose eight rows all pass the IR
+// test (_scale_epoch_additions, producer_parameters.py:183-263), in two
+// parts so a tile's cells spread over many threads: the eight quadrant trees
+// (visible and infrared response of each 4x4 quadrant), then the centring,
+// ratios and weights of the cell.
+
+// Quadrant tree `which` (0..3 visible quadrants, 4..7 infrared) of a cell;
 // raw(i, j) gives the cell's RGBI sample at row i, column j (uint2).
 template <class Raw>
-__device__ void cell_terms(Raw raw, const float *__restrict__ lut, double2 out[4]) {
-    // The reference accumulates the raw IR samples in float32, one at a
-    // time.  Every partial sum is an integer below 64 * 65535 < 2^24, so each
-    // float32 rounding is exact and the integer sum is the same value.
-    uint32_t raw_total = 0;
-#pragma unroll 8
-    for (int i = 0; i < 64; ++i) raw_total += raw(i >> 3, i & 7).y >> 16;
-    const float raw_sum = (float)raw_total;
-    const int qy[4] = {0, 0, 4, 4}, qx[4] = {0, 4, 0, 4};
-    float vq[4], iq[4], vd[4], id[4];
+__device__ float quadrant_value(Raw raw, const float *__restrict__ lut, int which) {
+    const int q = which & 3, ir_lane = which >> 2;
+    const int qy = (q >> 1) * 4, qx = (q & 1) * 4;
+    float v[8][8];  // only the quadrant's 4x4 entries are touched
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        float vr[8][8], ir[8][8];  // only the quadrant's 4x4 entries are touched
+    for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const uint2 px = raw(qy[q] + i, qx[q] + j);
-                vr[qy[q] + i][qx[q] + j] = __ldg(lut + (px.x & 0xFFFFu));
-                ir[qy[q] + i][qx[q] + j] = __ldg(lut + (px.y >> 16));
-            }
-        vq[q] = quadrant_tree(vr, qy[q], qx[q]);
-        iq[q] = quadrant_tree(ir, qy[q], qx[q]);
-    }
+        for (int j = 0; j < 4; ++j) {
+            const uint2 px = raw(qy + i, qx + j);
+            v[qy + i][qx + j] = __ldg(lut + (ir_lane ? (px.y >> 16) : (px.x & 0xFFFFu)));
+        }
+    return quadrant_tree(v, qy, qx);
+}
+
+// The four (term, ratio * term) pairs from the quadrant values and the raw
+// IR total.  The reference accumulates the raw IR samples in float32; every
+// partial sum is an integer below 64 * 65535 < 2^24, so each rounding is
+// exact and the integer total is the same value.
+__device__ void finish_terms(const float vq[4], const float iq[4], uint32_t raw_total,
+                             double2 out[4]) {
+    float vd[4], id[4];
     center_quadrants(vq, vd);
     center_quadrants(iq, id);
-    const double rs = (double)raw_sum;
+    const double rs = (double)(float)raw_total;
     const double low = (double)-0.125f, full_high = (double)0.3f, high = (double)0.425f;
     const double outer = (double)0.70710677f;
 #pragma unroll
@@ -153,8 +155,10 @@ __device__ void cell_terms(Raw raw, const float *__restrict__ lut, double2 out[4
 // arriving by cp.async while the current one is worked on:
 //   * every warp but the first finds, by ballot, the first IR position in
 //     each 8x8 cell that fails the threshold (cells of the tile);
-//   * warp 7 computes the quadrant terms of complete passing cells of
-//     complete 8-row blocks (the scale epochs);
+//   * warps 1..7 compute the quadrant trees of complete passing cells of
+//     complete 8-row blocks (the scale epochs), one tree per thread, and
+//     warp 7 the cells' raw IR totals; warp 0 finishes the cells' terms one
+//     tile later;
 //   * warps 1..6 compute the per-pixel products of the row sums (zero where
 //     the cell failed earlier: adding +0.0 leaves a non-negative sum
 //     unchanged) into shared memory;
@@ -171,6 +175,9 @@ struct RowSmem {
     uint2 raw[2][32][kRowTile];     // staged RGBI samples
     double p[2][3][32][kRowPitch];  // [buffer][visible, infrared, weight][row][column]
     int fp[4][8];                   // first failing position per (8-row block, cell)
+    float qv[2][32][8];             // quadrant trees per tile cell (rb * 8 + cc)
+    uint32_t rsum[2][32];           // raw IR total per tile cell
+    int flag[2][32];                // 0: no complete epoch cell, 1: failing, 2: passing
 };
 
 __device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
@@ -272,25 +279,53 @@ __global__ void __launch_bounds__(kRowWarps * 32, 1)
                     S.p[bt][2][k][j] = pw;
                 }
             }
-        } else if (t < tiles && warp == kRowWarps - 1) {
-            // scale-epoch terms: complete 8-row blocks, cells that pass
-            const int rb = lane >> 3, cc = lane & 7;
-            const int blk = (r0 >> 3) + rb, cell = t * 8 + cc;
-            if (blk < ne && cell < cells) {
-                const int64_t e_idx = (int64_t)blk * cells + cell;
-                if (S.fp[rb][cc] != 64) {
-                    b.cell_ok[e_idx] = 0;
-                } else {
-                    b.cell_ok[e_idx] = 1;
+        }
+        if (t < tiles && warp >= 1) {
+            // quadrant trees: trees 0..191 on warps 1..6, 192..255 on warp 7
+            const int z0 = tid - 32;
+            const int nz = warp == kRowWarps - 1 ? 2 : 1;
+#pragma unroll 1
+            for (int r = 0; r < nz; ++r) {
+                const int z = warp == kRowWarps - 1 ? 192 + lane + 32 * r : z0;
+                const int cl = z >> 3, rb = cl >> 3, cc = cl & 7;
+                const int blk = (r0 >> 3) + rb, cell = t * 8 + cc;
+                if (blk < ne && cell < cells && S.fp[rb][cc] == 64)
+                    S.qv[bt][cl][z & 7] = quadrant_value(
+                        [&](int i, int j) { return S.raw[bt][rb * 8 + i][cc * 8 + j]; }, lut,
+                        z & 7);
+            }
+            if (warp == kRowWarps - 1) {  // lane = tile cell: status and raw total
+                const int rb = lane >> 3, cc = lane & 7;
+                const int blk = (r0 >> 3) + rb, cell = t * 8 + cc;
+                int flag = 0;
+                if (blk < ne && cell < cells) flag = S.fp[rb][cc] == 64 ? 2 : 1;
+                uint32_t total = 0;
+                if (flag == 2) {
+#pragma unroll 8
+                    for (int i = 0; i < 64; ++i) total += S.raw[bt][rb * 8 + (i >> 3)][cc * 8 + (i & 7)].y >> 16;
+                }
+                S.flag[bt][lane] = flag;
+                S.rsum[bt][lane] = total;
+            }
+        }
+        if (warp == 0 && t > 0) {
+            // finish the previous tile's epoch cells (lane = tile cell)
+            const int u = t - 1, ub = u & 1;
+            const int flag = S.flag[ub][lane];
+            if (flag) {
+                const int rb = lane >> 3, cc = lane & 7;
+                const int64_t e_idx = (int64_t)((r0 >> 3) + rb) * cells + (u * 8 + cc);
+                b.cell_ok[e_idx] = flag == 2 ? 1 : 0;
+                if (flag == 2) {
+                    const float *qv = S.qv[ub][lane];
+                    const float vq[4] = {qv[0], qv[1], qv[2], qv[3]};
+                    const float iq[4] = {qv[4], qv[5], qv[6], qv[7]};
                     double2 terms[4];
-                    cell_terms([&](int i, int j) { return S.raw[bt][rb * 8 + i][cc * 8 + j]; },
-                               lut, terms);
+                    finish_terms(vq, iq, S.rsum[ub][lane], terms);
 #pragma unroll
                     for (int q = 0; q < 4; ++q) b.terms[e_idx * 4 + q] = terms[q];
                 }
             }
-        } else if (warp == 0 && t > 0) {
-            const int u = t - 1;
             const int n = min(kRowTile, active_width - u * kRowTile);
             const double *pv = S.p[u & 1][0][lane];
             const double *pi = S.p[u & 1][1][lane];
