@@ -382,10 +382,21 @@ struct StencilSmem {
     float rcs[3][4][kTileH][RC];  // [channel][S3,S5,S7,S9]
     Record rec[CR][RECC];
     float cw[kTileH][kTileW][4];
-    float auxt[RR][RC];  // aux at clamped (y0-4+r, x0-4+c): decision bars and point aux
+    union {
+        // aux at clamped (y0-4+r, x0-4+c): decision masks and point aux,
+        // dead once the records are built
+        float auxt[RR][RC];
+        struct {  // the attempted-pixel list of the per-pixel phase
+            uint32_t wcount[kStencilThreads / 32];
+            int n_attempted;
+            uint16_t attempted[kStencilThreads];  // thread index of each attempted pixel
+        } dec;
+    };
     unsigned long long rowlow[RR];  // bit c: auxt[r][c] below the decision threshold
     uint32_t collow[RC];            // bit r: the same, by column
 };
+static_assert(sizeof(float) * RR * RC >= 4 * (kStencilThreads / 32 + 1) + 2 * kStencilThreads,
+              "the attempted list fits in the aux tile");
 
 __global__ void __launch_bounds__(kStencilThreads)
     k_stencil(const uint16_t *__restrict__ rgbi, Geometry g, const float *__restrict__ lut,
@@ -538,35 +549,59 @@ __global__ void __launch_bounds__(kStencilThreads)
     }
     __syncthreads();
 
-    // ---- per output pixel --------------------------------------------------
-    const int ty = tid / kTileW, tx = tid % kTileW;
+    // ---- per output pixel: the decision -------------------------------------
+    // Each pixel decides whether it is attempted; the attempted ones are then
+    // listed in shared memory and processed densely (about half the pixels
+    // are attempted, mixed within every warp).
+    {
+        const int ty = tid / kTileW, tx = tid % kTileW;
+        const int y = y0 + ty, x = x0 + tx;
+        bool eligible = false;
+        if (y < h && x < w) {
+            const fx_stage ws = stages[y + 6];  // writer stage y+7
+            const bool floor_enabled = p.driver_gate_primary || ws.gate_secondary;
+            // decision bars (streaming.py:157-198), edge-replicated via the
+            // tile: rows ty..ty+8 of a column, columns tx..tx+8 of a row
+            const int rad = p.radius;
+            const int vl = __popc((S.collow[tx + 4 - rad] >> ty) & 0x1FFu);
+            const int vr = __popc((S.collow[tx + 4 + rad] >> ty) & 0x1FFu);
+            const int ha = __popcll((S.rowlow[ty + 4 - rad] >> tx) & 0x1FFull);
+            const int hb = __popcll((S.rowlow[ty + 4 + rad] >> tx) & 0x1FFull);
+            const int lim = p.count_limit;
+            eligible = !(vl > lim || ha > lim || vr > lim || hb > lim);
+            const float point_score = S.cw[ty][tx][3];
+            if (ws.row_gate != 0) eligible = false;
+            else if (floor_enabled && !(point_score < 1.0f)) eligible = false;
+            // driver_forces_fallback (reconstruction.py:890-904)
+            if (eligible && (ws.row_gate != 0 || (floor_enabled && point_score >= 1.0f)))
+                eligible = false;
+            if (!eligible) meta_out[6 * (int64_t)w + (int64_t)y * w + x] = 0;
+        }
+        const uint32_t bal = __ballot_sync(0xFFFFFFFFu, eligible);
+        if ((tid & 31) == 0) S.dec.wcount[tid >> 5] = __popc(bal);
+        __syncthreads();
+        uint32_t base = 0, total = 0;
+#pragma unroll
+        for (int k = 0; k < kStencilThreads / 32; ++k) {
+            const uint32_t c = S.dec.wcount[k];
+            base += k < (tid >> 5) ? c : 0u;
+            total += c;
+        }
+        if (eligible) S.dec.attempted[base + __popc(bal & ((1u << (tid & 31)) - 1u))] = (uint16_t)tid;
+        if (tid == 0) S.dec.n_attempted = total;
+        __syncthreads();
+    }
+
+    // ---- attempted pixels, densely -----------------------------------------
+    const int listed = S.dec.n_attempted;
+    if (tid >= listed) return;
+    const int me = S.dec.attempted[tid];
+    const int ty = me / kTileW, tx = me % kTileW;
     const int y = y0 + ty, x = x0 + tx;
-    if (y >= h || x >= w) return;
     const int64_t site = 6 * (int64_t)w + (int64_t)y * w + x;
-    // the original's samples: issued first so their latency overlaps the
-    // decision and candidate arithmetic
     const uint2 raw = reinterpret_cast<const uint2 *>(rgbi)[(int64_t)y * w + x];
     const fx_stage ws = stages[y + 6];  // writer stage y+7
     const bool floor_enabled = p.driver_gate_primary || ws.gate_secondary;
-
-    // decision bars (streaming.py:157-198), edge-replicated via the tile
-    const int rad = p.radius;
-    // bars of nine: rows ty..ty+8 of a column, columns tx..tx+8 of a row
-    const int vl = __popc((S.collow[tx + 4 - rad] >> ty) & 0x1FFu);
-    const int vr = __popc((S.collow[tx + 4 + rad] >> ty) & 0x1FFu);
-    const int ha = __popcll((S.rowlow[ty + 4 - rad] >> tx) & 0x1FFull);
-    const int hb = __popcll((S.rowlow[ty + 4 + rad] >> tx) & 0x1FFull);
-    const int lim = p.count_limit;
-    bool eligible = !(vl > lim || ha > lim || vr > lim || hb > lim);
-    const float point_score = S.cw[ty][tx][3];
-    if (ws.row_gate != 0) eligible = false;
-    else if (floor_enabled && !(point_score < 1.0f)) eligible = false;
-    // driver_forces_fallback (reconstruction.py:890-904)
-    if (eligible && (ws.row_gate != 0 || (floor_enabled && point_score >= 1.0f))) eligible = false;
-    if (!eligible) {
-        meta_out[site] = 0;
-        return;
-    }
     const float orig[3] = {__ldg(lut + (raw.x & 0xFFFFu)), __ldg(lut + (raw.x >> 16)),
                            __ldg(lut + (raw.y & 0xFFFFu))};
 
