@@ -192,21 +192,16 @@ def dist_setup():
 
 
 def max_over_ranks(value: float, world: int) -> float:
-    if world == 1:
-        return value
-    import torch
-    import torch.distributed as dist
+    from fauxice_b200 import replicas
 
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    return replicas.max_over_ranks(value) if world > 1 else value
 
 
 def barrier(world: int) -> None:
     if world > 1:
-        import torch.distributed as dist
+        from fauxice_b200 import replicas
 
-        dist.barrier()
+        replicas.barrier()
 
 
 def make_job(main, prepass):
