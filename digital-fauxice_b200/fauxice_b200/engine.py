@@ -238,7 +238,9 @@ def run_frame(ctx: _lib.Context, main: np.ndarray, params: _lib.FxParams,
 def replay_result(outcome: FrameOutcome) -> StreamingReplayResult:
     c = outcome.counters
     h, w = outcome.output.shape[:2]
-    digest = hashlib.sha256(outcome.output.astype("<u2", copy=False).tobytes(order="C"))
+    # little-endian uint16 bytes in row-major order, hashed in place (no copy)
+    out = np.ascontiguousarray(outcome.output.astype("<u2", copy=False))
+    digest = hashlib.sha256(memoryview(out).cast("B"))
     return StreamingReplayResult(
         shape=(h, w, 3),
         startup=StartupReplayResult(
