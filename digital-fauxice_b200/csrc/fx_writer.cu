@@ -312,10 +312,11 @@ __device__ void copy_intervals(const ChannelView &cv, AmbEntry &e, uint32_t *err
 }
 
 // Lists every RNG-dependent channel in chain order: entry a gets its site
-// (l1), channel (w1) and draw position; k_coef fills in the rest.
+// (site_of[a], a compact array so the writes coalesce) and its draw
+// position; k_coef fills in the intervals and jumps.
 __global__ void __launch_bounds__(kSegThreads)
     k_amb(const uint8_t *__restrict__ meta, int64_t sites, const uint32_t *__restrict__ seg_base,
-          const uint32_t *__restrict__ seg_amb, AmbEntry *__restrict__ entries,
+          const uint32_t *__restrict__ seg_amb, uint32_t *__restrict__ site_of,
           uint32_t *__restrict__ pos_out, int64_t capacity) {
     __shared__ uint32_t ws[kSegThreads / 32];
     const int64_t first = (int64_t)blockIdx.x * kSegment + threadIdx.x * kPer;
@@ -332,8 +333,7 @@ __global__ void __launch_bounds__(kSegThreads)
                 const int code = meta_code(m[i], c);
                 if (code == 3) {
                     if ((int64_t)a < capacity) {
-                        entries[a].l1 = (uint32_t)(first + i);
-                        entries[a].w1 = (uint32_t)c;
+                        site_of[a] = (uint32_t)(first + i);
                         pos_out[a] = pos;
                     }
                     ++a;
@@ -352,14 +352,24 @@ __global__ void __launch_bounds__(kSegThreads)
 // predicates) and the affine jumps from the previous listed channel.
 __global__ void k_coef(AmbEntry *__restrict__ entries, const uint32_t *__restrict__ pos,
                        const uint32_t *__restrict__ n_amb_ptr, int64_t capacity,
+                       const uint32_t *__restrict__ site_of, const uint8_t *__restrict__ meta,
                        const double *__restrict__ cand, int w, const uint16_t *__restrict__ rgbi,
                        const float *__restrict__ lut, fx_params p, uint32_t *err) {
     const uint32_t n = (uint32_t)min((int64_t)*n_amb_ptr, capacity);
     const DitherConst dc = dither_const(p);
     const int64_t su = 6 * (int64_t)w;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int64_t site = entries[i].l1;
-        const int c = (int)entries[i].w1;
+        const uint32_t site32 = site_of[i];
+        const int64_t site = site32;
+        // a site's RNG-dependent channels are listed in channel order: this
+        // entry is the k-th of its site
+        const int k = (i >= 1 && site_of[i - 1] == site32)
+                          ? ((i >= 2 && site_of[i - 2] == site32) ? 2 : 1)
+                          : 0;
+        const uint8_t mi = meta[site];
+        int c = 0;
+        for (int seen = 0; c < 3; ++c)
+            if (meta_code(mi, c) == 3 && seen++ == k) break;
         const int64_t pixel = site < su ? site % w : site - su;
         const uint2 raw = reinterpret_cast<const uint2 *>(rgbi)[pixel];
         const uint32_t lane = c == 0 ? (raw.x & 0xFFFFu) : (c == 1 ? (raw.x >> 16) : (raw.y & 0xFFFFu));
@@ -651,11 +661,12 @@ cudaError_t launch_writer(const Geometry &g, const uint8_t *meta, const double *
     cudaMemsetAsync(ctr, 0, sizeof(DevCounters), stream);
     k_seg_sums<<<(unsigned)segs, kSegThreads, 0, stream>>>(meta, g.sites, b.seg_base, b.seg_amb);
     k_seg_scan<<<1, 1024, 0, stream>>>(b.seg_base, b.seg_amb, segs);
+    // the site list lives in extra_after until the walk writes the counts
     k_amb<<<(unsigned)segs, kSegThreads, 0, stream>>>(meta, g.sites, b.seg_base, b.seg_amb,
-                                                      b.entries, b.pos, b.capacity);
+                                                      b.extra_after, b.pos, b.capacity);
     const uint32_t *n_amb = b.seg_amb + segs;
-    k_coef<<<1184, 256, 0, stream>>>(b.entries, b.pos, n_amb, b.capacity, cand, g.w, rgbi, lut, p,
-                                     err);
+    k_coef<<<1184, 256, 0, stream>>>(b.entries, b.pos, n_amb, b.capacity, b.extra_after, meta,
+                                     cand, g.w, rgbi, lut, p, err);
     marks.mark(5, stream);
     cudaError_t e = launch_walk(b.entries, b.pos, n_amb, b.capacity, s0, b.walk_scratch,
                                 b.per_wave, b.parallel_walk, b.extra_after, &ctr->walk_fallbacks,
