@@ -5,6 +5,7 @@
 #include <cstring>
 #include <mutex>
 #include <thread>
+#include <algorithm>
 #include <vector>
 
 #include "fx_internal.cuh"
@@ -122,6 +123,7 @@ struct Slot {
     void *h_out = nullptr;
     size_t h_out_bytes = 0;
     void *h_ctr = nullptr;  // DevCounters copy + error word
+    cudaEvent_t chunk_done[16] = {};  // staged downloads (fx_process)
     // request in flight
     bool busy = false;
     int64_t ticket = -1;
@@ -441,6 +443,8 @@ FX_API void fx_context_destroy(fx_context *ctx) {
         if (s.h_out) cudaFreeHost(s.h_out);
         if (s.h_ctr) cudaFreeHost(s.h_ctr);
         if (s.done) cudaEventDestroy(s.done);
+        for (cudaEvent_t e : s.chunk_done)
+            if (e) cudaEventDestroy(e);
         if (s.stream) cudaStreamDestroy(s.stream);
     }
     for (auto &v : ctx->pending)
@@ -514,6 +518,93 @@ FX_API int fx_producer_rows(fx_context *ctx, const uint16_t *main_rgbi, int32_t 
     return FX_OK;
 }
 
+// Host <-> device copies of caller (pageable) buffers through the slot's
+// pinned staging: the frame moves in chunks, host threads copying one chunk
+// between the caller's buffer and pinned memory while the DMA engine moves
+// another.
+constexpr int kCopyChunks = 16;
+
+static int copy_threads() {
+    const unsigned n = std::thread::hardware_concurrency();
+    return n >= 8 ? 8 : (n > 0 ? (int)n : 1);
+}
+
+static int ensure_pinned(fx_context *ctx, void **buf, size_t *have, size_t need) {
+    if (*have >= need) return FX_OK;
+    if (*buf) cudaFreeHost(*buf);
+    *buf = nullptr;
+    *have = 0;
+    FX_CUDA(ctx, cudaMallocHost(buf, need));
+    *have = need;
+    return FX_OK;
+}
+
+static int staged_upload(fx_context *ctx, Slot &s, void *d_dst, const void *h_src, size_t bytes) {
+    int rc = ensure_pinned(ctx, &s.h_in, &s.h_in_bytes, bytes);
+    if (rc) return rc;
+    const size_t chunk = (bytes + kCopyChunks - 1) / kCopyChunks;
+    const int nt = copy_threads();
+    std::vector<cudaError_t> errs(nt, cudaSuccess);
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nt; ++t)
+        pool.emplace_back([&, t] {
+            for (int k = t; k < kCopyChunks; k += nt) {
+                const size_t off = (size_t)k * chunk;
+                if (off >= bytes) break;
+                const size_t len = std::min(chunk, bytes - off);
+                std::memcpy(static_cast<char *>(s.h_in) + off,
+                            static_cast<const char *>(h_src) + off, len);
+                const cudaError_t e = cudaMemcpyAsync(static_cast<char *>(d_dst) + off,
+                                                      static_cast<char *>(s.h_in) + off, len,
+                                                      cudaMemcpyHostToDevice, s.stream);
+                if (e != cudaSuccess) errs[t] = e;
+            }
+        });
+    for (std::thread &th : pool) th.join();
+    for (cudaError_t e : errs)
+        if (e != cudaSuccess) return fail(ctx, FX_ERR_CUDA, "upload: %s", cudaGetErrorString(e));
+    return FX_OK;
+}
+
+static int staged_download(fx_context *ctx, Slot &s, void *h_dst, const void *d_src,
+                           size_t bytes) {
+    int rc = ensure_pinned(ctx, &s.h_out, &s.h_out_bytes, bytes);
+    if (rc) return rc;
+    const size_t chunk = (bytes + kCopyChunks - 1) / kCopyChunks;
+    for (int k = 0; k < kCopyChunks; ++k) {
+        const size_t off = (size_t)k * chunk;
+        if (off >= bytes) break;
+        if (!s.chunk_done[k])
+            FX_CUDA(ctx, cudaEventCreateWithFlags(&s.chunk_done[k], cudaEventDisableTiming));
+        FX_CUDA(ctx, cudaMemcpyAsync(static_cast<char *>(s.h_out) + off,
+                                     static_cast<const char *>(d_src) + off,
+                                     std::min(chunk, bytes - off), cudaMemcpyDeviceToHost,
+                                     s.stream));
+        FX_CUDA(ctx, cudaEventRecord(s.chunk_done[k], s.stream));
+    }
+    const int nt = copy_threads();
+    std::vector<cudaError_t> errs(nt, cudaSuccess);
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nt; ++t)
+        pool.emplace_back([&, t] {
+            for (int k = t; k < kCopyChunks; k += nt) {
+                const size_t off = (size_t)k * chunk;
+                if (off >= bytes) break;
+                const cudaError_t e = cudaEventSynchronize(s.chunk_done[k]);
+                if (e != cudaSuccess) {
+                    errs[t] = e;
+                    continue;
+                }
+                std::memcpy(static_cast<char *>(h_dst) + off,
+                            static_cast<const char *>(s.h_out) + off, std::min(chunk, bytes - off));
+            }
+        });
+    for (std::thread &th : pool) th.join();
+    for (cudaError_t e : errs)
+        if (e != cudaSuccess) return fail(ctx, FX_ERR_CUDA, "download: %s", cudaGetErrorString(e));
+    return FX_OK;
+}
+
 FX_API int fx_process(fx_context *ctx, const fx_frame *f, fx_counters *counters) {
     if (!ctx || !f || !f->main_rgbi || !f->rgb_out) return FX_ERR_INVALID_ARGUMENT;
     std::lock_guard<std::mutex> lock(ctx->mu);
@@ -529,8 +620,8 @@ FX_API int fx_process(fx_context *ctx, const fx_frame *f, fx_counters *counters)
     for (int attempt = 0; attempt < 2; ++attempt) {
         rc = ensure_arena(ctx, s, g, cap);
         if (rc) return rc;
-        FX_CUDA(ctx, cudaMemcpyAsync(s.arena.rgbi, f->main_rgbi, px * 8, cudaMemcpyHostToDevice,
-                                     s.stream));
+        rc = staged_upload(ctx, s, s.arena.rgbi, f->main_rgbi, px * 8);
+        if (rc) return rc;
         rc = enqueue_pass(ctx, s, g, *f->params, f->stages, f->rng_state, s.arena.rgbi,
                           s.arena.out, s.arena.changed, false);
         if (rc) return rc;
@@ -549,7 +640,8 @@ FX_API int fx_process(fx_context *ctx, const fx_frame *f, fx_counters *counters)
             cap = (int64_t)counters_n_amb(hc) + 1024;
             continue;
         }
-        FX_CUDA(ctx, cudaMemcpy(f->rgb_out, s.arena.out, px * 6, cudaMemcpyDeviceToHost));
+        rc = staged_download(ctx, s, f->rgb_out, s.arena.out, px * 6);
+        if (rc) return rc;
         if (f->score_out)
             FX_CUDA(ctx, cudaMemcpy2D(f->score_out, (size_t)g.w * 4,
                                       s.arena.hs + g.padded_index(0, 0), (size_t)g.pitch * 4,
