@@ -152,6 +152,25 @@ SIGNATURES = {
     "fx_frame_bytes": ([ctypes.c_int32, ctypes.c_int32], ctypes.c_int64),
     "fx_profile_enable": ([_P, ctypes.c_int], ctypes.c_int),
     "fx_profile_read": ([_P, _P, ctypes.POINTER(ctypes.c_int64), ctypes.c_int], ctypes.c_int),
+    # at-floor routing census primitives
+    "fx_label8": ([_P, ctypes.c_int32, ctypes.c_int32, _P, _P, _P, _P,
+                   ctypes.POINTER(ctypes.c_int64), _P], ctypes.c_int),
+    "fx_chessboard_distance": ([_P, ctypes.c_int32, ctypes.c_int32, _P, _P, _P, _P],
+                               ctypes.c_int),
+    "fx_label_stats": ([_P, _P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int64, _P, _P, _P, _P],
+                       ctypes.c_int),
+    "fx_dilate_square": ([_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _P, _P, _P],
+                         ctypes.c_int),
+    "fx_label_pairs": ([_P, _P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int64, _P, _P,
+                        ctypes.POINTER(ctypes.c_int64), _P], ctypes.c_int),
+    "fx_map_labels": ([_P, ctypes.c_int64, _P, ctypes.c_int64, _P, _P, _P], ctypes.c_int),
+    "fx_clear_label": ([_P, _P, ctypes.c_int64, ctypes.c_int32, _P,
+                        ctypes.POINTER(ctypes.c_int64), _P], ctypes.c_int),
+    "fx_count_where": ([_P, _P, ctypes.c_int64, ctypes.c_int64, _P, _P], ctypes.c_int),
+    "fx_tile_extract": ([_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                         ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _P, _P], ctypes.c_int),
+    "fx_tile_scatter": ([_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                         ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _P, _P], ctypes.c_int),
 }
 
 PROFILE_STAGES = ("producer", "planes", "stencil", "startup", "chain", "walk", "apply")

@@ -228,6 +228,68 @@ FX_API int fx_mem_info(fx_context *ctx, size_t *free_bytes, size_t *total_bytes)
 /* Device bytes one frame of the given size needs (admission estimate). */
 FX_API int64_t fx_frame_bytes(int32_t height, int32_t width);
 
+/* ------------------------------------------------------------------------
+ * At-floor routing census (hybrid routing.py:447-682, route_at_floor_mask).
+ * Context-free device primitives; the per-component tables, reasons and
+ * budget are host logic (fauxice_b200.routing).  Every pointer named d_* is
+ * device memory; `stream` is a cudaStream_t or NULL.  Each call waits for
+ * its own work before returning.
+ * ---------------------------------------------------------------------- */
+
+/* 8-connected components of a uint8 mask, ids 1..K in raster order of each
+ * component's first pixel, 0 for background (ndimage.label with a 3x3
+ * structure, routing.py:467-473 and :327-333).  d_forest int32[h*w] is
+ * scratch distinct from d_labels, d_block_scratch holds ceil(h*w/256) + 1
+ * uint32, d_err one uint32.  h*w < 2^31. */
+FX_API int fx_label8(const uint8_t *d_mask, int32_t h, int32_t w, int32_t *d_labels,
+                     int32_t *d_forest, uint32_t *d_block_scratch, uint32_t *d_err,
+                     int64_t *count, void *stream);
+/* Chessboard distance of every set pixel to the nearest in-frame unset pixel,
+ * 0 on unset pixels (distance_transform_cdt metric "chessboard",
+ * routing.py:277); the mask must hold at least one unset pixel.  d_work is
+ * int32[h*w] scratch, d_flag one uint32. */
+FX_API int fx_chessboard_distance(const uint8_t *d_mask, int32_t h, int32_t w, int32_t *d_dist,
+                                  int32_t *d_work, uint32_t *d_flag, void *stream);
+/* Per label 1..k (entry l-1): pixel count, half-open box [y0, x0, y1, x1)
+ * and, when d_plane is non-NULL, the maximum of d_plane over the label
+ * (bincount, find_objects and ndimage.maximum, routing.py:474-488, :278). */
+FX_API int fx_label_stats(const int32_t *d_labels, const int32_t *d_plane, int32_t h, int32_t w,
+                          int64_t k, unsigned long long *d_area, int32_t *d_box, int32_t *d_vmax,
+                          void *stream);
+/* Square (Chebyshev) dilation by `radius`, zero outside the frame, the
+ * radius clipped per axis to the frame (routing.py:304-336).  d_work is
+ * uint8[h*w] scratch. */
+FX_API int fx_dilate_square(const uint8_t *d_in, int32_t h, int32_t w, int32_t radius,
+                            uint8_t *d_work, uint8_t *d_out, void *stream);
+/* Distinct (a, b) pairs of two label planes over pixels where both are
+ * positive, written as int32 pairs to d_pairs with possible repeats (the
+ * caller sorts them unique, as routing.py:552-556 does).  FX_ERR_OUT_OF_MEMORY
+ * with *count set when more than `capacity` pairs were found. */
+FX_API int fx_label_pairs(const int32_t *d_a, const int32_t *d_b, int32_t h, int32_t w,
+                          int64_t capacity, int32_t *d_pairs, unsigned long long *d_count,
+                          int64_t *count, void *stream);
+/* out[i] = map[labels[i]] as int32 (d_out_i32) and/or as map != 0 (d_out_u8),
+ * for a map of k + 1 entries; labels outside 0..k give 0 (the lookups
+ * routed_lookup[...] and old_to_new[...], routing.py:504, :434). */
+FX_API int fx_map_labels(const int32_t *d_labels, int64_t n, const int32_t *d_map, int64_t k,
+                         int32_t *d_out_i32, uint8_t *d_out_u8, void *stream);
+/* Clear the mask where labels == id; *cleared = how many of those pixels were
+ * set (the perimeter rule, routing.py:517-522).  d_scratch one uint64. */
+FX_API int fx_clear_label(uint8_t *d_mask, const int32_t *d_labels, int64_t n, int32_t id,
+                          unsigned long long *d_scratch, int64_t *cleared, void *stream);
+/* d_counts[key] = pixels with 0 < key <= k and cond > 0, for keys 0..k (the
+ * overlap bincounts, routing.py:533-546). */
+FX_API int fx_count_where(const int32_t *d_key, const int32_t *d_cond, int64_t n, int64_t k,
+                          unsigned long long *d_counts, void *stream);
+/* tile = (labels[y0+ty][x0+tx] == id) over a th x tw window, and the write
+ * back of a labelled tile offset by `base` (the oversized-region tiling,
+ * routing.py:376-410). */
+FX_API int fx_tile_extract(const int32_t *d_labels, int32_t h, int32_t w, int32_t y0, int32_t x0,
+                           int32_t th, int32_t tw, int32_t id, uint8_t *d_tile, void *stream);
+FX_API int fx_tile_scatter(const int32_t *d_tile_labels, int32_t h, int32_t w, int32_t y0,
+                           int32_t x0, int32_t th, int32_t tw, int32_t base, int32_t *d_plane,
+                           void *stream);
+
 #ifdef __cplusplus
 }
 #endif
