@@ -70,7 +70,7 @@ def build(verbose: bool = False) -> str:
         newest = max(newest, os.path.getmtime(obj))
     if not os.path.exists(OUT) or os.path.getmtime(OUT) < newest:
         cmd = [nvcc(), *host_compiler(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared",
-               "-o", OUT, *objects, "-lcudart"]
+               "-o", OUT, *objects, "-lcudart", "-lcrypto"]
         res = subprocess.run(cmd, capture_output=True, text=True)
         if res.returncode:
             sys.stderr.write(res.stdout + res.stderr)

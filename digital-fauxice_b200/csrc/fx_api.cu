@@ -8,6 +8,8 @@
 #include <algorithm>
 #include <vector>
 
+#include <openssl/evp.h>
+
 #include "fx_internal.cuh"
 
 namespace fx {
@@ -158,6 +160,9 @@ struct fx_context {
     int64_t next_ticket = 1;
     std::mutex mu;
     char error[512] = {0};
+    bool hash_output = false;      // fx_process: SHA-256 of the RGB16 output
+    bool digest_valid = false;
+    unsigned char digest[32] = {0};
 };
 
 namespace fx {
@@ -566,8 +571,28 @@ static int staged_upload(fx_context *ctx, Slot &s, void *d_dst, const void *h_sr
     return FX_OK;
 }
 
+// SHA-256 of `bytes` of pinned memory, fed chunk by chunk as each chunk's
+// device-to-host copy completes (chunk k's event), so hashing overlaps the
+// remaining copies.  Returns false when a copy or the digest failed.
+static bool hash_chunks(Slot &s, const char *pinned, size_t bytes, size_t chunk,
+                        unsigned char *digest) {
+    EVP_MD_CTX *md = EVP_MD_CTX_new();
+    if (!md) return false;
+    bool ok = EVP_DigestInit_ex(md, EVP_sha256(), nullptr) == 1;
+    for (int k = 0; ok && k < kCopyChunks; ++k) {
+        const size_t off = (size_t)k * chunk;
+        if (off >= bytes) break;
+        ok = cudaEventSynchronize(s.chunk_done[k]) == cudaSuccess &&
+             EVP_DigestUpdate(md, pinned + off, std::min(chunk, bytes - off)) == 1;
+    }
+    unsigned int len = 0;
+    ok = ok && EVP_DigestFinal_ex(md, digest, &len) == 1 && len == 32;
+    EVP_MD_CTX_free(md);
+    return ok;
+}
+
 static int staged_download(fx_context *ctx, Slot &s, void *h_dst, const void *d_src,
-                           size_t bytes) {
+                           size_t bytes, unsigned char *digest = nullptr) {
     int rc = ensure_pinned(ctx, &s.h_out, &s.h_out_bytes, bytes);
     if (rc) return rc;
     const size_t chunk = (bytes + kCopyChunks - 1) / kCopyChunks;
@@ -585,6 +610,11 @@ static int staged_download(fx_context *ctx, Slot &s, void *h_dst, const void *d_
     const int nt = copy_threads();
     std::vector<cudaError_t> errs(nt, cudaSuccess);
     std::vector<std::thread> pool;
+    bool hashed = true;
+    if (digest)
+        pool.emplace_back([&] {
+            hashed = hash_chunks(s, static_cast<const char *>(s.h_out), bytes, chunk, digest);
+        });
     for (int t = 0; t < nt; ++t)
         pool.emplace_back([&, t] {
             for (int k = t; k < kCopyChunks; k += nt) {
@@ -602,6 +632,7 @@ static int staged_download(fx_context *ctx, Slot &s, void *h_dst, const void *d_
     for (std::thread &th : pool) th.join();
     for (cudaError_t e : errs)
         if (e != cudaSuccess) return fail(ctx, FX_ERR_CUDA, "download: %s", cudaGetErrorString(e));
+    if (!hashed) return fail(ctx, FX_ERR_INTERNAL, "output SHA-256 failed");
     return FX_OK;
 }
 
@@ -640,8 +671,11 @@ FX_API int fx_process(fx_context *ctx, const fx_frame *f, fx_counters *counters)
             cap = (int64_t)counters_n_amb(hc) + 1024;
             continue;
         }
-        rc = staged_download(ctx, s, f->rgb_out, s.arena.out, px * 6);
+        ctx->digest_valid = false;
+        rc = staged_download(ctx, s, f->rgb_out, s.arena.out, px * 6,
+                             ctx->hash_output ? ctx->digest : nullptr);
         if (rc) return rc;
+        ctx->digest_valid = ctx->hash_output;
         if (f->score_out)
             FX_CUDA(ctx, cudaMemcpy2D(f->score_out, (size_t)g.w * 4,
                                       s.arena.hs + g.padded_index(0, 0), (size_t)g.pitch * 4,
@@ -711,6 +745,23 @@ FX_API int fx_set_parallel_walk(fx_context *ctx, int enable) {
     if (!ctx) return FX_ERR_INVALID_ARGUMENT;
     std::lock_guard<std::mutex> lock(ctx->mu);
     ctx->parallel_walk = enable != 0;
+    return FX_OK;
+}
+
+FX_API int fx_set_output_digest(fx_context *ctx, int enable) {
+    if (!ctx) return FX_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    ctx->hash_output = enable != 0;
+    ctx->digest_valid = false;
+    return FX_OK;
+}
+
+FX_API int fx_output_digest(fx_context *ctx, uint8_t *digest) {
+    if (!ctx || !digest) return FX_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    if (!ctx->digest_valid)
+        return fail(ctx, FX_ERR_INVALID_ARGUMENT, "no output digest: enable it before fx_process");
+    std::memcpy(digest, ctx->digest, 32);
     return FX_OK;
 }
 

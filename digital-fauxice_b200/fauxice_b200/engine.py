@@ -152,6 +152,8 @@ def context(device: int = 0) -> _lib.Context:
             ctx = _lib.Context(device, lut=lut, high=high, low=low)
         except _lib.LibraryError as error:
             raise B200BackendUnavailable(str(error)) from error
+        # fx_process hashes the output while it is still being copied back
+        ctx.check(_lib.load().fx_set_output_digest(ctx.handle, 1))
         _CONTEXTS[device] = ctx
         return ctx
 
@@ -200,6 +202,7 @@ class FrameOutcome:
     counters: _lib.FxCounters
     score: np.ndarray | None
     changed: np.ndarray | None
+    digest: bytes | None = None  # SHA-256 of the output, when the library computed it
 
 
 def run_frame(ctx: _lib.Context, main: np.ndarray, params: _lib.FxParams,
@@ -225,22 +228,30 @@ def run_frame(ctx: _lib.Context, main: np.ndarray, params: _lib.FxParams,
         changed_out=changed.ctypes.data if changed is not None else None,
     )
     counters = _lib.FxCounters()
+    digest = None
     with ctx.lock:
-        status = _lib.load().fx_process(ctx.handle, ctypes.byref(frame), ctypes.byref(counters))
+        lib = _lib.load()
+        status = lib.fx_process(ctx.handle, ctypes.byref(frame), ctypes.byref(counters))
         if status:
             try:
                 ctx.check(status)
             except _lib.LibraryError as error:
                 raise_library_error(error)
-    return FrameOutcome(out, counters, score, changed)
+        buf = (ctypes.c_uint8 * 32)()
+        if lib.fx_output_digest(ctx.handle, buf) == 0:
+            digest = bytes(buf)
+    return FrameOutcome(out, counters, score, changed, digest)
 
 
 def replay_result(outcome: FrameOutcome) -> StreamingReplayResult:
     c = outcome.counters
     h, w = outcome.output.shape[:2]
-    # little-endian uint16 bytes in row-major order, hashed in place (no copy)
-    out = np.ascontiguousarray(outcome.output.astype("<u2", copy=False))
-    digest = hashlib.sha256(memoryview(out).cast("B"))
+    if outcome.digest is not None:  # hashed by the library during the download
+        hexdigest = outcome.digest.hex()
+    else:
+        # little-endian uint16 bytes in row-major order, hashed in place (no copy)
+        out = np.ascontiguousarray(outcome.output.astype("<u2", copy=False))
+        hexdigest = hashlib.sha256(memoryview(out).cast("B")).hexdigest()
     return StreamingReplayResult(
         shape=(h, w, 3),
         startup=StartupReplayResult(
@@ -252,7 +263,7 @@ def replay_result(outcome: FrameOutcome) -> StreamingReplayResult:
         written_pixels=int(c.written),
         public_rng_advances=int(c.public_advances),
         final_rng_state=int(c.final_state),
-        output_sha256=digest.hexdigest(),
+        output_sha256=hexdigest,
         changed_pixels=int(c.changed),
     )
 

@@ -197,6 +197,14 @@ FX_API int fx_set_parallel_walk(fx_context *ctx, int enable);
  * candidate windows (less total work, for throughput when several frames
  * are in flight) and more waves (longer latency for one frame). */
 FX_API int fx_set_walk_wave(fx_context *ctx, int32_t segments);
+/* SHA-256 of the RGB16 output of fx_process, little-endian bytes in
+ * row-major order (the replay result's output_sha256, streaming.py:533-536).
+ * When enabled, fx_process hashes each staged chunk of the output as soon as
+ * its device-to-host copy lands, while the other chunks are still copied,
+ * instead of leaving a second pass over the output to the caller.
+ * fx_output_digest returns the digest of the last successful fx_process. */
+FX_API int fx_set_output_digest(fx_context *ctx, int enable);
+FX_API int fx_output_digest(fx_context *ctx, uint8_t *digest32);
 FX_API int fx_submit(fx_context *ctx, const fx_frame *frame, int64_t *ticket);
 /* fx_submit for a frame already in device memory: the pass is enqueued on
  * a free slot's stream and writes d_rgb_out / d_score_out / d_changed_out
