@@ -102,6 +102,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
     ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--no-routing", action="store_true",
+                    help="skip the at-floor routing census measurement")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched and serving runs")
     ap.add_argument("--batch-steps", type=int, default=3)
@@ -436,7 +438,67 @@ def run_b200(args, world, rank, local, frames=None):
         if frames is not None:
             line["batched"] = run_batched(ctx, frames, args, golden)
             line["serving"] = run_serving(ctx, frames, args)
+        if not args.no_routing:
+            line["routing"] = run_routing(ctx, d_in, h, w)
         print(json.dumps(line), flush=True)
+
+
+def run_routing(ctx, d_in, h, w, repeats: int = 3):
+    """The at-floor routing census (hybrid routing.py:447-793) on this frame's
+    own at-floor mask (score == floor), mask resident on the device.
+
+    Times route_at_floor_mask (labelling, distance, dilation, tables, the
+    three planes copied back) and serialize_routing_json on the host clock,
+    and the CPU restatement of the same census (the oracle, one thread) as
+    its baseline; checks the census bytes and planes against it."""
+
+    import torch
+
+    from fauxice_b200 import _lib, routing
+    from fauxice_b200.profile import DEFAULT_PROFILE, NIKON_PE_INITIAL_STATE
+    from oracle import routing_oracle as ro
+
+    lib = _lib.load()
+    params = DEFAULT_PROFILE.hot_path_parameters().to_c()
+    d_out = torch.empty((h, w, 3), dtype=torch.int16, device=d_in.device)
+    d_score = torch.empty((h, w), dtype=torch.float32, device=d_in.device)
+    ctx.check(lib.fx_process_device(ctx.handle, d_in.data_ptr(), h, w, ctypes.byref(params), None,
+                                    NIKON_PE_INITIAL_STATE, d_out.data_ptr(), d_score.data_ptr(),
+                                    None, None, None))
+    torch.cuda.synchronize()
+    at_floor = d_score == float(DEFAULT_PROFILE.score_floor())
+    routing.serialize_routing_json(routing.route_at_floor_mask(at_floor))  # warm
+    census, serialize = [], []
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        result = routing.route_at_floor_mask(at_floor)
+        t1 = time.perf_counter()
+        payload = routing.serialize_routing_json(result)
+        census.append(t1 - t0)
+        serialize.append(time.perf_counter() - t1)
+    host_mask = at_floor.cpu().numpy()
+    t0 = time.perf_counter()
+    doc, prov, synth, final = ro.route(host_mask)
+    expected = ro.serialize(doc)
+    oracle_s = time.perf_counter() - t0
+    exact = (payload == expected and np.array_equal(result.provisional_labels, prov)
+             and np.array_equal(result.synthesis_mask, synth)
+             and np.array_equal(result.final_labels, final))
+    best = min(c + s for c, s in zip(census, serialize))
+    return {
+        "workload": f"at-floor mask of the seed-2 {h}x{w} frame ({h * w / 1e6:.1f} MP, "
+                    f"{int(host_mask.sum())} at-floor pixels), default policy, device-resident",
+        "regions": len(result.provisional_regions),
+        "final_regions": len(result.final_regions),
+        "census_ms": round(1e3 * min(census), 2),
+        "serialize_ms": round(1e3 * min(serialize), 2),
+        "mp_per_s": round(h * w / 1e6 / best, 1),
+        "json_bytes": len(payload),
+        "bit_exact_vs_oracle": bool(exact),
+        "cpu_baseline": {"value": round(1e3 * oracle_s, 1), "unit": "ms", "cores": 1,
+                         "kind": "port", "sample": "the same mask, census and serialization"},
+        "timing": "host clock, best of 3 after one warm run",
+    }
 
 
 def run_batched(ctx, frames, args, golden):

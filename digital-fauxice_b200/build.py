@@ -19,7 +19,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "fauxice_b200", "libfauxice_b200.so")
 BUILD = os.path.join(HERE, "_build")
 SOURCES = ("fx_analysis.cu", "fx_writer.cu", "fx_walk.cu", "fx_prelude.cu", "fx_api.cu",
-           "fx_static.cu", "fx_route.cu")
+           "fx_static.cu", "fx_route.cu", "fx_census.cu")
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

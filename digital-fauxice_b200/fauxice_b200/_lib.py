@@ -171,6 +171,10 @@ SIGNATURES = {
     "fx_count_where": ([_P, _P, ctypes.c_int64, ctypes.c_int64, _P, _P], ctypes.c_int),
     "fx_tile_extract": ([_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                          ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _P, _P], ctypes.c_int),
+    "fx_census_provisional_json": ([ctypes.c_int64, _P, _P, _P, _P, _P, _P, _P, _P, _P,
+                                    ctypes.c_int64], ctypes.c_int64),
+    "fx_census_final_json": ([ctypes.c_int64, _P, _P, _P, _P, _P, _P, _P, _P, ctypes.c_int64],
+                             ctypes.c_int64),
     "fx_tile_scatter": ([_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
                          ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, _P, _P], ctypes.c_int),
 }

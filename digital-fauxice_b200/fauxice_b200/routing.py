@@ -19,6 +19,7 @@ from __future__ import annotations
 import ctypes
 import json
 import math
+import weakref
 from dataclasses import dataclass
 from enum import StrEnum
 from fractions import Fraction
@@ -170,6 +171,15 @@ def _check_plane(array: np.ndarray, *, name: str, dtype: np.dtype,
         raise ValueError(f"{name} must be read-only")
 
 
+def _check_planes(result) -> None:
+    _check_plane(result.provisional_labels, name="provisional_labels",
+                 dtype=np.dtype(np.int32), shape=result.image_shape)
+    _check_plane(result.synthesis_mask, name="synthesis_mask", dtype=np.dtype(np.bool_),
+                 shape=result.image_shape)
+    _check_plane(result.final_labels, name="final_labels", dtype=np.dtype(np.int32),
+                 shape=result.image_shape)
+
+
 @dataclass(frozen=True)
 class RoutingResult:
     """Region tables and planes of one routing decision (routing.py:187-241)."""
@@ -192,12 +202,7 @@ class RoutingResult:
     within_synthesis_budget: bool
 
     def __post_init__(self) -> None:
-        _check_plane(self.provisional_labels, name="provisional_labels",
-                     dtype=np.dtype(np.int32), shape=self.image_shape)
-        _check_plane(self.synthesis_mask, name="synthesis_mask", dtype=np.dtype(np.bool_),
-                     shape=self.image_shape)
-        _check_plane(self.final_labels, name="final_labels", dtype=np.dtype(np.int32),
-                     shape=self.image_shape)
+        _check_planes(self)
         if not np.array_equal(self.final_labels > 0, self.synthesis_mask):
             raise ValueError("positive final labels must equal synthesis_mask")
 
@@ -216,12 +221,9 @@ def routed_reasons(areas: np.ndarray, radii: np.ndarray,
                    policy: RoutingPolicy) -> list[RoutedReason]:
     """Per-component reason from the two thresholds (routing.py:281-295)."""
 
-    area_hit = areas >= policy.min_area
-    radius_hit = radii >= policy.min_radius
-    table = (RoutedReason.NOT_ROUTED, RoutedReason.CHESSBOARD_RADIUS, RoutedReason.AREA,
-             RoutedReason.AREA_AND_CHESSBOARD_RADIUS)
-    codes = area_hit.astype(np.int64) * 2 + radius_hit.astype(np.int64)
-    return [table[c] for c in codes.tolist()]
+    codes = (np.asarray(areas) >= policy.min_area).astype(np.int64) * 2 + (
+        np.asarray(radii) >= policy.min_radius)
+    return [_REASONS[c] for c in codes.tolist()]
 
 
 def within_budget(synthesis_pixels: int, frame_pixels: int, maximum_fraction: float) -> bool:
@@ -262,6 +264,23 @@ class _Device:
         self.dev = torch.device("cuda", torch.cuda.current_device())
         self.stream = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
         self.err = torch.zeros(4, dtype=torch.int64, device=self.dev)  # err / flag / counter
+        self.copy_stream = torch.cuda.Stream(device=self.dev)
+
+    def download(self, t):
+        """Start copying device tensor ``t`` (in its final state) into pinned
+        host memory on the copy stream; the host tensor is valid after
+        finish_downloads."""
+
+        host = self.torch.empty(tuple(t.shape), dtype=t.dtype, pin_memory=True)
+        ready = self.torch.cuda.Event()
+        ready.record(self.torch.cuda.current_stream(self.dev))
+        self.copy_stream.wait_event(ready)
+        with self.torch.cuda.stream(self.copy_stream):
+            host.copy_(t, non_blocking=True)
+        return host
+
+    def finish_downloads(self) -> None:
+        self.copy_stream.synchronize()
 
     def empty(self, shape, dtype):
         return self.torch.empty(shape, dtype=dtype, device=self.dev)
@@ -481,6 +500,32 @@ def _read_only(array: np.ndarray) -> np.ndarray:
     return array
 
 
+_REASONS = (RoutedReason.NOT_ROUTED, RoutedReason.CHESSBOARD_RADIUS, RoutedReason.AREA,
+            RoutedReason.AREA_AND_CHESSBOARD_RADIUS)
+_ROUTED, _ABSORBED, _PRISTINE, _EXCLUDED = 0, 1, 2, 3
+_DISPOSITIONS = (RegionDisposition.ROUTED, RegionDisposition.ABSORBED,
+                 RegionDisposition.PRISTINE, RegionDisposition.PERIMETER_EXCLUDED)
+_new = object.__new__
+
+
+def _box(y0: int, x0: int, y1: int, x1: int) -> BoundingBox:
+    """A BoundingBox from device-measured extents (valid by construction)."""
+
+    b = _new(BoundingBox)
+    d = b.__dict__
+    d["y0"], d["x0"], d["y1"], d["x1"] = y0, x0, y1, x1
+    return b
+
+
+def _grouped(keys: np.ndarray, values: np.ndarray, count: int):
+    """values split by key 1..count (keys sorted ascending): the per-key
+    tuples, and the count + 1 offsets of the key ranges."""
+
+    offsets = np.searchsorted(keys, np.arange(1, count + 2)).astype(np.int64)
+    bounds, vals = offsets.tolist(), values.tolist()
+    return [tuple(vals[bounds[i]:bounds[i + 1]]) for i in range(count)], offsets
+
+
 def route_at_floor_mask(at_floor_mask, policy: RoutingPolicy = RoutingPolicy()) -> RoutingResult:
     """Measure and route an at-floor mask (routing.py:447-682) on the GPU.
 
@@ -502,10 +547,11 @@ def route_at_floor_mask(at_floor_mask, policy: RoutingPolicy = RoutingPolicy()) 
     areas, boxes, radii = dev.stats(prov, dist, height, width, k)
     if int(areas.sum()) == n:
         raise NoHealthyContextError((height, width))
+    prov_host = dev.download(prov)  # overlaps the rest of the census
 
-    reasons = routed_reasons(areas, radii, policy)
+    codes = (areas >= policy.min_area).astype(np.int64) * 2 + (radii >= policy.min_radius)
     perimeter_id = _perimeter_component(dev, prov)
-    direct = np.array([r is not RoutedReason.NOT_ROUTED for r in reasons], dtype=np.bool_)
+    direct = codes != 0
     if perimeter_id is not None:
         direct[perimeter_id - 1] = False
     routed_table = np.zeros(k + 1, np.int32)
@@ -516,76 +562,132 @@ def route_at_floor_mask(at_floor_mask, policy: RoutingPolicy = RoutingPolicy()) 
     halo = 0
     if perimeter_id is not None:
         halo = dev.clear_label(synthesis, prov, perimeter_id)
+    synthesis_host = dev.download(synthesis)
 
     final, final_boxes = _final_labels(dev, synthesis, height, width)
+    final_host = dev.download(final)
     final_count = len(final_boxes)
     final_areas, check_boxes, _ = dev.stats(final, None, height, width, final_count)
     if not np.array_equal(check_boxes, final_boxes):
         raise RuntimeError("final label boxes disagree with their fragments")
 
-    overlap = dev.count_where(prov, final, k)            # at-floor pixels synthesised, per region
+    # overlap accounting (routing.py:528-556): per-region synthesised at-floor
+    # pixels, per-final at-floor pixels, and the distinct (region, final) pairs
+    overlap = dev.count_where(prov, final, k)
     final_floor = dev.count_where(final, prov, final_count)
-    final_ids: list[list[int]] = [[] for _ in range(k)]
-    direct_ids: list[list[int]] = [[] for _ in range(final_count)]
-    absorbed_ids: list[list[int]] = [[] for _ in range(final_count)]
-    for pid, fid in dev.pairs(prov, final, height, width).tolist():
-        if pid == perimeter_id:
-            raise RuntimeError("perimeter-excluded region entered synthesis mask")
-        final_ids[pid - 1].append(fid)
-        (direct_ids if direct[pid - 1] else absorbed_ids)[fid - 1].append(pid)
+    pairs = dev.pairs(prov, final, height, width)     # sorted by (region, final)
+    pids, fids = pairs[:, 0], pairs[:, 1]
+    if perimeter_id is not None and (np.any(pids == perimeter_id) or overlap[perimeter_id]):
+        raise RuntimeError("perimeter-excluded region entered synthesis mask")
+    synthesised = overlap[1:]
+    disposition = np.where(direct, _ROUTED, np.where(synthesised > 0, _ABSORBED, _PRISTINE))
+    if perimeter_id is not None:
+        disposition[perimeter_id - 1] = _EXCLUDED
+    final_ids, final_offsets = _grouped(pids, fids, k)
+    if direct.any() and not np.all(np.isin(np.flatnonzero(direct) + 1, pids)):
+        raise RuntimeError("directly routed region lost its final binding")
+    by_final = np.lexsort((pids, fids))                # (final, region) order
+    direct_pair = direct[pids[by_final] - 1]
+    direct_vals, absorbed_vals = pids[by_final][direct_pair], pids[by_final][~direct_pair]
+    direct_ids, direct_offsets = _grouped(fids[by_final][direct_pair], direct_vals, final_count)
+    absorbed_ids, absorbed_offsets = _grouped(fids[by_final][~direct_pair], absorbed_vals,
+                                              final_count)
+    absorbed = np.where(disposition == _ABSORBED, synthesised, 0)
 
-    regions: list[ProvisionalRegion] = []
-    for i in range(1, k + 1):
-        synthesised = int(overlap[i])
-        if i == perimeter_id:
-            if synthesised:
-                raise RuntimeError("perimeter-excluded region entered synthesis mask")
-            disposition, absorbed = RegionDisposition.PERIMETER_EXCLUDED, 0
-        elif direct[i - 1]:
-            if not final_ids[i - 1]:
-                raise RuntimeError("directly routed region lost its final binding")
-            disposition, absorbed = RegionDisposition.ROUTED, 0
-        elif synthesised:
-            disposition, absorbed = RegionDisposition.ABSORBED, synthesised
-        else:
-            disposition, absorbed = RegionDisposition.PRISTINE, 0
-        b = boxes[i - 1]
-        regions.append(ProvisionalRegion(
-            id=i, bbox=BoundingBox(int(b[0]), int(b[1]), int(b[2]), int(b[3])),
-            area=int(areas[i - 1]), max_chessboard_radius=int(radii[i - 1]),
-            routed_reason=reasons[i - 1], disposition=disposition,
-            final_component_ids=tuple(final_ids[i - 1]), absorbed_pixel_count=absorbed))
-
-    finals = tuple(
-        FinalSynthesisRegion(
-            id=f, bbox=BoundingBox(*(int(v) for v in final_boxes[f - 1])),
-            area=int(final_areas[f - 1]), direct_region_ids=tuple(direct_ids[f - 1]),
-            absorbed_region_ids=tuple(absorbed_ids[f - 1]),
-            non_floor_synth_pixel_count=int(final_areas[f - 1] - final_floor[f]))
-        for f in range(1, final_count + 1))
+    regions = []
+    box_rows, area_l, radius_l = boxes.tolist(), areas.tolist(), radii.tolist()
+    code_l, disp_l, absorbed_l = codes.tolist(), disposition.tolist(), absorbed.tolist()
+    for i in range(k):
+        r = _new(ProvisionalRegion)
+        r.__dict__.update(id=i + 1, bbox=_box(*box_rows[i]), area=area_l[i],
+                          max_chessboard_radius=radius_l[i], routed_reason=_REASONS[code_l[i]],
+                          disposition=_DISPOSITIONS[disp_l[i]], final_component_ids=final_ids[i],
+                          absorbed_pixel_count=absorbed_l[i])
+        regions.append(r)
+    finals = []
+    fbox_rows, farea_l = final_boxes.tolist(), final_areas.tolist()
+    ffloor_l = final_floor.tolist()
+    for f in range(final_count):
+        r = _new(FinalSynthesisRegion)
+        r.__dict__.update(id=f + 1, bbox=_box(*fbox_rows[f]), area=farea_l[f],
+                          direct_region_ids=direct_ids[f], absorbed_region_ids=absorbed_ids[f],
+                          non_floor_synth_pixel_count=farea_l[f] - ffloor_l[f + 1])
+        finals.append(r)
 
     at_floor = int(areas.sum())
-    directly_routed = sum(r.area for r in regions if r.disposition is RegionDisposition.ROUTED)
-    absorbed_total = sum(r.absorbed_pixel_count for r in regions
-                         if r.disposition is RegionDisposition.ABSORBED)
+    directly_routed = int(areas[disposition == _ROUTED].sum())
+    absorbed_total = int(absorbed.sum())
     synthesis_pixels = int(final_areas.sum())
-    non_floor = synthesis_pixels - int(overlap[1:].sum())
+    non_floor = synthesis_pixels - int(synthesised.sum())
     if synthesis_pixels != directly_routed + absorbed_total + non_floor:
         raise RuntimeError("synthesis pixel accounting is not conservative")
 
-    return RoutingResult(
+    dev.finish_downloads()
+    fields = dict(
         image_shape=(height, width), policy=policy, provisional_regions=tuple(regions),
-        final_regions=finals,
-        provisional_labels=_read_only(prov.cpu().numpy()),
-        synthesis_mask=_read_only(synthesis.cpu().numpy().view(np.bool_)),
-        final_labels=_read_only(final.cpu().numpy()),
-        at_floor_pixel_count=at_floor, directly_routed_pixel_count=int(directly_routed),
+        final_regions=tuple(finals),
+        provisional_labels=_read_only(prov_host.numpy()),
+        synthesis_mask=_read_only(synthesis_host.numpy().view(np.bool_)),
+        final_labels=_read_only(final_host.numpy()),
+        at_floor_pixel_count=at_floor, directly_routed_pixel_count=directly_routed,
         perimeter_excluded_region_count=int(perimeter_id is not None),
         perimeter_excluded_pixel_count=(int(areas[perimeter_id - 1])
                                         if perimeter_id is not None else 0),
         perimeter_suppressed_halo_pixel_count=halo, synthesis_pixel_count=synthesis_pixels,
         non_floor_synth_pixel_count=non_floor, synthesis_fraction=synthesis_pixels / n,
         within_synthesis_budget=within_budget(synthesis_pixels, n, policy.max_synth_fraction))
+    # The planes' dtype, shape, contiguity and read-only flags are checked as
+    # in the constructor; the full-plane (final_labels > 0) == synthesis_mask
+    # comparison is skipped because it holds by construction (the final
+    # labels are the labelling of the synthesis mask), and the GPU tests
+    # compare both planes with the oracle's.
+    result = _new(RoutingResult)
+    result.__dict__.update(fields)
+    _check_planes(result)
+    _attach_tables(result, _CensusTables(
+        boxes=np.ascontiguousarray(boxes, np.int64), areas=areas.astype(np.int64),
+        radii=radii.astype(np.int64), reasons=codes.astype(np.int32),
+        dispositions=disposition.astype(np.int32), absorbed=absorbed.astype(np.int64),
+        final_offsets=final_offsets, final_ids=np.ascontiguousarray(fids, np.int64),
+        final_boxes=np.ascontiguousarray(final_boxes, np.int64),
+        final_areas=final_areas.astype(np.int64), direct_offsets=direct_offsets,
+        direct_ids=np.ascontiguousarray(direct_vals, np.int64), absorbed_offsets=absorbed_offsets,
+        absorbed_ids=np.ascontiguousarray(absorbed_vals, np.int64),
+        non_floor=(final_areas - final_floor[1:]).astype(np.int64)))
+    return result
+
+
+@dataclass(frozen=True)
+class _CensusTables:
+    """Flat region tables of a device-built result, for the native JSON writer."""
+
+    boxes: np.ndarray
+    areas: np.ndarray
+    radii: np.ndarray
+    reasons: np.ndarray
+    dispositions: np.ndarray
+    absorbed: np.ndarray
+    final_offsets: np.ndarray
+    final_ids: np.ndarray
+    final_boxes: np.ndarray
+    final_areas: np.ndarray
+    direct_offsets: np.ndarray
+    direct_ids: np.ndarray
+    absorbed_offsets: np.ndarray
+    absorbed_ids: np.ndarray
+    non_floor: np.ndarray
+
+
+# Tables of live device-built results, by id(result); an entry goes when its
+# result is collected.  Results built any other way are serialized from
+# their region objects.
+_TABLES: dict[int, _CensusTables] = {}
+
+
+def _attach_tables(result: RoutingResult, tables: _CensusTables) -> None:
+    key = id(result)
+    _TABLES[key] = tables
+    weakref.finalize(result, _TABLES.pop, key, None)
 
 
 def routing_json_document(result: RoutingResult) -> dict[str, object]:
@@ -593,6 +695,37 @@ def routing_json_document(result: RoutingResult) -> dict[str, object]:
 
     if not isinstance(result, RoutingResult):
         raise TypeError("result must be a RoutingResult")
+    doc = _document_head(result)
+    doc["provisional_regions"] = [
+        {
+            "id": r.id,
+            "bbox_yxyx_half_open": r.bbox.as_list(),
+            "area": r.area,
+            "max_chessboard_radius": r.max_chessboard_radius,
+            "routed_reason": r.routed_reason.value,
+            "disposition": r.disposition.value,
+            "final_component_ids": list(r.final_component_ids),
+            "absorbed_pixel_count": r.absorbed_pixel_count,
+        }
+        for r in result.provisional_regions
+    ]
+    doc["final_regions"] = [
+        {
+            "id": r.id,
+            "bbox_yxyx_half_open": r.bbox.as_list(),
+            "area": r.area,
+            "direct_region_ids": list(r.direct_region_ids),
+            "absorbed_region_ids": list(r.absorbed_region_ids),
+            "non_floor_synthesis_pixels": r.non_floor_synth_pixel_count,
+        }
+        for r in result.final_regions
+    ]
+    return doc
+
+
+def _document_head(result: RoutingResult) -> dict[str, object]:
+    """Every key of the census document except the two region lists."""
+
     excluded = next((r for r in result.provisional_regions
                      if r.disposition is RegionDisposition.PERIMETER_EXCLUDED), None)
     height, width = result.image_shape
@@ -645,39 +778,62 @@ def routing_json_document(result: RoutingResult) -> dict[str, object]:
             "predicate": "contains_every_frame_perimeter_pixel",
             "content_interpretation": "unverified",
         },
-        "provisional_regions": [
-            {
-                "id": r.id,
-                "bbox_yxyx_half_open": r.bbox.as_list(),
-                "area": r.area,
-                "max_chessboard_radius": r.max_chessboard_radius,
-                "routed_reason": r.routed_reason.value,
-                "disposition": r.disposition.value,
-                "final_component_ids": list(r.final_component_ids),
-                "absorbed_pixel_count": r.absorbed_pixel_count,
-            }
-            for r in result.provisional_regions
-        ],
-        "final_regions": [
-            {
-                "id": r.id,
-                "bbox_yxyx_half_open": r.bbox.as_list(),
-                "area": r.area,
-                "direct_region_ids": list(r.direct_region_ids),
-                "absorbed_region_ids": list(r.absorbed_region_ids),
-                "non_floor_synthesis_pixels": r.non_floor_synth_pixel_count,
-            }
-            for r in result.final_regions
-        ],
     }
 
 
-def serialize_routing_json(result: RoutingResult) -> bytes:
-    """Canonical UTF-8 JSON of the census (routing.py:782-793)."""
+def _dumps(doc: dict) -> bytes:
+    return json.dumps(doc, ensure_ascii=False, allow_nan=False, sort_keys=True,
+                      separators=(",", ":")).encode("utf-8")
 
-    payload = json.dumps(routing_json_document(result), ensure_ascii=False, allow_nan=False,
-                         sort_keys=True, separators=(",", ":"))
-    return payload.encode("utf-8") + b"\n"
+
+_PROVISIONAL_MARK, _FINAL_MARK = "@@provisional_regions@@", "@@final_regions@@"
+
+
+def _native_lists(tables: _CensusTables) -> tuple[bytes, bytes]:
+    """The two region lists written by the library from the flat tables."""
+
+    lib = _lib.load()
+    p = _lib.ptr
+    k, f = len(tables.areas), len(tables.final_areas)
+    cap = 256 + k * 330 + 21 * len(tables.final_ids)
+    buf = np.empty(cap, np.uint8)
+    n = lib.fx_census_provisional_json(
+        k, p(tables.boxes), p(tables.areas), p(tables.radii), p(tables.reasons),
+        p(tables.dispositions), p(tables.absorbed), p(tables.final_offsets), p(tables.final_ids),
+        p(buf), cap)
+    if n < 0:
+        raise RuntimeError("fx_census_provisional_json failed")
+    provisional = buf[:n].tobytes()
+    cap = 256 + f * 250 + 21 * (len(tables.direct_ids) + len(tables.absorbed_ids))
+    buf = np.empty(cap, np.uint8)
+    n = lib.fx_census_final_json(
+        f, p(tables.final_boxes), p(tables.final_areas), p(tables.direct_offsets),
+        p(tables.direct_ids), p(tables.absorbed_offsets), p(tables.absorbed_ids),
+        p(tables.non_floor), p(buf), cap)
+    if n < 0:
+        raise RuntimeError("fx_census_final_json failed")
+    return provisional, buf[:n].tobytes()
+
+
+def serialize_routing_json(result: RoutingResult) -> bytes:
+    """Canonical UTF-8 JSON of the census (routing.py:782-793).
+
+    For a result of route_at_floor_mask the two region lists are written by
+    the library from the result's flat tables (same bytes, one pass); other
+    results are serialized from their region objects."""
+
+    if not isinstance(result, RoutingResult):
+        raise TypeError("result must be a RoutingResult")
+    tables = _TABLES.get(id(result))
+    if tables is None:
+        return _dumps(routing_json_document(result)) + b"\n"
+    head = _document_head(result)
+    head["provisional_regions"], head["final_regions"] = _PROVISIONAL_MARK, _FINAL_MARK
+    provisional, final = _native_lists(tables)
+    text = _dumps(head)
+    text = text.replace(b'"' + _PROVISIONAL_MARK.encode() + b'"', provisional, 1)
+    text = text.replace(b'"' + _FINAL_MARK.encode() + b'"', final, 1)
+    return text + b"\n"
 
 
 __all__ = [

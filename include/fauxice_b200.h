@@ -298,6 +298,26 @@ FX_API int fx_tile_scatter(const int32_t *d_tile_labels, int32_t h, int32_t w, i
                            int32_t x0, int32_t th, int32_t tw, int32_t base, int32_t *d_plane,
                            void *stream);
 
+/* Canonical JSON text of the census's two region lists (host code): the
+ * "provisional_regions" and "final_regions" arrays of routing_json_document
+ * (routing.py:736-777) as serialize_routing_json writes them (sorted keys, no
+ * whitespace, routing.py:782-793).  Tables are flat, ids run 1..count in
+ * order; box holds [y0, x0, y1, x1) per region; each id list is an offset
+ * range (count + 1 offsets) into its values.  reason and disposition are
+ * codes: reason 0 not_routed, 1 chessboard_radius, 2 area,
+ * 3 area+chessboard_radius; disposition 0 routed, 1 absorbed, 2 pristine,
+ * 3 perimeter_excluded.  Returns the bytes written, or -1 for a bad argument
+ * or too small a buffer. */
+FX_API int64_t fx_census_provisional_json(int64_t k, const int64_t *box, const int64_t *area,
+                                          const int64_t *radius, const int32_t *reason,
+                                          const int32_t *disposition, const int64_t *absorbed,
+                                          const int64_t *final_offsets, const int64_t *final_ids,
+                                          char *out, int64_t capacity);
+FX_API int64_t fx_census_final_json(int64_t count, const int64_t *box, const int64_t *area,
+                                    const int64_t *direct_offsets, const int64_t *direct_ids,
+                                    const int64_t *absorbed_offsets, const int64_t *absorbed_ids,
+                                    const int64_t *non_floor, char *out, int64_t capacity);
+
 #ifdef __cplusplus
 }
 #endif

@@ -113,6 +113,77 @@ def test_census_document_matches_reference_bytes(name, route_golden):
     assert sha(routing.serialize_routing_json(result)) == expected["json_sha256"]
 
 
+_REASON_CODE = {"not_routed": 0, "chessboard_radius": 1, "area": 2, "area+chessboard_radius": 3}
+_DISPOSITION_CODE = {"routed": 0, "absorbed": 1, "pristine": 2, "perimeter_excluded": 3}
+
+
+def _offsets(lists):
+    offsets = np.zeros(len(lists) + 1, np.int64)
+    offsets[1:] = np.cumsum([len(v) for v in lists])
+    values = np.array([x for v in lists for x in v], dtype=np.int64)
+    return offsets, values
+
+
+def tables_from_oracle(doc: dict) -> "routing._CensusTables":
+    prov, fin = doc["provisional_regions"], doc["final_regions"]
+    i64 = lambda v: np.array(v, dtype=np.int64).reshape(-1)  # noqa: E731
+    final_offsets, final_ids = _offsets([r["final_component_ids"] for r in prov])
+    direct_offsets, direct_ids = _offsets([r["direct_region_ids"] for r in fin])
+    absorbed_offsets, absorbed_ids = _offsets([r["absorbed_region_ids"] for r in fin])
+    return routing._CensusTables(
+        boxes=np.array([r["bbox_yxyx_half_open"] for r in prov], np.int64).reshape(-1, 4),
+        areas=i64([r["area"] for r in prov]), radii=i64([r["max_chessboard_radius"] for r in prov]),
+        reasons=np.array([_REASON_CODE[r["routed_reason"]] for r in prov], np.int32),
+        dispositions=np.array([_DISPOSITION_CODE[r["disposition"]] for r in prov], np.int32),
+        absorbed=i64([r["absorbed_pixel_count"] for r in prov]),
+        final_offsets=final_offsets, final_ids=final_ids,
+        final_boxes=np.array([r["bbox_yxyx_half_open"] for r in fin], np.int64).reshape(-1, 4),
+        final_areas=i64([r["area"] for r in fin]), direct_offsets=direct_offsets,
+        direct_ids=direct_ids, absorbed_offsets=absorbed_offsets, absorbed_ids=absorbed_ids,
+        non_floor=i64([r["non_floor_synthesis_pixels"] for r in fin]))
+
+
+@pytest.mark.parametrize("name", [n for n in route_cases.CASES
+                                  if not route_cases.CASES[n].get("slow")])
+def test_native_region_writer_matches_reference_bytes(name, route_golden):
+    """The library's region-list writer, fed flat tables, gives the
+    reference's canonical bytes (host code: no GPU needed)."""
+
+    expected = route_golden[name]
+    if "error" in expected:
+        pytest.skip("the reference raised for this mask")
+    policy = routing.RoutingPolicy(**route_cases.policy_kwargs(name))
+    mask = route_cases.mask(name)
+    result = result_from_oracle(mask, policy)
+    doc, *_ = ro.route(mask, **route_cases.policy_kwargs(name))
+    routing._attach_tables(result, tables_from_oracle(doc))
+    assert id(result) in routing._TABLES
+    assert sha(routing.serialize_routing_json(result)) == expected["json_sha256"]
+    key = id(result)
+    del result
+    assert key not in routing._TABLES  # the side table follows the result's lifetime
+
+
+def test_native_writer_rejects_short_buffers_and_bad_codes():
+    from fauxice_b200 import _lib
+
+    lib = _lib.load()
+    z = np.zeros(4, np.int64)
+    offsets = np.zeros(2, np.int64)
+    codes = np.zeros(1, np.int32)
+    buf = np.empty(8, np.uint8)
+    p = _lib.ptr
+    assert lib.fx_census_provisional_json(1, p(z), p(z), p(z), p(codes), p(codes), p(z),
+                                          p(offsets), p(z), p(buf), 8) == -1
+    bad = np.array([7], np.int32)
+    big = np.empty(4096, np.uint8)
+    assert lib.fx_census_provisional_json(1, p(z), p(z), p(z), p(bad), p(codes), p(z),
+                                          p(offsets), p(z), p(big), 4096) == -1
+    assert lib.fx_census_final_json(0, None, None, None, None, None, None, None, p(big),
+                                    4096) == 2
+    assert big[:2].tobytes() == b"[]"
+
+
 def test_budget_is_an_exact_rational_test():
     assert routing.within_budget(2, 100, 0.02)
     assert not routing.within_budget(3, 100, 0.02)
