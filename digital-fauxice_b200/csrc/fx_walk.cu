@@ -60,6 +60,24 @@ __device__ __forceinline__ uint32_t jump_t(uint32_t t0, uint64_t n) {
     return f.a * t0 + f.c;
 }
 
+// Steps n with G^n(from) = to (T space, 24-bit state in the high bits), by
+// matching one bit per round: G^(2^j) leaves the bits below j unchanged and
+// flips bit j (full-period LCG: multiplier 1 mod 4, odd increment).
+__device__ __forceinline__ uint32_t lcg_distance_t(uint32_t from_t, uint32_t to_t) {
+    uint32_t cur = from_t >> 8, target = to_t >> 8, a = 125u, c = 1u, d = 0u;
+#pragma unroll
+    for (int j = 0; j < 24; ++j) {
+        const uint32_t bit = 1u << j;
+        if ((cur ^ target) & bit) {
+            cur = (a * cur + c) & 0xFFFFFFu;
+            d |= bit;
+        }
+        c = (a + 1u) * c;
+        a = a * a;
+    }
+    return d;
+}
+
 __device__ __forceinline__ bool copies(const uint4 &lw, uint32_t T) {
     return ((T - lw.x) <= lw.y) | ((T - lw.z) <= lw.w);
 }
@@ -209,8 +227,8 @@ static_assert(kWinSlots <= 32, "live mask is 32 bits");
 // step.
 template <int SLOTS, int LEN>
 __device__ __forceinline__ void walk_group(const uint4 *r4, uint32_t r, bool tail_next,
-                                           uint32_t (&rE)[kWinSlots], uint32_t (&rT)[kWinSlots],
-                                           uint32_t live_mask, uint32_t &steps) {
+                                           uint32_t (&rT)[kWinSlots], uint32_t live_mask,
+                                           uint32_t &steps) {
     uint4 lw[LEN], ac[LEN];
 #pragma unroll
     for (int k = 0; k < LEN; ++k) {
@@ -222,38 +240,33 @@ __device__ __forceinline__ void walk_group(const uint4 *r4, uint32_t r, bool tai
 #pragma unroll
     for (int k = 0; k < LEN; ++k) {
 #pragma unroll
-        for (int s = 0; s < SLOTS; ++s) {
-            const uint32_t x = copies(lw[k], rT[s]) ? 0u : 1u;
-            rE[s] += x;
-            rT[s] = x ? ac[k].z * rT[s] + ac[k].w : ac[k].x * rT[s] + ac[k].y;
-        }
+        for (int s = 0; s < SLOTS; ++s)
+            rT[s] = copies(lw[k], rT[s]) ? ac[k].x * rT[s] + ac[k].y : ac[k].z * rT[s] + ac[k].w;
     }
 }
 
 // Single channels (segment and compaction boundaries).
 template <int SLOTS>
 __device__ __forceinline__ void walk_one(const uint4 *r4, uint32_t r, bool has_next,
-                                         uint32_t (&rE)[kWinSlots], uint32_t (&rT)[kWinSlots],
-                                         uint32_t live_mask, uint32_t &steps) {
+                                         uint32_t (&rT)[kWinSlots], uint32_t live_mask,
+                                         uint32_t &steps) {
     const uint4 lw = r4[2 * r];
     const uint4 ac = r4[2 * (r + (has_next ? 1u : 0u)) + 1];
     steps += (uint32_t)__popc(live_mask & ((1u << SLOTS) - 1u));
 #pragma unroll
-    for (int s = 0; s < SLOTS; ++s) {
-        const uint32_t x = copies(lw, rT[s]) ? 0u : 1u;
-        rE[s] += x;
-        rT[s] = x ? ac.z * rT[s] + ac.w : ac.x * rT[s] + ac.y;
-    }
+    for (int s = 0; s < SLOTS; ++s)
+        rT[s] = copies(lw, rT[s]) ? ac.x * rT[s] + ac.y : ac.z * rT[s] + ac.w;
 }
 
-// Warp-local merge: lanes of one slot hold consecutive candidates.
+// Warp-local merge: lanes of one slot hold consecutive candidates; equal
+// states mean equal counts.
 template <int SLOTS>
-__device__ __forceinline__ void warp_merge(const uint32_t (&rE)[kWinSlots], uint32_t &live_mask) {
+__device__ __forceinline__ void warp_merge(const uint32_t (&rT)[kWinSlots], uint32_t &live_mask) {
     const int lane = threadIdx.x & 31;
 #pragma unroll
     for (int s = 0; s < SLOTS; ++s) {
         const bool alive = live_mask & (1u << s);
-        uint32_t x = alive ? rE[s] : kNone;
+        uint32_t x = alive ? rT[s] : kNone;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
@@ -261,7 +274,7 @@ __device__ __forceinline__ void warp_merge(const uint32_t (&rE)[kWinSlots], uint
         }
         uint32_t prev = __shfl_up_sync(0xFFFFFFFFu, x, 1);
         if (lane == 0) prev = kNone;
-        if (alive && rE[s] == prev) live_mask &= ~(1u << s);
+        if (alive && rT[s] == prev) live_mask &= ~(1u << s);
     }
 }
 
@@ -269,25 +282,25 @@ __device__ __forceinline__ void warp_merge(const uint32_t (&rE)[kWinSlots], uint
 template <int SLOTS>
 __device__ __forceinline__ void walk_span(const uint4 *r4, uint32_t r, uint32_t stop,
                                           bool end_next, uint32_t merge_len,
-                                          uint32_t (&rE)[kWinSlots], uint32_t (&rT)[kWinSlots],
-                                          uint32_t &live_mask, uint32_t &steps) {
+                                          uint32_t (&rT)[kWinSlots], uint32_t &live_mask,
+                                          uint32_t &steps) {
     // many slots give their own parallelism: stage fewer channels at once
-    constexpr int kLen = SLOTS <= 2 ? 8 : (SLOTS <= 8 ? 4 : 2);
+    constexpr int kLen = SLOTS == 1 ? 16 : (SLOTS <= 2 ? 8 : (SLOTS <= 8 ? 4 : 2));
     uint32_t since = 0;
     while (r < stop) {
         if (r + kLen <= stop) {
             const bool tail_next = (r + kLen < stop) || end_next;
-            walk_group<SLOTS, kLen>(r4, r, tail_next, rE, rT, live_mask, steps);
+            walk_group<SLOTS, kLen>(r4, r, tail_next, rT, live_mask, steps);
             r += kLen;
             since += kLen;
         } else {
             const bool has_next = (r + 1 < stop) || end_next;
-            walk_one<SLOTS>(r4, r, has_next, rE, rT, live_mask, steps);
+            walk_one<SLOTS>(r4, r, has_next, rT, live_mask, steps);
             r += 1;
             since += 1;
         }
         if (since >= merge_len || r == stop) {
-            warp_merge<SLOTS>(rE, live_mask);
+            warp_merge<SLOTS>(rT, live_mask);
             since = 0;
         }
     }
@@ -351,7 +364,7 @@ __global__ void __launch_bounds__(kWinThreads, kWinBlocksPerSM)
 
     // candidates in list order k = slot * kWinThreads + tid; E_in of the
     // candidate at list position k is S.ein[k] (kept in shared memory)
-    uint32_t rE[kWinSlots], rT[kWinSlots];
+    uint32_t rT[kWinSlots];
     uint32_t live_mask = 0;
     uint32_t live = count;
     {
@@ -360,7 +373,6 @@ __global__ void __launch_bounds__(kWinThreads, kWinBlocksPerSM)
 #pragma unroll
         for (int s = 0; s < kWinSlots; ++s) {
             const uint32_t k = s * kWinThreads + tid;
-            rE[s] = wlo + k;
             rT[s] = t;
             if (k < live) live_mask |= 1u << s;
             S.ein[k] = wlo + k;
@@ -380,9 +392,12 @@ __global__ void __launch_bounds__(kWinThreads, kWinBlocksPerSM)
     };
 
     // Block-wide merge and compaction.  List order is slot-major
-    // (k = slot * kWinThreads + tid) and E is non-decreasing along it; after
-    // warp_merge the live values of one warp-slot are strictly increasing, so
-    // only its first live lane can equal the last live value before it.
+    // (k = slot * kWinThreads + tid) and E is non-decreasing along it.  The
+    // candidates carry only their state T: at one channel, equal T means
+    // equal E (distinct counts of one window are far closer than the LCG's
+    // 2^24 period).  After warp_merge the live values of one warp-slot are
+    // distinct, so only its first live lane can equal the last live value
+    // before it.
     auto merge_and_compact = [&](int slots) {
         const int lane = tid & 31, warp = tid >> 5;
         constexpr int kW = kWinThreads / 32;
@@ -393,7 +408,7 @@ __global__ void __launch_bounds__(kWinThreads, kWinBlocksPerSM)
             if (s < slots) {  // block-uniform
                 const bool alive = live_mask & (1u << s);
                 const uint32_t bal = __ballot_sync(0xFFFFFFFFu, alive);
-                const uint32_t last = bal ? __shfl_sync(0xFFFFFFFFu, rE[s], 31 - __clz(bal)) : kNone;
+                const uint32_t last = bal ? __shfl_sync(0xFFFFFFFFu, rT[s], 31 - __clz(bal)) : kNone;
                 if (lane == 0) S.wlast[s * kW + warp] = last;
                 if (alive) ein[s] = S.ein[s * kWinThreads + tid];
             }
@@ -415,7 +430,7 @@ __global__ void __launch_bounds__(kWinThreads, kWinBlocksPerSM)
                             break;
                         }
                     }
-                    if (prev == rE[s]) live_mask &= ~(1u << s);
+                    if (prev == rT[s]) live_mask &= ~(1u << s);
                 }
                 const uint32_t cnt = __popc(__ballot_sync(0xFFFFFFFFu, live_mask & (1u << s)));
                 if (lane == 0) S.wcount[s * kW + warp] = cnt;
@@ -452,7 +467,6 @@ __global__ void __launch_bounds__(kWinThreads, kWinBlocksPerSM)
                 if (alive) {
                     const uint32_t at = base + __popc(bal & ((1u << lane) - 1u));
                     S.ein[at] = ein[s];
-                    S.e[at] = rE[s];
                     S.t[at] = rT[s];
                 }
             }
@@ -465,7 +479,6 @@ __global__ void __launch_bounds__(kWinThreads, kWinBlocksPerSM)
             const uint32_t k = s * kWinThreads + tid;
             if (k < live) {
                 live_mask |= 1u << s;
-                rE[s] = S.e[k];
                 rT[s] = S.t[k];
             }
         }
@@ -480,8 +493,11 @@ __global__ void __launch_bounds__(kWinThreads, kWinBlocksPerSM)
     int b = 0;
     int slots = (int)((live + kWinThreads - 1) / kWinThreads);
     uint32_t next_compact = 8;  // then 16, 32, ..., every kCompactEvery channels
-    for (uint32_t c0 = i0; c0 < i1; c0 += kWinChunk) {
-        const uint32_t c1 = min(i1, c0 + (uint32_t)kWinChunk);
+    // Walk channels [i0, iw): every candidate ends at the state of the last
+    // channel iw, whose extra draw is added when the counts are recovered.
+    const uint32_t iw = i1 - 1;
+    for (uint32_t c0 = i0; c0 < iw; c0 += kWinChunk) {
+        const uint32_t c1 = min(iw, c0 + (uint32_t)kWinChunk);
         asm volatile("cp.async.wait_group 1;\n" ::);
         __syncthreads();
         const uint32_t c2 = c0 + 2 * kWinChunk;
@@ -495,34 +511,54 @@ __global__ void __launch_bounds__(kWinThreads, kWinBlocksPerSM)
             const uint32_t stop =
                 min(len, r + (next_compact > done0 ? next_compact - done0 : len));
             const bool end_next = (c0 + stop) < i1;
-            const uint32_t merge_len = (done0 < 256u) ? 8u : 32u;
+            // one slot: merging cannot lower the slot count, so only the
+            // span ends merge (duplicates step in lanes that run anyway)
+            const uint32_t merge_len = slots <= 1 ? kSegLen : ((done0 < 256u) ? 8u : 32u);
             if (__any_sync(0xFFFFFFFFu, live_mask != 0)) {
                 switch (slots) {
 #define FX_WALK_CASE(K)                                                                         \
     case K:                                                                                     \
-        walk_span<K>(r4, r, stop, end_next, merge_len, rE, rT, live_mask, steps);               \
+        walk_span<K>(r4, r, stop, end_next, merge_len, rT, live_mask, steps);                   \
         break;
                     FX_WALK_CASE(1) FX_WALK_CASE(2) FX_WALK_CASE(3) FX_WALK_CASE(4)
                     FX_WALK_CASE(5) FX_WALK_CASE(6) FX_WALK_CASE(7) FX_WALK_CASE(8)
                     FX_WALK_CASE(9) FX_WALK_CASE(10) FX_WALK_CASE(11) FX_WALK_CASE(12)
                     FX_WALK_CASE(13) FX_WALK_CASE(14) FX_WALK_CASE(15)
                 default:
-                    walk_span<16>(r4, r, stop, end_next, merge_len, rE, rT, live_mask, steps);
+                    walk_span<16>(r4, r, stop, end_next, merge_len, rT, live_mask, steps);
                     break;
 #undef FX_WALK_CASE
                 }
             }
             r = stop;
             const uint32_t done = (c0 - i0) + r;
-            if (done >= next_compact || c0 + r == i1) {
+            if (done >= next_compact || c0 + r == iw) {
                 merge_and_compact(slots);
                 slots = (int)((live + kWinThreads - 1) / kWinThreads);
-                next_compact = min(2 * next_compact, done + kCompactEvery);
+                next_compact = slots <= 1 ? (iw - i0) : min(2 * next_compact, done + kCompactEvery);
             }
         }
         b = (b + 1) % kWinRing;
     }
     asm volatile("cp.async.wait_group 0;\n" ::);
+    __syncthreads();
+    if (iw == i0) merge_and_compact(slots);  // one-channel segment: nothing walked
+
+    // Exit counts: a survivor's state at channel iw is G^(pos_iw + 1 + E)(t0),
+    // so E - wlo is its LCG distance from the state of count wlo (exact: the
+    // difference is below count + kSegLen, far under the 2^24 period); the
+    // last channel adds its extra draw.  Channel iw's entry is still staged
+    // (chunk q of the ring, whose buffer no later staging reused).
+    {
+        const uint32_t q = (iw - i0) / kWinChunk;
+        const uint4 lw_last = reinterpret_cast<const uint4 *>(S.ring[q % kWinRing])
+            [2 * ((iw - i0) % kWinChunk)];
+        const uint32_t t_ref = jump_t(t0, (uint64_t)pos[iw] + 1u + wlo);
+        for (uint32_t k = tid; k < live; k += kWinThreads) {
+            const uint32_t t = S.t[k];
+            S.e[k] = wlo + lcg_distance_t(t_ref, t) + (copies(lw_last, t) ? 0u : 1u);
+        }
+    }
 
     // Outputs.  Survivors sit compacted in S.* in E_in order.
     uint32_t *out = table + (size_t)blockIdx.x * kWinMax;
