@@ -52,6 +52,9 @@ SERVE_RATES = (2.0, 8.0, 32.0)
 STENCIL_PROFILE = os.path.join(ROOT, "profiles", "k_stencil_native_frame.md")
 
 
+WALK_BLOCKS_PER_SM = 3   # window-walk segments per SM in one wave (kWinBlocksPerSM)
+
+
 def launches_per_frame(h: int, w: int, per_wave: int) -> int:
     """Kernel launches of one plain pass (the library's launch sequence):
     producer 4, planes 2, stencil 1, startup 1, chain 4, walk 1 + 2 per wave
@@ -427,7 +430,7 @@ def run_b200(args, world, rank, local, frames=None):
             "cpu_baseline": cpu,
             "e2e": e2e,
             "clocks": clocks,
-            "gpu_launches": launches_per_frame(h, w, 2 * torch.cuda.get_device_properties(
+            "gpu_launches": launches_per_frame(h, w, WALK_BLOCKS_PER_SM * torch.cuda.get_device_properties(
                 local).multi_processor_count) * args.steps,
             "rng_dependent_channels": int(counters.rng_dependent),
             "walk_fallback_segments": int(counters.walk_fallbacks),
@@ -554,7 +557,7 @@ def run_batched(ctx, frames, args, golden):
         "ms_per_step": round(1000 * med, 2), "steps": args.batch_steps,
         "plain_same_mix": {"value": round(mp / plain_med, 1), "unit": "MP/s",
                            "ms_per_step": round(1000 * plain_med, 2), "slots": 1},
-        "slots": slots, "walk_wave": wave or "default (2 per SM)",
+        "slots": slots, "walk_wave": wave or f"default ({WALK_BLOCKS_PER_SM} per SM)",
         "tuning_ms": {f"slots={k[0]},wave={k[1] or 'default'}": round(1000 * v, 1)
                       for k, v in tuning.items()},
         "timing": "host clock around the whole batch, synchronize on both sides (frames run on "

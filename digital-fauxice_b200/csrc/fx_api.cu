@@ -56,7 +56,7 @@ struct Arena {
     int64_t amb_capacity = 0;
 };
 
-static int g_per_wave = 296;  // window blocks per wave: walk_per_wave(SM count)
+static int g_per_wave = 444;  // window blocks per wave: walk_per_wave(SM count)
 
 static size_t arena_layout(const Geometry &g, int64_t amb_cap, Arena *a) {
     size_t off = 0;
@@ -148,7 +148,7 @@ struct fx_context {
     int device = 0;
     bool profile = false;
     bool parallel_walk = true;
-    int walk_wave = 0;  // window segments per wave; 0: g_per_wave (two per SM)
+    int walk_wave = 0;  // window segments per wave; 0: g_per_wave (three per SM)
     std::vector<std::vector<cudaEvent_t>> pending;  // recorded, not yet read
     std::vector<std::vector<cudaEvent_t>> spare;
     double profile_ms[fx::kProfileStages] = {0};
@@ -769,6 +769,26 @@ FX_API int fx_set_walk_wave(fx_context *ctx, int32_t segments) {
     if (!ctx || segments < 0) return FX_ERR_INVALID_ARGUMENT;
     std::lock_guard<std::mutex> lock(ctx->mu);
     ctx->walk_wave = segments;
+    return FX_OK;
+}
+
+FX_API int fx_reserve_frames(fx_context *ctx, int32_t max_height, int32_t max_width) {
+    if (!ctx || max_height < 1 || max_width < 1) return FX_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    cudaSetDevice(ctx->device);
+    if ((int64_t)max_height * max_width > (int64_t)1 << 30)
+        return fail(ctx, FX_ERR_INVALID_ARGUMENT, "frame too large");
+    // every buffer of the layout grows with the height and the width, so the
+    // arena of the largest frame holds any frame within both bounds
+    const Geometry g = make_geometry(max_height, max_width);
+    for (Slot &s : ctx->slots) {
+        if (s.busy) return fail(ctx, FX_ERR_INVALID_ARGUMENT, "a slot is busy: reserve first");
+        const int64_t cap = s.arena.base && s.arena.amb_capacity > default_amb_capacity(g)
+                                ? s.arena.amb_capacity
+                                : default_amb_capacity(g);
+        const int rc = ensure_arena(ctx, s, g, cap);
+        if (rc) return rc;
+    }
     return FX_OK;
 }
 

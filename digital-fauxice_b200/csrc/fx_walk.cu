@@ -26,7 +26,7 @@
 namespace fx {
 
 constexpr int kWinThreads = 256;
-constexpr int kWinBlocksPerSM = 2;                  // two segments resident per SM
+constexpr int kWinBlocksPerSM = 3;                  // three segments resident per SM
 constexpr int kWinSlots = 16;                       // candidates per thread
 constexpr int kWinMax = kWinThreads * kWinSlots;    // 4096 candidates
 constexpr uint32_t kSegLen = 4096;                  // channels per walk segment

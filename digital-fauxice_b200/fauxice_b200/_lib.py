@@ -142,6 +142,7 @@ SIGNATURES = {
     "fx_set_parallel_walk": ([_P, ctypes.c_int], ctypes.c_int),
     "fx_set_walk_wave": ([_P, ctypes.c_int32], ctypes.c_int),
     "fx_set_output_digest": ([_P, ctypes.c_int], ctypes.c_int),
+    "fx_reserve_frames": ([_P, ctypes.c_int32, ctypes.c_int32], ctypes.c_int),
     "fx_output_digest": ([_P, _P], ctypes.c_int),
     "fx_submit": ([_P, ctypes.POINTER(FxFrame), ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
     "fx_submit_device": ([_P, _P, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(FxParams), _P,

@@ -70,8 +70,16 @@ def set_slots(ctx: _lib.Context, slots: int) -> None:
         _check(ctx, _lib.load().fx_set_slots(ctx.handle, int(slots)))
 
 
+def reserve_frames(ctx: _lib.Context, max_height: int, max_width: int) -> None:
+    """Size every slot for frames up to max_height x max_width now, so that no
+    frame of the run reallocates device memory while others are in flight."""
+
+    with ctx.lock:
+        _check(ctx, _lib.load().fx_reserve_frames(ctx.handle, int(max_height), int(max_width)))
+
+
 def set_walk_wave(ctx: _lib.Context, segments: int) -> None:
-    """Segments per speculative walk wave (0: the default, two per SM)."""
+    """Segments per speculative walk wave (0: the default, three per SM)."""
 
     with ctx.lock:
         _check(ctx, _lib.load().fx_set_walk_wave(ctx.handle, int(segments)))
@@ -87,6 +95,8 @@ def run_device_batch(ctx: _lib.Context, frames: Sequence[DeviceFrame], *, slots:
 
     lib = _lib.load()
     set_slots(ctx, slots)
+    if frames:
+        reserve_frames(ctx, max(f.height for f in frames), max(f.width for f in frames))
     if params is None:
         params = DEFAULT_PROFILE.hot_path_parameters().to_c()
     pending: deque[tuple[int, int]] = deque()  # (frame index, ticket)
@@ -162,6 +172,9 @@ def process_batch(jobs: Sequence, *, slots: int = 4, export_diagnostics: bool = 
         DEFAULT_PROFILE.check_prepass_record(payload)
     lib = _lib.load()
     set_slots(ctx, slots)
+    if jobs:
+        shapes = [job.acquisition.main.pixels.shape for job in jobs]
+        reserve_frames(ctx, max(int(sh[0]) for sh in shapes), max(int(sh[1]) for sh in shapes))
     params = DEFAULT_PROFILE.hot_path_parameters().to_c()
     floor = DEFAULT_PROFILE.score_floor()
 

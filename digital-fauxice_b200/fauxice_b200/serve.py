@@ -88,6 +88,9 @@ def serve(ctx: _lib.Context, requests: Sequence[Request], *, slots: int = 4,
 
     lib = _lib.load()
     batch.set_slots(ctx, slots)
+    if requests:  # size the slots once: no reallocation while frames are in flight
+        batch.reserve_frames(ctx, max(int(r.pixels.shape[0]) for r in requests),
+                             max(int(r.pixels.shape[1]) for r in requests))
     params = DEFAULT_PROFILE.hot_path_parameters().to_c()
     copy_stream = torch.cuda.Stream()
     report = ServeReport()

@@ -193,7 +193,7 @@ FX_API int fx_set_slots(fx_context *ctx, int32_t slots);
  * chain (leaves the rest of the GPU to other frames' kernels). */
 FX_API int fx_set_parallel_walk(fx_context *ctx, int enable);
 /* Segments of 4096 RNG-dependent channels walked speculatively per wave
- * (0, the default: two per SM).  Fewer segments per wave mean narrower
+ * (0, the default: three per SM).  Fewer segments per wave mean narrower
  * candidate windows (less total work, for throughput when several frames
  * are in flight) and more waves (longer latency for one frame). */
 FX_API int fx_set_walk_wave(fx_context *ctx, int32_t segments);
@@ -205,6 +205,13 @@ FX_API int fx_set_walk_wave(fx_context *ctx, int32_t segments);
  * fx_output_digest returns the digest of the last successful fx_process. */
 FX_API int fx_set_output_digest(fx_context *ctx, int enable);
 FX_API int fx_output_digest(fx_context *ctx, uint8_t *digest32);
+/* Size every slot's device buffers for frames up to max_height x max_width
+ * now, so that later frames within both bounds never reallocate (a
+ * reallocation frees device memory, which waits for the whole device and
+ * stalls the frames in flight).  No reference counterpart; call it after
+ * fx_set_slots and before submitting.  FX_ERR_OUT_OF_MEMORY when the device
+ * cannot hold them. */
+FX_API int fx_reserve_frames(fx_context *ctx, int32_t max_height, int32_t max_width);
 FX_API int fx_submit(fx_context *ctx, const fx_frame *frame, int64_t *ticket);
 /* fx_submit for a frame already in device memory: the pass is enqueued on
  * a free slot's stream and writes d_rgb_out / d_score_out / d_changed_out

@@ -17,7 +17,7 @@ import cases
 from _helpers import b200_mismatches, make_job, sha
 from fauxice_b200 import _lib, batch, engine
 from fauxice_b200.engine import process_b200
-from fauxice_b200.profile import DEFAULT_PROFILE
+from fauxice_b200.profile import DEFAULT_PROFILE, NIKON_PE_INITIAL_STATE
 
 pytestmark = pytest.mark.gpu
 
@@ -90,3 +90,24 @@ def test_batch_refuses_invalid_jobs_before_any_work():
     bad = make_job(main[:4], prepass)
     with pytest.raises(ValueError, match="at least 5 rows by 8 columns"):
         batch.process_batch([good, bad])
+
+
+def test_reserved_slots_do_not_grow():
+    """After fx_reserve_frames, frames within the bounds allocate no device
+    memory (the free device memory stays the same)."""
+
+    ctx = engine.context()
+    lib = _lib.load()
+    batch.set_slots(ctx, 2)
+    batch.reserve_frames(ctx, 300, 280)
+    free0, total = ctypes.c_size_t(), ctypes.c_size_t()
+    assert lib.fx_mem_info(ctx.handle, ctypes.byref(free0), ctypes.byref(total)) == 0
+    params = DEFAULT_PROFILE.hot_path_parameters().to_c()
+    for k, (h, w) in enumerate(((300, 280), (120, 97), (299, 13), (41, 280))):
+        px = cases.generated(500 + k, h, w, "native")[0]
+        engine.run_frame(ctx, px, params, None, NIKON_PE_INITIAL_STATE, False)
+    free1 = ctypes.c_size_t()
+    assert lib.fx_mem_info(ctx.handle, ctypes.byref(free1), ctypes.byref(total)) == 0
+    assert free1.value == free0.value
+    with pytest.raises(Exception):
+        batch.reserve_frames(ctx, 0, 10)
