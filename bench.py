@@ -79,6 +79,46 @@ def stencil_traffic():
     return None
 
 
+def issue_roofline(stencil_ms: float, device: int):
+    """The stencil's second bound: it is instruction-bound (binary64 chains in
+    the reference's operation order), so its warp instructions per launch
+    over its CUDA-event time are compared with the SMs' peak issue rate (four
+    warp instructions per SM per cycle at the maximum SM clock)."""
+
+    import torch
+
+    inst = stencil_warp_instructions()
+    if inst is None or stencil_ms <= 0:
+        return None
+    sms = torch.cuda.get_device_properties(device).multi_processor_count
+    try:
+        mhz = float(subprocess.run(
+            ["nvidia-smi", "-i", str(device), "--query-gpu=clocks.max.sm",
+             "--format=csv,noheader,nounits"], capture_output=True, text=True,
+            timeout=10).stdout.strip().splitlines()[0])
+    except (OSError, ValueError, IndexError, subprocess.SubprocessError):
+        mhz = 1965.0
+    achieved = inst / (stencil_ms / 1000.0) / 1e9
+    peak = 4.0 * sms * mhz / 1000.0
+    return {"bound": "issue", "warp_instructions_per_launch": inst,
+            "achieved": round(achieved, 1), "peak": round(peak, 1), "unit": "G warp-inst/s",
+            "frac": round(achieved / peak, 4),
+            "source": "instructions from profiles/k_stencil_native_frame.md (ncu), "
+                      "time from this run's CUDA events, peak = 4 x SMs x max SM clock"}
+
+
+def stencil_warp_instructions():
+    """Warp instructions per k_stencil launch from the committed ncu summary."""
+
+    try:
+        for line in open(STENCIL_PROFILE):
+            if line.startswith("| warp instructions |"):
+                return float(line.split("|")[2].split()[0]) * 1e9  # "1.298 G (...)"
+    except (OSError, ValueError, IndexError):
+        pass
+    return None
+
+
 def generate_batch(count: int):
     """Frames of the batched workload, generated in spawn workers (before
     any CUDA call in this process)."""
@@ -373,6 +413,7 @@ def run_b200(args, world, rank, local, frames=None):
         "traffic": stencil_traffic(),
         "algorithmic_bytes_per_launch": bytes_per_launch,
         "stage_ms": {k: round(v, 4) for k, v in stages.items()},
+        "issue": issue_roofline(stages["stencil"], local),
         "walk": {"bytes_per_channel": WALK_BYTES_PER_CHANNEL,
                  "achieved_gbs": round(WALK_BYTES_PER_CHANNEL * counters.rng_dependent
                                        / (stages["walk"] / 1000.0) / 1e9, 2),
