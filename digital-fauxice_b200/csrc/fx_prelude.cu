@@ -167,9 +167,10 @@ __device__ void finish_terms(const float vq[4], const float iq[4], uint32_t raw_
 // ---------------------------------------------------------------------------
 
 constexpr int kRowTile = 64;          // columns per tile (8 cells)
-constexpr int kRowWarps = 8;
+constexpr int kRowWarps = 16;
 constexpr int kRowPitch = kRowTile + 1;
-constexpr int kProductWarps = 6;      // warps 1..6
+constexpr int kProductWarps = 14;     // warps 1..14
+constexpr int kStageRows = kRowWarps * 32 / kRowTile;  // rows one staging pass covers
 
 struct RowSmem {
     uint2 raw[2][32][kRowTile];     // staged RGBI samples
@@ -198,14 +199,14 @@ __global__ void __launch_bounds__(kRowWarps * 32, 1)
     // staging: thread tid copies column tid % 64 of rows tid / 64 + 4 m
     const int sj = tid % kRowTile, sk0 = tid / kRowTile;
     const uint16_t *srow = rgbi + ((int64_t)(r0 + sk0) * w + sj) * 4;
-    const int64_t srow_step = (int64_t)4 * w * 4;  // four rows of samples
+    const int64_t srow_step = (int64_t)kStageRows * w * 4;  // kStageRows rows of samples
     auto stage = [&](int t) {
         if (t < tiles) {
             const int col = t * kRowTile + sj;
             const uint16_t *src = srow + (int64_t)t * kRowTile * 4;
 #pragma unroll
-            for (int m = 0; m < 32 / (kRowWarps * 32 / kRowTile); ++m) {
-                const int k = sk0 + 4 * m;
+            for (int m = 0; m < 32 / kStageRows; ++m) {
+                const int k = sk0 + kStageRows * m;
                 if (r0 + k < h && col < active_width) cp_async8(&S.raw[t & 1][k][sj], src);
                 src += srow_step;
             }
@@ -281,12 +282,9 @@ __global__ void __launch_bounds__(kRowWarps * 32, 1)
             }
         }
         if (t < tiles && warp >= 1) {
-            // quadrant trees: trees 0..191 on warps 1..6, 192..255 on warp 7
-            const int z0 = tid - 32;
-            const int nz = warp == kRowWarps - 1 ? 2 : 1;
-#pragma unroll 1
-            for (int r = 0; r < nz; ++r) {
-                const int z = warp == kRowWarps - 1 ? 192 + lane + 32 * r : z0;
+            // quadrant trees: one per thread of warps 1..8 (32 cells x 8)
+            const int z = tid - 32;
+            if (warp <= 8) {
                 const int cl = z >> 3, rb = cl >> 3, cc = cl & 7;
                 const int blk = (r0 >> 3) + rb, cell = t * 8 + cc;
                 if (blk < ne && cell < cells && S.fp[rb][cc] == 64)
