@@ -394,7 +394,11 @@ struct StencilSmem {
     };
     unsigned long long rowlow[RR];  // bit c: auxt[r][c] below the decision threshold
     uint32_t collow[RC];            // bit r: the same, by column
+    uint32_t rowbal[kTileH];        // bit x: pixel (row, x) of the tile is attempted
 };
+// three blocks per SM: 228 KB less 1 KB reserved per block
+static_assert(sizeof(StencilSmem) <= 76800, "the stencil tile keeps three blocks per SM");
+static_assert(kTileW == 32, "one warp per pixel row of the stencil tile");
 static_assert(sizeof(float) * RR * RC >= 4 * (kStencilThreads / 32 + 1) + 2 * kStencilThreads,
               "the attempted list fits in the aux tile");
 
@@ -451,6 +455,42 @@ __global__ void __launch_bounds__(kStencilThreads)
         for (int r = 0; r < RR; ++r) m |= (uint32_t)(S.auxt[r][c] < thr) << r;
         S.collow[c] = m;
     }
+    __syncthreads();
+
+    // ---- per output pixel: the decision -------------------------------------
+    // It needs only the aux masks, the point score and the stage gates, so it
+    // comes first: a tile without an attempted pixel stops here, and the
+    // others build only the records their attempted pixels read.
+    const int dty = tid / kTileW, dtx = tid % kTileW;
+    bool eligible = false;
+    {
+        const int y = y0 + dty, x = x0 + dtx;
+        if (y < h && x < w) {
+            const fx_stage ws = stages[y + 6];  // writer stage y+7
+            const bool floor_enabled = p.driver_gate_primary || ws.gate_secondary;
+            // decision bars (streaming.py:157-198), edge-replicated via the
+            // tile: rows ty..ty+8 of a column, columns tx..tx+8 of a row
+            const int rad = p.radius;
+            const int vl = __popc((S.collow[dtx + 4 - rad] >> dty) & 0x1FFu);
+            const int vr = __popc((S.collow[dtx + 4 + rad] >> dty) & 0x1FFu);
+            const int ha = __popcll((S.rowlow[dty + 4 - rad] >> dtx) & 0x1FFull);
+            const int hb = __popcll((S.rowlow[dty + 4 + rad] >> dtx) & 0x1FFull);
+            const int lim = p.count_limit;
+            eligible = !(vl > lim || ha > lim || vr > lim || hb > lim);
+            const float point_score = S.hs[dty + 5][dtx + 5];
+            if (ws.row_gate != 0) eligible = false;
+            else if (floor_enabled && !(point_score < 1.0f)) eligible = false;
+            // driver_forces_fallback (reconstruction.py:890-904)
+            if (eligible && (ws.row_gate != 0 || (floor_enabled && point_score >= 1.0f)))
+                eligible = false;
+            if (!eligible) meta_out[6 * (int64_t)w + (int64_t)y * w + x] = 0;
+        }
+        // a warp is one pixel row of the tile (kTileW == 32)
+        const uint32_t bal = __ballot_sync(0xFFFFFFFFu, eligible);
+        if (dtx == 0) S.rowbal[dty] = bal;
+    }
+    if (!__syncthreads_or(eligible)) return;  // no attempted pixel in the tile
+
     // One work item is a vertical run of column sums in one column: the
     // samples are loaded and widened once and shared by the run's chains.
     // Items 0..167: score / waux planes, runs of 5 record rows; items
@@ -495,6 +535,17 @@ __global__ void __launch_bounds__(kStencilThreads)
     // ---- feature records (streaming.py:236-308) ---------------------------
     for (int i = tid; i < CR * RECC; i += kStencilThreads) {
         const int r = i / RECC, c = i % RECC;
+        {   // read by an attempted pixel: record row r is the centre row of
+            // pixel row r-1 and the cross neighbour of pixel rows r and r-2
+            unsigned long long need = 0;
+            if (r >= 1 && r <= kTileH) {
+                const unsigned long long b = S.rowbal[r - 1];
+                need |= b | (b << 1) | (b << 2);
+            }
+            if (r < kTileH) need |= (unsigned long long)S.rowbal[r] << 1;
+            if (r >= 2) need |= (unsigned long long)S.rowbal[r - 2] << 1;
+            if (!((need >> c) & 1ull)) continue;
+        }
         const int xx = x0 - 1 + c;
         Record rec;
         if (xx < 0 || xx >= w) {
@@ -549,34 +600,11 @@ __global__ void __launch_bounds__(kStencilThreads)
     }
     __syncthreads();
 
-    // ---- per output pixel: the decision -------------------------------------
-    // Each pixel decides whether it is attempted; the attempted ones are then
-    // listed in shared memory and processed densely (about half the pixels
-    // are attempted, mixed within every warp).
+    // ---- the attempted pixels, listed ----------------------------------------
+    // About half the pixels are attempted, mixed within every warp: they are
+    // listed in shared memory (over the aux tile, dead once the records are
+    // built) and processed densely.
     {
-        const int ty = tid / kTileW, tx = tid % kTileW;
-        const int y = y0 + ty, x = x0 + tx;
-        bool eligible = false;
-        if (y < h && x < w) {
-            const fx_stage ws = stages[y + 6];  // writer stage y+7
-            const bool floor_enabled = p.driver_gate_primary || ws.gate_secondary;
-            // decision bars (streaming.py:157-198), edge-replicated via the
-            // tile: rows ty..ty+8 of a column, columns tx..tx+8 of a row
-            const int rad = p.radius;
-            const int vl = __popc((S.collow[tx + 4 - rad] >> ty) & 0x1FFu);
-            const int vr = __popc((S.collow[tx + 4 + rad] >> ty) & 0x1FFu);
-            const int ha = __popcll((S.rowlow[ty + 4 - rad] >> tx) & 0x1FFull);
-            const int hb = __popcll((S.rowlow[ty + 4 + rad] >> tx) & 0x1FFull);
-            const int lim = p.count_limit;
-            eligible = !(vl > lim || ha > lim || vr > lim || hb > lim);
-            const float point_score = S.cw[ty][tx][3];
-            if (ws.row_gate != 0) eligible = false;
-            else if (floor_enabled && !(point_score < 1.0f)) eligible = false;
-            // driver_forces_fallback (reconstruction.py:890-904)
-            if (eligible && (ws.row_gate != 0 || (floor_enabled && point_score >= 1.0f)))
-                eligible = false;
-            if (!eligible) meta_out[6 * (int64_t)w + (int64_t)y * w + x] = 0;
-        }
         const uint32_t bal = __ballot_sync(0xFFFFFFFFu, eligible);
         if ((tid & 31) == 0) S.dec.wcount[tid >> 5] = __popc(bal);
         __syncthreads();
