@@ -155,6 +155,8 @@ struct fx_context {
     int64_t profile_passes = 0;
     float *lut = nullptr;
     uint32_t *high = nullptr, *low = nullptr;
+    uint16_t *ident = nullptr;  // emit(lut[v]) for every raw value v
+    uint32_t *ident_bad = nullptr;
     bool tables = false;
     std::vector<fx::Slot> slots;
     int64_t next_ticket = 1;
@@ -275,7 +277,7 @@ static int enqueue_pass(fx_context *ctx, Slot &s, const Geometry &g, const fx_pa
                                                                          : g_per_wave;
     WriterBuffers wb{a.seg_base, a.seg_amb, a.entries, a.pos, a.extra, a.counters,
                      a.amb_capacity, a.walk, wave, ctx->parallel_walk};
-    FX_CUDA(ctx, launch_writer(g, a.meta, a.cand, d_in, ctx->lut, ctx->high, ctx->low, a.stages,
+    FX_CUDA(ctx, launch_writer(g, a.meta, a.cand, d_in, ctx->lut, ctx->high, ctx->low, ctx->ident, a.stages,
                                p, rng, wb, d_out, d_changed, a.err, st, marks));
     return FX_OK;
 }
@@ -429,7 +431,9 @@ FX_API int fx_context_create(int device, fx_context **out) {
     if (analysis_init() != cudaSuccess || ensure_slots(ctx, 1) != FX_OK ||
         cudaMalloc(&ctx->lut, 65536 * 4) != cudaSuccess ||
         cudaMalloc(&ctx->high, 256 * 4) != cudaSuccess ||
-        cudaMalloc(&ctx->low, 256 * 4) != cudaSuccess) {
+        cudaMalloc(&ctx->low, 256 * 4) != cudaSuccess ||
+        cudaMalloc(&ctx->ident, 65536 * 2) != cudaSuccess ||
+        cudaMalloc(&ctx->ident_bad, 4) != cudaSuccess) {
         cudaGetLastError();
         fx_context_destroy(ctx);
         return fail(nullptr, FX_ERR_CUDA, "context initialisation failed");
@@ -459,6 +463,8 @@ FX_API void fx_context_destroy(fx_context *ctx) {
     if (ctx->lut) cudaFree(ctx->lut);
     if (ctx->high) cudaFree(ctx->high);
     if (ctx->low) cudaFree(ctx->low);
+    if (ctx->ident) cudaFree(ctx->ident);
+    if (ctx->ident_bad) cudaFree(ctx->ident_bad);
     delete ctx;
 }
 
@@ -476,6 +482,13 @@ FX_API int fx_set_tables(fx_context *ctx, const float *lut, const uint32_t *high
     FX_CUDA(ctx, cudaMemcpy(ctx->lut, lut, 65536 * 4, cudaMemcpyHostToDevice));
     FX_CUDA(ctx, cudaMemcpy(ctx->high, high, 256 * 4, cudaMemcpyHostToDevice));
     FX_CUDA(ctx, cudaMemcpy(ctx->low, low, 256 * 4, cudaMemcpyHostToDevice));
+    FX_CUDA(ctx, writer_identity_table(ctx->lut, ctx->high, ctx->low, ctx->ident, ctx->ident_bad, 0));
+    uint32_t bad = 0;
+    FX_CUDA(ctx, cudaMemcpy(&bad, ctx->ident_bad, 4, cudaMemcpyDeviceToHost));
+    if (bad) {
+        ctx->tables = false;
+        return fail(ctx, FX_ERR_NONFINITE_WORK, "work RGB must be finite: the LUT holds a non-finite value");
+    }
     ctx->tables = true;
     return FX_OK;
 }

@@ -180,9 +180,12 @@ cudaError_t launch_analysis(const uint16_t *rgbi, const Geometry &g, const float
                             const fx_stage *stages, const fx_params &p, float *aux, float *hs,
                             float *hwa, float *hwr, int64_t plane, double *cand, uint8_t *meta,
                             uint32_t *err, cudaStream_t stream, const Marks &marks);
+cudaError_t writer_identity_table(const float *lut, const uint32_t *hi, const uint32_t *lo,
+                                  uint16_t *ident, uint32_t *bad, cudaStream_t stream);
 cudaError_t launch_writer(const Geometry &g, const uint8_t *meta, const double *cand,
                           const uint16_t *rgbi, const float *lut, const uint32_t *high,
-                          const uint32_t *low, const fx_stage *stages, const fx_params &p,
+                          const uint32_t *low, const uint16_t *ident, const fx_stage *stages,
+                          const fx_params &p,
                           uint32_t s0, const WriterBuffers &b, uint16_t *rgb_out,
                           uint8_t *changed_out, uint32_t *err, cudaStream_t stream,
                           const Marks &marks);

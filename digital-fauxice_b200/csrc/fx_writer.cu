@@ -448,6 +448,29 @@ __device__ __forceinline__ bool emit_one(float v, const uint32_t *hi, const uint
     return true;
 }
 
+// Identity emits: ident[v] = emit(lut[v]), the output of a channel whose
+// value is its original (every unattempted pixel, and the comparison emit of
+// an attempted one).  *bad is set when a LUT value is not finite.
+__global__ void k_identity(const float *__restrict__ lut, const uint32_t *__restrict__ hi,
+                           const uint32_t *__restrict__ lo, uint16_t *__restrict__ ident,
+                           uint32_t *bad) {
+    const int v = blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= 65536) return;
+    uint16_t e = 0;
+    if (!emit_one(lut[v], hi, lo, e)) {
+        atomicOr(bad, 1u);
+        e = 0;
+    }
+    ident[v] = e;
+}
+
+cudaError_t writer_identity_table(const float *lut, const uint32_t *hi, const uint32_t *lo,
+                                  uint16_t *ident, uint32_t *bad, cudaStream_t stream) {
+    cudaMemsetAsync(bad, 0, sizeof(uint32_t), stream);
+    k_identity<<<256, 256, 0, stream>>>(lut, hi, lo, ident, bad);
+    return cudaGetLastError();
+}
+
 // Affine jump tables: g_jump[j][d] = g^(d * 64^j) in T space, so any jump
 // below 2^36 draws is six table lookups and compositions.
 constexpr int kJumpDigits = 6;
@@ -484,14 +507,14 @@ __global__ void __launch_bounds__(kSegThreads)
     k_apply(const uint8_t *__restrict__ meta, const double *__restrict__ cand, int64_t sites,
             int w, const uint16_t *__restrict__ rgbi, const float *__restrict__ lut,
             const uint32_t *__restrict__ g_high, const uint32_t *__restrict__ g_low,
-            const fx_stage *__restrict__ stages, fx_params p,
+            const uint16_t *__restrict__ ident, const fx_stage *__restrict__ stages, fx_params p,
             const uint32_t *__restrict__ seg_base, const uint32_t *__restrict__ seg_amb,
             const uint32_t *__restrict__ extra_after, uint32_t s0, uint16_t *__restrict__ rgb_out,
             uint8_t *__restrict__ changed_out, DevCounters *ctr, uint32_t *err,
             int64_t capacity) {
     __shared__ uint32_t ws[kSegThreads / 32];
     __shared__ uint32_t hi[256], lo[256];
-    __shared__ unsigned long long scratch[8];
+    __shared__ unsigned long long s_sums[kSegThreads / 32][4];
     __shared__ Affine s_jump[kJumpDigits][64];
     __shared__ uint32_t s_ref[kSegment], s_p[kSegment], s_a[kSegment];
     for (int i = threadIdx.x; i < 256; i += kSegThreads) {
@@ -526,14 +549,10 @@ __global__ void __launch_bounds__(kSegThreads)
             } else {
                 const int64_t pixel = site - su;
                 const uint2 raw = reinterpret_cast<const uint2 *>(rgbi)[pixel];
-                uint16_t e0[3];
-                ok &= emit_one(__ldg(lut + (raw.x & 0xFFFFu)), hi, lo, e0[0]);
-                ok &= emit_one(__ldg(lut + (raw.x >> 16)), hi, lo, e0[1]);
-                ok &= emit_one(__ldg(lut + (raw.y & 0xFFFFu)), hi, lo, e0[2]);
                 uint16_t *o = rgb_out + 3 * pixel;
-                o[0] = e0[0];
-                o[1] = e0[1];
-                o[2] = e0[2];
+                o[0] = __ldg(ident + (raw.x & 0xFFFFu));
+                o[1] = __ldg(ident + (raw.x >> 16));
+                o[2] = __ldg(ident + (raw.y & 0xFFFFu));
                 if (changed_out) changed_out[pixel] = 0;
             }
         }
@@ -604,10 +623,11 @@ __global__ void __launch_bounds__(kSegThreads)
         att += 1;
         draws_total += draws;
         written += (values[0] != orig[0] || values[1] != orig[1] || values[2] != orig[2]);
-        uint16_t e[3], e0[3];
+        const uint16_t e0[3] = {__ldg(ident + (raw.x & 0xFFFFu)), __ldg(ident + (raw.x >> 16)),
+                                __ldg(ident + (raw.y & 0xFFFFu))};
+        uint16_t e[3];
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            ok &= emit_one(orig[c], hi, lo, e0[c]);
             e[c] = e0[c];
             if (!(values[c] == orig[c])) ok &= emit_one(values[c], hi, lo, e[c]);
         }
@@ -620,15 +640,25 @@ __global__ void __launch_bounds__(kSegThreads)
         if (changed_out) changed_out[pixel] = ch ? 1 : 0;
     }
     if (!ok) raise_error(err, FX_ERR_NONFINITE_WORK);
-    att = block_sum<kSegThreads, unsigned long long>(att, scratch);
-    written = block_sum<kSegThreads, unsigned long long>(written, scratch);
-    changed = block_sum<kSegThreads, unsigned long long>(changed, scratch);
-    draws_total = block_sum<kSegThreads, unsigned long long>(draws_total, scratch);
+    // the four counters in one reduction: warps, then thread 0
+    unsigned long long v4[4] = {att, written, changed, draws_total};
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v4[q] += __shfl_down_sync(0xFFFFFFFFu, v4[q], o);
+    if ((threadIdx.x & 31) == 0)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) s_sums[threadIdx.x >> 5][q] = v4[q];
+    __syncthreads();
     if (threadIdx.x == 0) {
-        if (att) atomicAdd(&ctr->attempted, att);
-        if (written) atomicAdd(&ctr->written, written);
-        if (changed) atomicAdd(&ctr->changed, changed);
-        if (draws_total) atomicAdd(&ctr->public_advances, draws_total);
+        unsigned long long t4[4] = {0, 0, 0, 0};
+        for (int wq = 0; wq < kSegThreads / 32; ++wq)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) t4[q] += s_sums[wq][q];
+        if (t4[0]) atomicAdd(&ctr->attempted, t4[0]);
+        if (t4[1]) atomicAdd(&ctr->written, t4[1]);
+        if (t4[2]) atomicAdd(&ctr->changed, t4[2]);
+        if (t4[3]) atomicAdd(&ctr->public_advances, t4[3]);
     }
 }
 
@@ -652,7 +682,8 @@ __global__ void k_final(const uint32_t *__restrict__ seg_base, const uint32_t *_
 
 cudaError_t launch_writer(const Geometry &g, const uint8_t *meta, const double *cand,
                           const uint16_t *rgbi, const float *lut, const uint32_t *high,
-                          const uint32_t *low, const fx_stage *stages, const fx_params &p,
+                          const uint32_t *low, const uint16_t *ident, const fx_stage *stages,
+                          const fx_params &p,
                           uint32_t s0, const WriterBuffers &b, uint16_t *rgb_out,
                           uint8_t *changed_out, uint32_t *err, cudaStream_t stream,
                           const Marks &marks) {
@@ -676,7 +707,7 @@ cudaError_t launch_writer(const Geometry &g, const uint8_t *meta, const double *
     k_startup_counts<<<1, 256, 0, stream>>>(meta, g.w, b.extra_after, s0 & kLcgMask, ctr,
                                             b.capacity);
     k_apply<<<(unsigned)segs, kSegThreads, 0, stream>>>(
-        meta, cand, g.sites, g.w, rgbi, lut, high, low, stages, p, b.seg_base, b.seg_amb,
+        meta, cand, g.sites, g.w, rgbi, lut, high, low, ident, stages, p, b.seg_base, b.seg_amb,
         b.extra_after, s0 & kLcgMask, rgb_out, changed_out, ctr, err, b.capacity);
     k_final<<<1, 1, 0, stream>>>(b.seg_base, b.seg_amb, segs, b.extra_after, s0 & kLcgMask,
                                  ctr, err, b.capacity);
