@@ -731,13 +731,18 @@ __global__ void __launch_bounds__(kResolveThreads)
 // ---------------------------------------------------------------------------
 
 constexpr int kRewalkWarps = 4;
-constexpr int kRewalkChunk = 128;  // 13.8 KB of staging per warp: every segment resident at once
+constexpr int kRewalkLanes = 4;    // segments per warp: lane l < 4 walks one
+constexpr int kRewalkChunk = 128;  // channels per staged chunk and segment
 constexpr int kRewalkRing = 3;
 constexpr int kGroup = 8;
 
+// A warp walks kRewalkLanes segments at once, one per lane, so resident
+// warps no longer each issue a full instruction stream for a single chain
+// (with one walking lane, lane 0 measured 61 cycles per channel against 30
+// for the bare step).  216 KB: one block of 16 segments per SM.
 struct RewalkSmem {
-    AmbEntry ring[kRewalkWarps][kRewalkRing][kRewalkChunk];
-    uint32_t out[kRewalkWarps][kRewalkRing][kRewalkChunk];
+    AmbEntry ring[kRewalkWarps][kRewalkLanes][kRewalkRing][kRewalkChunk];
+    uint32_t out[kRewalkWarps][kRewalkLanes][kRewalkRing][kRewalkChunk];
 };
 
 __device__ __forceinline__ void step(const uint4 &lw, const uint4 &ac, uint32_t &T, uint32_t &extra,
@@ -761,42 +766,59 @@ __global__ void __launch_bounds__(kRewalkWarps * 32)
     // a short chain (or the serial mode) is one segment walked from E = 0
     const bool serial = n < serial_below;
     const uint32_t seg_len = serial ? (n > 0 ? n : 1u) : parallel_seg_len;
-    const uint32_t j = blockIdx.x * kRewalkWarps + warp;
-    const uint64_t i0_64 = (uint64_t)j * seg_len;
-    if (i0_64 >= n) return;
-    const uint32_t i0 = (uint32_t)i0_64;
-    const uint32_t i1 = (uint32_t)min((uint64_t)n, i0_64 + seg_len);
-    const uint32_t chunks = (i1 - i0 + kRewalkChunk - 1) / kRewalkChunk;
-    AmbEntry(*ring)[kRewalkChunk] = S.ring[warp];
-    uint32_t(*out)[kRewalkChunk] = S.out[warp];
+    const uint32_t jbase = (blockIdx.x * kRewalkWarps + warp) * kRewalkLanes;
+    if ((uint64_t)jbase * seg_len >= n) return;  // the whole warp is past the chain
+    // bounds of the warp's segments (every lane computes all of them)
+    uint32_t s_i0[kRewalkLanes], s_i1[kRewalkLanes];
+#pragma unroll
+    for (int q = 0; q < kRewalkLanes; ++q) {
+        const uint64_t a = (uint64_t)(jbase + q) * seg_len;
+        s_i0[q] = a < n ? (uint32_t)a : n;
+        s_i1[q] = a < n ? (uint32_t)min((uint64_t)n, a + seg_len) : n;
+    }
+    const uint32_t chunks = (s_i1[0] - s_i0[0] + kRewalkChunk - 1) / kRewalkChunk;  // longest
     auto issue = [&](uint32_t k) {
         if (k < chunks) {
-            const uint32_t first = i0 + k * kRewalkChunk;
-            const uint32_t count = min((uint32_t)kRewalkChunk, i1 - first);
-            const uint4 *src = reinterpret_cast<const uint4 *>(entries + first);
-            uint4 *dst = reinterpret_cast<uint4 *>(ring[k % kRewalkRing]);
-            for (uint32_t v = lane; v < 2 * count; v += 32) {
-                const uint32_t s = (uint32_t)__cvta_generic_to_shared(dst + v);
-                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(src + v));
+#pragma unroll
+            for (int q = 0; q < kRewalkLanes; ++q) {
+                const uint32_t first = s_i0[q] + k * kRewalkChunk;
+                if (first >= s_i1[q]) continue;  // warp-uniform
+                const uint32_t count = min((uint32_t)kRewalkChunk, s_i1[q] - first);
+                const uint4 *src = reinterpret_cast<const uint4 *>(entries + first);
+                uint4 *dst = reinterpret_cast<uint4 *>(S.ring[warp][q][k % kRewalkRing]);
+                for (uint32_t v = lane; v < 2 * count; v += 32) {
+                    const uint32_t sa = (uint32_t)__cvta_generic_to_shared(dst + v);
+                    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa),
+                                 "l"(src + v));
+                }
             }
         }
         asm volatile("cp.async.commit_group;\n" ::);
     };
 #pragma unroll
     for (int k = 0; k < kRewalkRing - 1; ++k) issue(k);
-    const uint32_t e_in = serial ? 0u : e_in_exact[j];
-    uint32_t T = jump_t(t0, (uint64_t)pos[i0] + 1u + e_in);  // state at channel i0's first draw
-    uint32_t E = e_in;
-    uint32_t extra = 0u;
+    // this lane's own segment (lanes 0..kRewalkLanes-1)
+    const uint64_t my_a = (uint64_t)(jbase + (lane < kRewalkLanes ? lane : 0)) * seg_len;
+    const bool walker = lane < kRewalkLanes && my_a < n;
+    const int me = walker ? lane : 0;
+    const uint32_t i0 = walker ? (uint32_t)my_a : 0u;
+    const uint32_t i1 = walker ? (uint32_t)min((uint64_t)n, my_a + seg_len) : 0u;
+    uint32_t T = 0, E = 0, extra = 0u;
+    if (walker) {
+        const uint32_t e_in = serial ? 0u : e_in_exact[jbase + me];
+        T = jump_t(t0, (uint64_t)pos[i0] + 1u + e_in);  // state at channel i0's first draw
+        E = e_in;
+    }
     for (uint32_t k = 0; k < chunks; ++k) {
         issue(k + kRewalkRing - 1);
         asm volatile("cp.async.wait_group %0;\n" ::"n"(kRewalkRing - 1));
         __syncwarp();
         const uint32_t first = i0 + k * kRewalkChunk;
-        const uint32_t count = min((uint32_t)kRewalkChunk, i1 - first);
-        if (lane == 0) {
-            const uint4 *__restrict__ e4 = reinterpret_cast<const uint4 *>(ring[k % kRewalkRing]);
-            uint32_t *__restrict__ o = out[k % kRewalkRing];
+        if (walker && first < i1) {
+            const uint32_t count = min((uint32_t)kRewalkChunk, i1 - first);
+            const uint4 *__restrict__ e4 =
+                reinterpret_cast<const uint4 *>(S.ring[warp][me][k % kRewalkRing]);
+            uint32_t *__restrict__ o = S.out[warp][me][k % kRewalkRing];
             uint32_t i = 0;
             if (k == 0) {
                 // the first channel needs no transition: its state is the jump
@@ -806,34 +828,18 @@ __global__ void __launch_bounds__(kRewalkWarps * 32)
                 i = 1;
             }
             const uint32_t groups = (count - i) / kGroup;
-            uint4 lw[kGroup], ac[kGroup];
-            if (groups) {
-#pragma unroll
-                for (int q = 0; q < kGroup; ++q) {
-                    lw[q] = e4[2 * (i + q)];
-                    ac[q] = e4[2 * (i + q) + 1];
-                }
-            }
             for (uint32_t g = 0; g < groups; ++g) {
                 const uint32_t base = i + g * kGroup;
-                const uint32_t next = (g + 1 < groups) ? base + kGroup : base;
-                uint4 nlw[kGroup], nac[kGroup];
+                uint4 lw[kGroup], ac[kGroup];
 #pragma unroll
                 for (int q = 0; q < kGroup; ++q) {
-                    nlw[q] = e4[2 * (next + q)];
-                    nac[q] = e4[2 * (next + q) + 1];
+                    lw[q] = e4[2 * (base + q)];
+                    ac[q] = e4[2 * (base + q) + 1];
                 }
-                uint32_t res[kGroup];
 #pragma unroll
                 for (int q = 0; q < kGroup; ++q) {
                     step(lw[q], ac[q], T, extra, E);
-                    res[q] = E;
-                }
-#pragma unroll
-                for (int q = 0; q < kGroup; ++q) {
-                    o[base + q] = res[q];
-                    lw[q] = nlw[q];
-                    ac[q] = nac[q];
+                    o[base + q] = E;
                 }
             }
             for (uint32_t r = i + groups * kGroup; r < count; ++r) {
@@ -842,8 +848,14 @@ __global__ void __launch_bounds__(kRewalkWarps * 32)
             }
         }
         __syncwarp();
-        const uint32_t *o = out[k % kRewalkRing];
-        for (uint32_t r = lane; r < count; r += 32) extra_after[first + r] = o[r];
+#pragma unroll
+        for (int q = 0; q < kRewalkLanes; ++q) {
+            const uint32_t f = s_i0[q] + k * kRewalkChunk;
+            if (f >= s_i1[q]) continue;  // warp-uniform
+            const uint32_t count = min((uint32_t)kRewalkChunk, s_i1[q] - f);
+            const uint32_t *o = S.out[warp][q][k % kRewalkRing];
+            for (uint32_t r = lane; r < count; r += 32) extra_after[f + r] = o[r];
+        }
         __syncwarp();
     }
     asm volatile("cp.async.wait_group 0;\n" ::);
@@ -924,7 +936,8 @@ cudaError_t launch_walk(const AmbEntry *entries, const uint32_t *pos, const uint
                 serial_below);
         }
     }
-    k_rewalk<<<(segs + kRewalkWarps - 1) / kRewalkWarps, kRewalkWarps * 32, sizeof(RewalkSmem),
+    constexpr uint32_t kRewalkPerBlock = kRewalkWarps * kRewalkLanes;
+    k_rewalk<<<(segs + kRewalkPerBlock - 1) / kRewalkPerBlock, kRewalkWarps * 32, sizeof(RewalkSmem),
                stream>>>(entries, pos, n_ptr, capacity, kSegLen, e_in, t0, extra_after,
                          serial_below);
     if (fallbacks_out)
