@@ -1,10 +1,10 @@
 // fx_analysis.cu -- per-pixel scoring and the 9x9 reconstruction stencil.
 //
 // Kernels (all exact binary64/binary32 in the reference's order):
-//   k_auxiliary   x3a.py:193-221 derive_auxiliary with the stage y+1 alpha
-//   k_planes      x3a.py:245-286 continuous_score + streaming.py:139-147
+//   k_planes      x3a.py:193-221 derive_auxiliary with the stage y+1 alpha,
+//                 x3a.py:245-286 continuous_score + streaming.py:139-147
 //                 weighted planes, written into zero/pseudo-row/repeat padded
-//                 history planes (streaming.py:201-233)
+//                 history planes (streaming.py:201-233), and the aux plane
 //   k_stencil     streaming.py:454-521: decision gate, five feature records,
 //                 RGB candidates, combiner, then the writer classification
 //   k_startup     startup.py:186-353 hidden centres -6..-1 (RNG-free part)
@@ -16,19 +16,15 @@ namespace fx {
 // Planes
 // ---------------------------------------------------------------------------
 
-__global__ void k_auxiliary(const uint16_t *__restrict__ rgbi, int h, int w,
-                            const float *__restrict__ lut, const fx_stage *__restrict__ stages,
-                            int visible, float *__restrict__ aux, uint32_t *err) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x;
-    const int y = blockIdx.y;
-    if (x >= w || y >= h) return;
-    const fx_stage st = stages[y];  // stage y+1 (stage_parameters.py:207-212)
+// The auxiliary value of one pixel (x3a.py:193-221): stage y+1's alpha and
+// offset, visible lane and IR lane through the LUT, binary64 then float.
+__device__ __forceinline__ float aux_value(const uint2 raw, const fx_stage &st, int visible,
+                                           const float *__restrict__ lut, uint32_t *err) {
     float a;
     if (st.alpha == 1.0f) {
         if (!st.replacement_valid) raise_error(err, FX_ERR_ALPHA_ONE_UNBOUND);
         a = st.replacement;
     } else {
-        const uint2 raw = reinterpret_cast<const uint2 *>(rgbi)[(int64_t)y * w + x];
         const uint32_t lanes[4] = {raw.x & 0xFFFFu, raw.x >> 16, raw.y & 0xFFFFu, raw.y >> 16};
         const double vis = (double)__ldg(lut + lanes[visible]);
         const double ir = (double)__ldg(lut + lanes[3]);
@@ -37,26 +33,52 @@ __global__ void k_auxiliary(const uint16_t *__restrict__ rgbi, int h, int w,
         a = (float)((ir - alpha * vis) / (1.0 - alpha) - offset);
     }
     if (!isfinite(a)) raise_error(err, FX_ERR_NONFINITE_AUX);
-    aux[(int64_t)y * w + x] = a;
+    return a;
 }
 
-__global__ void k_planes(const uint16_t *__restrict__ rgbi, Geometry g,
-                         const float *__restrict__ lut, const fx_stage *__restrict__ stages,
-                         fx_params p, const float *__restrict__ aux, float *__restrict__ hs,
-                         float *__restrict__ hwa, float *__restrict__ hwr, int64_t plane) {
+// One padded row segment of the history planes (streaming.py:111-147,
+// 201-233), with the auxiliary plane computed on the way: each thread
+// computes the aux of its own column (the edge threads also their outer
+// neighbour's, for the horizontal minimum) and writes it once for the real
+// pixels.  Rows above the image take the pseudo row, rows below repeat the
+// last row, columns outside are zero.
+__global__ void __launch_bounds__(256)
+    k_planes(const uint16_t *__restrict__ rgbi, Geometry g, const float *__restrict__ lut,
+             const fx_stage *__restrict__ stages, fx_params p, float *__restrict__ aux,
+             float *__restrict__ hs, float *__restrict__ hwa, float *__restrict__ hwr,
+             int64_t plane, uint32_t *err) {
+    __shared__ float s_aux[256 + 2];  // aux of columns x-1 .. x+256 of the segment
     const int px = blockIdx.x * blockDim.x + threadIdx.x;
     const int py = blockIdx.y;
-    if (px >= g.pitch) return;
     const int y = py - kPad, x = px - kPad;
+    const bool live = y >= -1;  // rows above the pseudo row are zero
+    const int r = y < 0 ? 0 : (y < g.h ? y : g.h - 1);
+    const int64_t row0 = (int64_t)r * g.w;
+    const fx_stage ast = stages[r];  // stage y+1 (stage_parameters.py:207-212)
+    const bool own = live && px < g.pitch && x >= 0 && x < g.w;
+    uint2 raw = make_uint2(0u, 0u);
+    float a = 0.0f;
+    if (own) {
+        raw = reinterpret_cast<const uint2 *>(rgbi)[row0 + x];
+        a = aux_value(raw, ast, p.visible_channel, lut, err);
+        if (y >= 0 && y < g.h) aux[row0 + x] = a;
+    }
+    s_aux[threadIdx.x + 1] = a;
+    if (threadIdx.x == 0 || threadIdx.x == blockDim.x - 1) {
+        const int xe = threadIdx.x == 0 ? x - 1 : x + 1;
+        float ae = 0.0f;
+        if (live && xe >= 0 && xe < g.w)
+            ae = aux_value(reinterpret_cast<const uint2 *>(rgbi)[row0 + xe], ast,
+                           p.visible_channel, lut, err);
+        s_aux[threadIdx.x == 0 ? 0 : blockDim.x + 1] = ae;
+    }
+    __syncthreads();
+    if (px >= g.pitch) return;
     const float floor = p.score_floor;
     float s = 0.0f, wa = 0.0f, wr[3] = {0.0f, 0.0f, 0.0f};
-    if (x >= 0 && x < g.w && y >= -1) {
-        const int r = y < 0 ? 0 : (y < g.h ? y : g.h - 1);
-        const int64_t i = (int64_t)r * g.w + x;
-        const uint2 raw = reinterpret_cast<const uint2 *>(rgbi)[i];
+    if (own) {
         const float rgb[3] = {__ldg(lut + (raw.x & 0xFFFFu)), __ldg(lut + (raw.x >> 16)),
                               __ldg(lut + (raw.y & 0xFFFFu))};
-        const float a = aux[i];
         if (y == -1) {
             // the pseudo row above the image (streaming.py:218-228)
             s = floor;
@@ -65,7 +87,7 @@ __global__ void k_planes(const uint16_t *__restrict__ rgbi, Geometry g,
         } else {
             float sample = a;
             if (p.horizontal_minimum && g.w > 2 && x > 0 && x < g.w - 1) {
-                const float l = aux[i - 1], rr = aux[i + 1];
+                const float l = s_aux[threadIdx.x], rr = s_aux[threadIdx.x + 2];
                 const float m = (l < a) ? l : a;
                 sample = (m < rr) ? m : rr;
             }
@@ -839,13 +861,9 @@ cudaError_t launch_analysis(const uint16_t *rgbi, const Geometry &g, const float
                             uint32_t *err, cudaStream_t stream, const Marks &marks) {
     const CombineConst cc = combine_const(p);
     {
-        dim3 block(256), grid((g.w + 255) / 256, g.h);
-        k_auxiliary<<<grid, block, 0, stream>>>(rgbi, g.h, g.w, lut, stages, p.visible_channel,
-                                                aux, err);
-    }
-    {
         dim3 block(256), grid((g.pitch + 255) / 256, g.prow);
-        k_planes<<<grid, block, 0, stream>>>(rgbi, g, lut, stages, p, aux, hs, hwa, hwr, plane);
+        k_planes<<<grid, block, 0, stream>>>(rgbi, g, lut, stages, p, aux, hs, hwa, hwr, plane,
+                                             err);
     }
     marks.mark(2, stream);
     {
