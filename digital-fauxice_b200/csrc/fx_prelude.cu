@@ -171,14 +171,22 @@ constexpr int kRowWarps = 16;
 constexpr int kRowPitch = kRowTile + 1;
 constexpr int kProductWarps = 14;     // warps 1..14
 constexpr int kStageRows = kRowWarps * 32 / kRowTile;  // rows one staging pass covers
+// Rows per block: five 8-row epochs, so a native frame (5782 rows) is 145
+// blocks, one wave on 148 SMs.  Warp 0 sums rows 0..31 on its lanes and rows
+// 32..39 on lanes 0..7 as a second, interleaved set of chains.
+constexpr int kRows = 40;
+constexpr int kRowBlocks = kRows / 8;
+constexpr int kTileCells = kRowBlocks * 8;  // epoch cells of one tile
+static_assert(kRows % 8 == 0 && kRows % kStageRows == 0 && kRows > 32 && kRows <= 64,
+              "warp 0 sums kRows rows in two lane sets");
 
 struct RowSmem {
-    uint2 raw[2][32][kRowTile];     // staged RGBI samples
-    double p[2][3][32][kRowPitch];  // [buffer][visible, infrared, weight][row][column]
-    int fp[4][8];                   // first failing position per (8-row block, cell)
-    float qv[2][32][8];             // quadrant trees per tile cell (rb * 8 + cc)
-    uint32_t rsum[2][32];           // raw IR total per tile cell
-    int flag[2][32];                // 0: no complete epoch cell, 1: failing, 2: passing
+    uint2 raw[2][kRows][kRowTile];     // staged RGBI samples
+    double p[2][3][kRows][kRowPitch];  // [buffer][visible, infrared, weight][row][column]
+    int fp[kRowBlocks][8];             // first failing position per (8-row block, cell)
+    float qv[2][kTileCells][8];        // quadrant trees per tile cell (rb * 8 + cc)
+    uint32_t rsum[2][kTileCells];      // raw IR total per tile cell
+    int flag[2][kTileCells];           // 0: no complete epoch cell, 1: failing, 2: passing
 };
 
 __device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
@@ -192,7 +200,7 @@ __global__ void __launch_bounds__(kRowWarps * 32, 1)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     RowSmem &S = *reinterpret_cast<RowSmem *>(smem_raw);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int r0 = blockIdx.x * 32;
+    const int r0 = blockIdx.x * kRows;
     const int tiles = (active_width + kRowTile - 1) / kRowTile;
     const int ne = h / 8;  // complete 8-row blocks
     const double thr = (double)kIrThreshold;
@@ -205,7 +213,7 @@ __global__ void __launch_bounds__(kRowWarps * 32, 1)
             const int col = t * kRowTile + sj;
             const uint16_t *src = srow + (int64_t)t * kRowTile * 4;
 #pragma unroll
-            for (int m = 0; m < 32 / kStageRows; ++m) {
+            for (int m = 0; m < kRows / kStageRows; ++m) {
                 const int k = sk0 + kStageRows * m;
                 if (r0 + k < h && col < active_width) cp_async8(&S.raw[t & 1][k][sj], src);
                 src += srow_step;
@@ -214,7 +222,9 @@ __global__ void __launch_bounds__(kRowWarps * 32, 1)
         asm volatile("cp.async.commit_group;\n" ::);
     };
     stage(0);
-    double rv = 0.0, ri = 0.0, rw = 0.0;
+    double rv = 0.0, ri = 0.0, rw = 0.0;     // row r0 + lane
+    double rv2 = 0.0, ri2 = 0.0, rw2 = 0.0;  // row r0 + 32 + lane (lanes < kRows - 32)
+    const int lane2 = lane < kRows - 32 ? lane + 32 : lane;  // other lanes re-read their row
     for (int t = 0; t <= tiles; ++t) {
         asm volatile("cp.async.wait_group 0;\n" ::);
         __syncthreads();  // tile t staged; tile t-1's products complete
@@ -223,7 +233,7 @@ __global__ void __launch_bounds__(kRowWarps * 32, 1)
         const int bt = t & 1;
         if (t < tiles && warp >= 1) {
             // first failing IR position of each cell (row-major inside the cell)
-            for (int ci = warp - 1; ci < 32; ci += kRowWarps - 1) {
+            for (int ci = warp - 1; ci < kTileCells; ci += kRowWarps - 1) {
                 const int rb = ci >> 3, cc = ci & 7;
                 const int cell = t * 8 + cc;
                 if (cell >= cells) continue;  // warp-uniform
@@ -246,7 +256,7 @@ __global__ void __launch_bounds__(kRowWarps * 32, 1)
             // fixed trip count, fully unrolled: every LUT gather of the
             // thread's pixels is in flight before the first product
             constexpr int kStride = kProductWarps * 32;
-            constexpr int kPerThread = (32 * kRowTile + kStride - 1) / kStride;
+            constexpr int kPerThread = (kRows * kRowTile + kStride - 1) / kStride;
             const int q0 = tid - 32;
             float lv[kPerThread], li[kPerThread];
             uint32_t wir[kPerThread];
@@ -256,7 +266,7 @@ __global__ void __launch_bounds__(kRowWarps * 32, 1)
                 const int q = q0 + m * kStride;
                 const int k = q / kRowTile, j = q % kRowTile;
                 const int row = r0 + k, col = col0 + j;
-                use[m] = q < 32 * kRowTile && row < h && col < active_width &&
+                use[m] = q < kRows * kRowTile && row < h && col < active_width &&
                          (row & 7) * 8 + (col & 7) < S.fp[k >> 3][j >> 3];
                 const uint2 px = use[m] ? S.raw[bt][k][j] : make_uint2(0u, 0u);
                 wir[m] = px.y >> 16;
@@ -266,7 +276,7 @@ __global__ void __launch_bounds__(kRowWarps * 32, 1)
 #pragma unroll
             for (int m = 0; m < kPerThread; ++m) {
                 const int q = q0 + m * kStride;
-                if (q < 32 * kRowTile) {
+                if (q < kRows * kRowTile) {
                     const int k = q / kRowTile, j = q % kRowTile;
                     double pv = 0.0, pi = 0.0, pw = 0.0;
                     if (use[m]) {
@@ -282,9 +292,9 @@ __global__ void __launch_bounds__(kRowWarps * 32, 1)
             }
         }
         if (t < tiles && warp >= 1) {
-            // quadrant trees: one per thread of warps 1..8 (32 cells x 8)
+            // quadrant trees: one per thread of warps 1..kTileCells/4 (cells x 8)
             const int z = tid - 32;
-            if (warp <= 8) {
+            if (z < kTileCells * 8) {
                 const int cl = z >> 3, rb = cl >> 3, cc = cl & 7;
                 const int blk = (r0 >> 3) + rb, cell = t * 8 + cc;
                 if (blk < ne && cell < cells && S.fp[rb][cc] == 64)
@@ -293,53 +303,68 @@ __global__ void __launch_bounds__(kRowWarps * 32, 1)
                         z & 7);
             }
             if (warp == kRowWarps - 1) {  // lane = tile cell: status and raw total
-                const int rb = lane >> 3, cc = lane & 7;
-                const int blk = (r0 >> 3) + rb, cell = t * 8 + cc;
-                int flag = 0;
-                if (blk < ne && cell < cells) flag = S.fp[rb][cc] == 64 ? 2 : 1;
-                uint32_t total = 0;
-                if (flag == 2) {
+                for (int cl = lane; cl < kTileCells; cl += 32) {
+                    const int rb = cl >> 3, cc = cl & 7;
+                    const int blk = (r0 >> 3) + rb, cell = t * 8 + cc;
+                    int flag = 0;
+                    if (blk < ne && cell < cells) flag = S.fp[rb][cc] == 64 ? 2 : 1;
+                    uint32_t total = 0;
+                    if (flag == 2) {
 #pragma unroll 8
-                    for (int i = 0; i < 64; ++i) total += S.raw[bt][rb * 8 + (i >> 3)][cc * 8 + (i & 7)].y >> 16;
+                        for (int i = 0; i < 64; ++i)
+                            total += S.raw[bt][rb * 8 + (i >> 3)][cc * 8 + (i & 7)].y >> 16;
+                    }
+                    S.flag[bt][cl] = flag;
+                    S.rsum[bt][cl] = total;
                 }
-                S.flag[bt][lane] = flag;
-                S.rsum[bt][lane] = total;
             }
         }
         if (warp == 0 && t > 0) {
             // finish the previous tile's epoch cells (lane = tile cell)
             const int u = t - 1, ub = u & 1;
-            const int flag = S.flag[ub][lane];
-            if (flag) {
-                const int rb = lane >> 3, cc = lane & 7;
-                const int64_t e_idx = (int64_t)((r0 >> 3) + rb) * cells + (u * 8 + cc);
-                b.cell_ok[e_idx] = flag == 2 ? 1 : 0;
-                if (flag == 2) {
-                    const float *qv = S.qv[ub][lane];
-                    const float vq[4] = {qv[0], qv[1], qv[2], qv[3]};
-                    const float iq[4] = {qv[4], qv[5], qv[6], qv[7]};
-                    double2 terms[4];
-                    finish_terms(vq, iq, S.rsum[ub][lane], terms);
+            for (int cl = lane; cl < kTileCells; cl += 32) {
+                const int flag = S.flag[ub][cl];
+                if (flag) {
+                    const int rb = cl >> 3, cc = cl & 7;
+                    const int64_t e_idx = (int64_t)((r0 >> 3) + rb) * cells + (u * 8 + cc);
+                    b.cell_ok[e_idx] = flag == 2 ? 1 : 0;
+                    if (flag == 2) {
+                        const float *qv = S.qv[ub][cl];
+                        const float vq[4] = {qv[0], qv[1], qv[2], qv[3]};
+                        const float iq[4] = {qv[4], qv[5], qv[6], qv[7]};
+                        double2 terms[4];
+                        finish_terms(vq, iq, S.rsum[ub][cl], terms);
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) b.terms[e_idx * 4 + q] = terms[q];
+                        for (int q = 0; q < 4; ++q) b.terms[e_idx * 4 + q] = terms[q];
+                    }
                 }
             }
+            // the ordered row sums, two rows per lane interleaved
             const int n = min(kRowTile, active_width - u * kRowTile);
             const double *pv = S.p[u & 1][0][lane];
             const double *pi = S.p[u & 1][1][lane];
             const double *pw = S.p[u & 1][2][lane];
+            const double *pv2 = S.p[u & 1][0][lane2];
+            const double *pi2 = S.p[u & 1][1][lane2];
+            const double *pw2 = S.p[u & 1][2][lane2];
             if (n == kRowTile) {
 #pragma unroll 16
                 for (int j = 0; j < kRowTile; ++j) {
                     rv += pv[j];
                     ri += pi[j];
                     rw += pw[j];
+                    rv2 += pv2[j];
+                    ri2 += pi2[j];
+                    rw2 += pw2[j];
                 }
             } else {
                 for (int j = 0; j < n; ++j) {
                     rv += pv[j];
                     ri += pi[j];
                     rw += pw[j];
+                    rv2 += pv2[j];
+                    ri2 += pi2[j];
+                    rw2 += pw2[j];
                 }
             }
         }
@@ -350,6 +375,12 @@ __global__ void __launch_bounds__(kRowWarps * 32, 1)
         b.row_sums[row] = rv;
         b.row_sums[h + row] = ri;
         b.row_sums[2 * h + row] = rw;
+    }
+    const int row2 = r0 + 32 + lane;
+    if (warp == 0 && lane < kRows - 32 && row2 < h) {
+        b.row_sums[row2] = rv2;
+        b.row_sums[h + row2] = ri2;
+        b.row_sums[2 * h + row2] = rw2;
     }
 }
 
@@ -543,7 +574,7 @@ cudaError_t launch_producer(const uint16_t *rgbi, int h, int w, const float *lut
     b.cum = (double *)take(3 * (size_t)h * sizeof(double));
     b.add = (float *)take(2 * (size_t)ne * sizeof(float));
     b.p_epoch = (float *)take(2 * (size_t)ne * sizeof(float));
-    k_producer_rows<<<(h + 31) / 32, kRowWarps * 32, sizeof(RowSmem), stream>>>(rgbi, h, w, aw,
+    k_producer_rows<<<(h + kRows - 1) / kRows, kRowWarps * 32, sizeof(RowSmem), stream>>>(rgbi, h, w, aw,
                                                                                cells, lut, b);
     if (ne > 0) k_producer_epochs<<<ne, 32, 0, stream>>>(cells, ne, b);
     k_producer_scan<<<1, kScanThreads, sizeof(ScanSmem), stream>>>(h, ne, b);
