@@ -427,8 +427,11 @@ constexpr int kScanChunk = 1024;
 constexpr int kScanThreads = 256;
 constexpr int kScanLoaders = kScanThreads - 32;
 
+constexpr int kEpochChunk = 1024;
+
 struct ScanSmem {
     double v[2][3][kScanChunk];
+    float add[2][kEpochChunk];  // the epoch chain's inputs, staged by warp 1
 };
 
 __device__ __forceinline__ void scan_barrier() {
@@ -440,21 +443,34 @@ __global__ void __launch_bounds__(kScanThreads) k_producer_scan(int h, int ne, P
     ScanSmem &S = *reinterpret_cast<ScanSmem *>(smem_raw);
     const int tid = threadIdx.x;
     if (tid >= 32 && tid < 64) {
-        if (tid == 32) {
-            float den = 0.0f, num = 0.0f, p1 = kInitialScale, p2 = kInitialScale;
-            for (int e = 0; e < ne; ++e) {
-                const double dw = (double)den + (double)b.add[e];
-                const double nw = (double)num + (double)b.add[ne + e];
-                den = (float)dw;
-                num = (float)nw;
-                if (dw != 0.0) {
-                    const double ratio = nw / dw;
-                    p2 = (float)ratio;
-                    p1 = (float)((double)kScaleMultiplier * ratio);
-                }
-                b.p_epoch[e] = p1;
-                b.p_epoch[ne + e] = p2;
+        // the epoch chain: warp 1 stages each chunk of its inputs into shared
+        // memory (coalesced), lane 0 walks it (shared loads do not wait for
+        // the chain's global stores)
+        const int lane = tid - 32;
+        float den = 0.0f, num = 0.0f, p1 = kInitialScale, p2 = kInitialScale;
+        for (int e0 = 0; e0 < ne; e0 += kEpochChunk) {
+            const int n = min(kEpochChunk, ne - e0);
+            for (int k = lane; k < n; k += 32) {
+                S.add[0][k] = b.add[e0 + k];
+                S.add[1][k] = b.add[ne + e0 + k];
             }
+            __syncwarp();
+            if (lane == 0) {
+                for (int k = 0; k < n; ++k) {
+                    const double dw = (double)den + (double)S.add[0][k];
+                    const double nw = (double)num + (double)S.add[1][k];
+                    den = (float)dw;
+                    num = (float)nw;
+                    if (dw != 0.0) {
+                        const double ratio = nw / dw;
+                        p2 = (float)ratio;
+                        p1 = (float)((double)kScaleMultiplier * ratio);
+                    }
+                    b.p_epoch[e0 + k] = p1;
+                    b.p_epoch[ne + e0 + k] = p2;
+                }
+            }
+            __syncwarp();
         }
         return;
     }
