@@ -37,6 +37,8 @@ struct DevCounters {
     uint32_t n_amb;
     uint32_t walk_fallbacks;
     unsigned long long walk_stats[3];  // candidate steps, window sum, survivor sum
+    uint32_t su_base[6], su_amb[6];    // per startup row, for the last block's prefix
+    uint32_t su_done;                  // startup rows summed
 };
 
 // ---------------------------------------------------------------------------
@@ -401,39 +403,52 @@ __global__ void k_coef(AmbEntry *__restrict__ entries, const uint32_t *__restric
 // Startup counters, apply + emit, final state
 // ---------------------------------------------------------------------------
 
+// Startup counters: one block per startup row sums its attempted sites,
+// fixed draws and RNG-dependent channels; the last block to finish chains
+// the six rows (the extra draws of a row come from the walk's running count
+// at the row's ends).
 __global__ void k_startup_counts(const uint8_t *__restrict__ meta, int w,
                                  const uint32_t *__restrict__ extra_after, uint32_t s0,
                                  DevCounters *ctr, int64_t capacity) {
     __shared__ unsigned long long scratch[8];
-    uint32_t a_run = 0, p_run = 0;
-    for (int k = 0; k < 6; ++k) {
-        unsigned long long att = 0, base = 0, amb = 0;
-        for (int x = threadIdx.x; x < w; x += blockDim.x) {
-            const uint8_t m = meta[(int64_t)k * w + x];
-            att += (m >> 7) & 1u;
-            base += meta_base(m);
-            amb += meta_amb(m);
-        }
-        att = block_sum<256, unsigned long long>(att, scratch);
-        base = block_sum<256, unsigned long long>(base, scratch);
-        amb = block_sum<256, unsigned long long>(amb, scratch);
-        const uint32_t e_start = extra_before(extra_after, a_run, capacity);
-        const uint32_t a_end = a_run + (uint32_t)amb;
-        const uint32_t e_end = extra_before(extra_after, a_end, capacity);
-        if (threadIdx.x == 0) {
-            ctr->su_attempted[k] = att;
-            ctr->su_advances[k] = base + (e_end - e_start);
-        }
-        a_run = a_end;
-        p_run += (uint32_t)base;
+    __shared__ bool last;
+    const int k = blockIdx.x;  // startup row 0..5
+    unsigned long long att = 0, base = 0, amb = 0;
+    for (int x = threadIdx.x; x < w; x += blockDim.x) {
+        const uint8_t m = meta[(int64_t)k * w + x];
+        att += (m >> 7) & 1u;
+        base += meta_base(m);
+        amb += meta_amb(m);
     }
+    att = block_sum<256, unsigned long long>(att, scratch);
+    base = block_sum<256, unsigned long long>(base, scratch);
+    amb = block_sum<256, unsigned long long>(amb, scratch);
     if (threadIdx.x == 0) {
-        const uint32_t e = extra_before(extra_after, a_run, capacity);
-        ctr->startup_base = p_run;
-        ctr->startup_amb = a_run;
-        ctr->startup_extra = e;
-        ctr->su_final_state = lcg_jump(s0, (uint64_t)p_run + e);
+        ctr->su_attempted[k] = att;
+        ctr->su_base[k] = (uint32_t)base;
+        ctr->su_amb[k] = (uint32_t)amb;
+        __threadfence();
+        last = atomicAdd(&ctr->su_done, 1u) == 5u;
     }
+    __syncthreads();
+    if (!last || threadIdx.x != 0) return;
+    __threadfence();
+    const volatile DevCounters *vc = ctr;
+    uint32_t a_run = 0, p_run = 0;
+    for (int r = 0; r < 6; ++r) {
+        const uint32_t rb = vc->su_base[r], ra = vc->su_amb[r];
+        const uint32_t e_start = extra_before(extra_after, a_run, capacity);
+        const uint32_t a_end = a_run + ra;
+        const uint32_t e_end = extra_before(extra_after, a_end, capacity);
+        ctr->su_advances[r] = (unsigned long long)rb + (e_end - e_start);
+        a_run = a_end;
+        p_run += rb;
+    }
+    const uint32_t e = extra_before(extra_after, a_run, capacity);
+    ctr->startup_base = p_run;
+    ctr->startup_amb = a_run;
+    ctr->startup_extra = e;
+    ctr->su_final_state = lcg_jump(s0, (uint64_t)p_run + e);
 }
 
 __device__ __forceinline__ bool emit_one(float v, const uint32_t *hi, const uint32_t *lo,
@@ -704,7 +719,7 @@ cudaError_t launch_writer(const Geometry &g, const uint8_t *meta, const double *
                                 ctr->walk_stats, stream);
     if (e != cudaSuccess) return e;
     marks.mark(6, stream);
-    k_startup_counts<<<1, 256, 0, stream>>>(meta, g.w, b.extra_after, s0 & kLcgMask, ctr,
+    k_startup_counts<<<6, 256, 0, stream>>>(meta, g.w, b.extra_after, s0 & kLcgMask, ctr,
                                             b.capacity);
     k_apply<<<(unsigned)segs, kSegThreads, 0, stream>>>(
         meta, cand, g.sites, g.w, rgbi, lut, high, low, ident, stages, p, b.seg_base, b.seg_amb,
