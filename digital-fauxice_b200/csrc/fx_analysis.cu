@@ -400,10 +400,9 @@ struct StencilSmem {
     float hs[PR][PC];
     float hwa[PR][PC];
     float hwr[3][RR][RC];
-    double cs[2][5][CR][CC];      // [score|waux][S3,S5,S7,S9,B16], float-rounded
+    float cs[2][5][CR][CC];       // [score|waux][S3,S5,S7,S9,B16]
     float rcs[3][4][kTileH][RC];  // [channel][S3,S5,S7,S9]
     Record rec[CR][RECC];
-    float cw[kTileH][kTileW][4];
     union {
         // aux at clamped (y0-4+r, x0-4+c): decision masks and point aux,
         // dead once the records are built
@@ -418,13 +417,13 @@ struct StencilSmem {
     uint32_t collow[RC];            // bit r: the same, by column
     uint32_t rowbal[kTileH];        // bit x: pixel (row, x) of the tile is attempted
 };
-// three blocks per SM: 228 KB less 1 KB reserved per block
-static_assert(sizeof(StencilSmem) <= 76800, "the stencil tile keeps three blocks per SM");
+// four blocks per SM: 228 KB less 1 KB reserved per block
+static_assert(sizeof(StencilSmem) <= 57344, "the stencil tile keeps four blocks per SM");
 static_assert(kTileW == 32, "one warp per pixel row of the stencil tile");
 static_assert(sizeof(float) * RR * RC >= 4 * (kStencilThreads / 32 + 1) + 2 * kStencilThreads,
               "the attempted list fits in the aux tile");
 
-__global__ void __launch_bounds__(kStencilThreads)
+__global__ void __launch_bounds__(kStencilThreads, 4)
     k_stencil(const uint16_t *__restrict__ rgbi, Geometry g, const float *__restrict__ lut,
               const fx_stage *__restrict__ stages, fx_params p, CombineConst cc,
               const float *__restrict__ aux, const float *__restrict__ hs,
@@ -529,11 +528,11 @@ __global__ void __launch_bounds__(kStencilThreads)
 #pragma unroll
             for (int j = 0; j < 5; ++j) {
                 const ColumnSums cs = column_sums_wide(v + j);
-                S.cs[src][0][r0 + j][c] = (double)cs.s3;
-                S.cs[src][1][r0 + j][c] = (double)cs.s5;
-                S.cs[src][2][r0 + j][c] = (double)cs.s7;
-                S.cs[src][3][r0 + j][c] = (double)cs.s9;
-                S.cs[src][4][r0 + j][c] = (double)cs.b16;
+                S.cs[src][0][r0 + j][c] = cs.s3;
+                S.cs[src][1][r0 + j][c] = cs.s5;
+                S.cs[src][2][r0 + j][c] = cs.s7;
+                S.cs[src][3][r0 + j][c] = cs.s9;
+                S.cs[src][4][r0 + j][c] = cs.b16;
             }
         } else {
             const int q = it - kWaItems;
@@ -578,11 +577,11 @@ __global__ void __launch_bounds__(kStencilThreads)
             double wq[3], nq[3];
 #pragma unroll
             for (int src = 0; src < 2; ++src) {
-                const double(*s3)[CC] = S.cs[src][0];
-                const double(*s5)[CC] = S.cs[src][1];
-                const double(*s7)[CC] = S.cs[src][2];
-                const double(*s9)[CC] = S.cs[src][3];
-                const double(*bb)[CC] = S.cs[src][4];
+                const float(*s3)[CC] = S.cs[src][0];
+                const float(*s5)[CC] = S.cs[src][1];
+                const float(*s7)[CC] = S.cs[src][2];
+                const float(*s9)[CC] = S.cs[src][3];
+                const float(*bb)[CC] = S.cs[src][4];
                 double q69, q21;
                 q69_q21([&](int k) { return s3[r][c + k]; }, [&](int k) { return s5[r][c + k]; },
                         [&](int k) { return s7[r][c + k]; }, [&](int k) { return s9[r][c + k]; },
@@ -609,13 +608,6 @@ __global__ void __launch_bounds__(kStencilThreads)
             } else {
                 rec.a[3] = 0.0f;
                 rec.fb |= 8u;
-            }
-            if (r >= 1 && r <= kTileH && c >= 1 && c <= kTileW) {
-                float *cw = S.cw[r - 1][c - 1];
-                cw[0] = (float)wq[0];
-                cw[1] = (float)wq[1];
-                cw[2] = (float)wq[2];
-                cw[3] = point_score;
             }
         }
         S.rec[r][c] = rec;
@@ -667,7 +659,23 @@ __global__ void __launch_bounds__(kStencilThreads)
     }
     float weights[4];
 #pragma unroll
-    for (int l = 0; l < 4; ++l) weights[l] = S.cw[ty][tx][l];
+    {   // W of the centre record: the score patch averages, recomputed from
+        // the column sums (record row ty + 1, column tx + 1)
+        const float(*s3)[CC] = S.cs[0][0];
+        const float(*s5)[CC] = S.cs[0][1];
+        const float(*s7)[CC] = S.cs[0][2];
+        const float(*s9)[CC] = S.cs[0][3];
+        const float(*bb)[CC] = S.cs[0][4];
+        const int r = ty + 1, c = tx + 1;
+        double q69, q21;
+        q69_q21([&](int k) { return s3[r][c + k]; }, [&](int k) { return s5[r][c + k]; },
+                [&](int k) { return s7[r][c + k]; }, [&](int k) { return s9[r][c + k]; }, q69,
+                q21);
+        weights[0] = (float)q69;
+        weights[1] = (float)q21;
+        weights[2] = (float)q16_wa([&](int k) { return bb[r][c + k]; });
+        weights[3] = S.hs[ty + 5][tx + 5];  // point score
+    }
 
     // RGB candidates (reconstruction.py:425-462)
     float cand[3][3];
