@@ -518,7 +518,7 @@ __device__ __forceinline__ uint32_t jump_by_table(const Affine (*tab)[64], uint3
 // the attempted ones in shared memory; phase 2 processes that list densely,
 // each entry from its own start state g^(fixed + extra before it)(s0), and
 // checks the draws it makes against the classification and the walk.
-__global__ void __launch_bounds__(kSegThreads)
+__global__ void __launch_bounds__(kSegThreads, 5)
     k_apply(const uint8_t *__restrict__ meta, const double *__restrict__ cand, int64_t sites,
             int w, const uint16_t *__restrict__ rgbi, const float *__restrict__ lut,
             const uint32_t *__restrict__ g_high, const uint32_t *__restrict__ g_low,
