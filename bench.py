@@ -57,14 +57,14 @@ WALK_BLOCKS_PER_SM = 3   # window-walk segments per SM in one wave (kWinBlocksPe
 
 def launches_per_frame(h: int, w: int, per_wave: int) -> int:
     """Kernel launches of one plain pass (the library's launch sequence):
-    producer 4, planes 1, stencil 1, startup 1, chain 4, walk 1 + 2 per wave
+    producer 3, planes 1, stencil 1, startup 1, chain 4, walk 1 + 2 per wave
     + 1, apply 3.  Waves are sized from the RNG-dependent list capacity."""
 
     sites = 6 * w + h * w
     capacity = max(65536, sites // 2)
     segments = (capacity + 4095) // 4096 + 1
     waves = (segments + per_wave - 1) // per_wave
-    return 16 + 2 * waves
+    return 15 + 2 * waves
 
 
 def stencil_traffic():

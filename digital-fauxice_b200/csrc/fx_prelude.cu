@@ -56,8 +56,12 @@ __host__ __device__ inline int setter_stage(float p1, float p2, float p3, float 
 // ---------------------------------------------------------------------------
 
 struct ProducerBuffers {
-    uint8_t *cell_ok;      // [ne][cells]
-    double2 *terms;        // [ne][cells][4]  (term, ratio * term)
+    // [ne][cells] and [ne][cells][4]: kept in the scratch layout but no
+    // longer written (k_producer_rows accumulates the epoch sums itself), so
+    // the layout and the fixed-size scratch limits of the no-alloc entry stay
+    // as they are
+    uint8_t *cell_ok;
+    double2 *terms;
     double *row_sums;      // [3][h]  visible, infrared, weight
     double *cum;           // [3][h]
     float *add;            // [2][ne]
@@ -187,6 +191,8 @@ struct RowSmem {
     float qv[2][kTileCells][8];        // quadrant trees per tile cell (rb * 8 + cc)
     uint32_t rsum[2][kTileCells];      // raw IR total per tile cell
     int flag[2][kTileCells];           // 0: no complete epoch cell, 1: failing, 2: passing
+    double2 tq[kTileCells][4];         // finished terms of the previous tile's cells
+    int tok[kTileCells];               // 1: the cell's terms count (passing)
 };
 
 __device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
@@ -225,6 +231,7 @@ __global__ void __launch_bounds__(kRowWarps * 32, 1)
     double rv = 0.0, ri = 0.0, rw = 0.0;     // row r0 + lane
     double rv2 = 0.0, ri2 = 0.0, rw2 = 0.0;  // row r0 + 32 + lane (lanes < kRows - 32)
     const int lane2 = lane < kRows - 32 ? lane + 32 : lane;  // other lanes re-read their row
+    double den = 0.0, num = 0.0;  // lane rb < kRowBlocks: epoch (r0 / 8 + rb) sums
     for (int t = 0; t <= tiles; ++t) {
         asm volatile("cp.async.wait_group 0;\n" ::);
         __syncthreads();  // tile t staged; tile t-1's products complete
@@ -324,21 +331,33 @@ __global__ void __launch_bounds__(kRowWarps * 32, 1)
             const int u = t - 1, ub = u & 1;
             for (int cl = lane; cl < kTileCells; cl += 32) {
                 const int flag = S.flag[ub][cl];
-                if (flag) {
-                    const int rb = cl >> 3, cc = cl & 7;
-                    const int64_t e_idx = (int64_t)((r0 >> 3) + rb) * cells + (u * 8 + cc);
-                    b.cell_ok[e_idx] = flag == 2 ? 1 : 0;
-                    if (flag == 2) {
-                        const float *qv = S.qv[ub][cl];
-                        const float vq[4] = {qv[0], qv[1], qv[2], qv[3]};
-                        const float iq[4] = {qv[4], qv[5], qv[6], qv[7]};
-                        double2 terms[4];
-                        finish_terms(vq, iq, S.rsum[ub][cl], terms);
+                S.tok[cl] = flag == 2;
+                if (flag == 2) {
+                    const float *qv = S.qv[ub][cl];
+                    const float vq[4] = {qv[0], qv[1], qv[2], qv[3]};
+                    const float iq[4] = {qv[4], qv[5], qv[6], qv[7]};
+                    double2 terms[4];
+                    finish_terms(vq, iq, S.rsum[ub][cl], terms);
 #pragma unroll
-                        for (int q = 0; q < 4; ++q) b.terms[e_idx * 4 + q] = terms[q];
+                    for (int q = 0; q < 4; ++q) S.tq[cl][q] = terms[q];
+                }
+            }
+            __syncwarp();
+            // the epoch sums (producer_parameters.py epoch cell order): cells
+            // in column order, quadrants in order, passing cells only
+            if (lane < kRowBlocks) {
+                for (int cc = 0; cc < 8; ++cc) {
+                    const int cl = lane * 8 + cc;
+                    if (S.tok[cl]) {
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            den += S.tq[cl][q].x;
+                            num += S.tq[cl][q].y;
+                        }
                     }
                 }
             }
+            __syncwarp();
             // the ordered row sums, two rows per lane interleaved
             const int n = min(kRowTile, active_width - u * kRowTile);
             const double *pv = S.p[u & 1][0][lane];
@@ -382,38 +401,8 @@ __global__ void __launch_bounds__(kRowWarps * 32, 1)
         b.row_sums[h + row2] = ri2;
         b.row_sums[2 * h + row2] = rw2;
     }
-}
-
-// Epoch sums: one warp per complete epoch, sequential over cells and
-// quadrants (every lane carries the same running sums).
-__global__ void __launch_bounds__(32)
-    k_producer_epochs(int cells, int ne, ProducerBuffers b) {
-    const int e = blockIdx.x;
-    if (e >= ne) return;
-    const int lane = threadIdx.x;
-    double den = 0.0, num = 0.0;
-    for (int c0 = 0; c0 < cells; c0 += 32) {
-        const int c = c0 + lane;
-        const bool ok = c < cells && b.cell_ok[(int64_t)e * cells + c];
-        double2 t[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q)
-            t[q] = ok ? b.terms[((int64_t)e * cells + c) * 4 + q] : make_double2(0.0, 0.0);
-        const int n = min(32, cells - c0);
-        for (int j = 0; j < n; ++j) {
-            const bool okj = __shfl_sync(0xFFFFFFFFu, ok, j);
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const double tx = __shfl_sync(0xFFFFFFFFu, t[q].x, j);
-                const double ty = __shfl_sync(0xFFFFFFFFu, t[q].y, j);
-                if (okj) {
-                    den += tx;
-                    num += ty;
-                }
-            }
-        }
-    }
-    if (lane == 0) {
+    const int e = (r0 >> 3) + lane;
+    if (warp == 0 && lane < kRowBlocks && e < ne) {
         b.add[e] = (float)den;
         b.add[ne + e] = (float)num;
     }
@@ -592,7 +581,6 @@ cudaError_t launch_producer(const uint16_t *rgbi, int h, int w, const float *lut
     b.p_epoch = (float *)take(2 * (size_t)ne * sizeof(float));
     k_producer_rows<<<(h + kRows - 1) / kRows, kRowWarps * 32, sizeof(RowSmem), stream>>>(rgbi, h, w, aw,
                                                                                cells, lut, b);
-    if (ne > 0) k_producer_epochs<<<ne, 32, 0, stream>>>(cells, ne, b);
     k_producer_scan<<<1, kScanThreads, sizeof(ScanSmem), stream>>>(h, ne, b);
     k_stage_table<<<(h + 6 + 255) / 256, 256, 0, stream>>>(h, ne, 1.0f, b, stages, rows_out, err);
     return cudaGetLastError();
