@@ -129,7 +129,11 @@ FX_API void fx_context_destroy(fx_context *ctx);
 FX_API int fx_last_error(const fx_context *ctx, char *buf, size_t len);
 
 /* Upload the response LUT (x3a.py:111-132) and the two inverse-response
- * factor tables (output.py:40-58).  The caller hash-checks them. */
+ * factor tables (output.py:40-58).  The caller hash-checks them.  The call
+ * also builds, on the device, the emitted value of every raw sample (the
+ * output of every unattempted channel), and refuses a LUT holding a
+ * non-finite value with FX_ERR_NONFINITE_WORK ("work RGB must be finite");
+ * the context then has no tables until a valid set is uploaded. */
 FX_API int fx_set_tables(fx_context *ctx, const float *lut65536, const uint32_t *high256,
                          const uint32_t *low256);
 
