@@ -512,8 +512,9 @@ __global__ void __launch_bounds__(kWinThreads, kWinBlocksPerSM)
                 min(len, r + (next_compact > done0 ? next_compact - done0 : len));
             const bool end_next = (c0 + stop) < i1;
             // one slot: merging cannot lower the slot count, so only the
-            // span ends merge (duplicates step in lanes that run anyway)
-            const uint32_t merge_len = slots <= 1 ? kSegLen : ((done0 < 256u) ? 8u : 32u);
+            // span ends merge (duplicates step in lanes that run anyway);
+            // otherwise warps merge every 16 channels, then every 32
+            const uint32_t merge_len = slots <= 1 ? kSegLen : ((done0 < 256u) ? 16u : 32u);
             if (__any_sync(0xFFFFFFFFu, live_mask != 0)) {
                 switch (slots) {
 #define FX_WALK_CASE(K)                                                                         \
