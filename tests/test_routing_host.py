@@ -261,3 +261,31 @@ def test_no_cpu_fallback_without_a_device():
         pytest.skip("a CUDA device is present")
     with pytest.raises((RuntimeError, OSError)):
         routing.route_at_floor_mask(np.zeros((8, 8), dtype=np.bool_))
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_native_region_writer_matches_json_on_random_tables(seed):
+    """Random tables (empty and long id lists, large values): the library's
+    region lists equal json.dumps of the same region dicts, canonical form."""
+
+    rng = np.random.default_rng(seed)
+    k, f = int(rng.integers(0, 60)), int(rng.integers(0, 25))
+    big = np.iinfo(np.int64).max // 4
+    reasons = ["not_routed", "chessboard_radius", "area", "area+chessboard_radius"]
+    dispositions = ["routed", "absorbed", "pristine", "perimeter_excluded"]
+    rand_ids = lambda n: sorted(rng.choice(10**6, size=n, replace=False).tolist())  # noqa: E731
+    prov = [{"id": i + 1, "bbox_yxyx_half_open": rng.integers(0, big, 4).tolist(),
+             "area": int(rng.integers(0, big)), "max_chessboard_radius": int(rng.integers(0, 10**9)),
+             "routed_reason": reasons[int(rng.integers(0, 4))],
+             "disposition": dispositions[int(rng.integers(0, 4))],
+             "final_component_ids": rand_ids(int(rng.integers(0, 6))),
+             "absorbed_pixel_count": int(rng.integers(0, big))} for i in range(k)]
+    fin = [{"id": i + 1, "bbox_yxyx_half_open": rng.integers(0, big, 4).tolist(),
+            "area": int(rng.integers(0, big)), "direct_region_ids": rand_ids(int(rng.integers(0, 5))),
+            "absorbed_region_ids": rand_ids(int(rng.integers(0, 40))),
+            "non_floor_synthesis_pixels": int(rng.integers(0, big))} for i in range(f)]
+    tables = tables_from_oracle({"provisional_regions": prov, "final_regions": fin})
+    provisional, final = routing._native_lists(tables)
+    dumps = lambda v: ro.serialize(v)[:-1]  # noqa: E731  (canonical, no trailing newline)
+    assert provisional == dumps(prov)
+    assert final == dumps(fin)
