@@ -41,7 +41,7 @@ METRIC = ("bit-exact full-frame megapixels/s on 1 B200 (batched vs plain); "
           "p50/p99 frame latency")
 HEIGHT, WIDTH = 5782, 3946
 SEED = 2
-# Algorithmic bytes (DESIGN.md "Roofline"): the stencil stage reads 8 B of
+# Algorithmic bytes: the stencil stage reads 8 B of
 # RGBI and writes a 24 B float64 candidate plus 1 B of status per pixel; the
 # serial walk reads a 32 B interval/jump entry and writes a 4 B running count
 # per RNG-dependent channel.
@@ -262,7 +262,7 @@ def make_job(main, prepass):
         focus_exposure_locked=True)
 
 
-def cpu_reference(main, prepass, steps: int, warmup: int, budget_s: float = 6.0):
+def cpu_reference(main, prepass, steps: int, warmup: int, sample_s: float = 6.0):
     """Time the oracle (C, OpenMP, all host cores) on bounded row bands."""
 
     from oracle import oracle as ox
@@ -272,8 +272,8 @@ def cpu_reference(main, prepass, steps: int, warmup: int, budget_s: float = 6.0)
     ox.process(main, prepass, threads=cores, diagnostics=False)
     full_s = time.perf_counter() - t0
     rows = main.shape[0]
-    if full_s > budget_s:
-        rows = max(64, int(main.shape[0] * budget_s / full_s))
+    if full_s > sample_s:
+        rows = max(64, int(main.shape[0] * sample_s / full_s))
     sample = np.ascontiguousarray(main[:rows])
     times = []
     for i in range(warmup + steps):
@@ -439,7 +439,7 @@ def run_b200(args, world, rank, local, frames=None):
 
     cpu = None
     if not args.no_cpu_baseline and world == 1 and rank == 0:
-        cpu = cpu_reference(main, prepass, steps=1, warmup=0, budget_s=12.0)
+        cpu = cpu_reference(main, prepass, steps=1, warmup=0, sample_s=12.0)
         cpu.pop("seconds_per_step", None)
 
     if rank == 0:

@@ -117,7 +117,7 @@ def serve(ctx: _lib.Context, requests: Sequence[Request], *, slots: int = 4,
     free_pairs: deque[int] = deque(range(slots))
     copy_stream = torch.cuda.Stream()
     waiting: deque[int] = deque()
-    staging: deque[tuple] = deque()  # (index, pair, event): uploads in flight, in order
+    staging: deque[tuple] = deque()  # (index, pair, event, admitted): uploads in flight, in order
     inflight: dict[int, tuple] = {}  # ticket -> (index, admitted, pair)
     torch.cuda.synchronize()
     nxt = 0
