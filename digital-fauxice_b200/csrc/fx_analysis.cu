@@ -48,6 +48,7 @@ __global__ void __launch_bounds__(256)
              float *__restrict__ hs, float *__restrict__ hwa, float *__restrict__ hwr,
              int64_t plane, uint32_t *err) {
     __shared__ float s_aux[256 + 2];  // aux of columns x-1 .. x+256 of the segment
+    if (pass_stopped(err)) return;
     const int px = blockIdx.x * blockDim.x + threadIdx.x;
     const int py = blockIdx.y;
     const int y = py - kPad, x = px - kPad;
@@ -431,6 +432,7 @@ __global__ void __launch_bounds__(kStencilThreads, 4)
               double *__restrict__ cand_out, uint8_t *__restrict__ meta_out, uint32_t *err) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     StencilSmem &S = *reinterpret_cast<StencilSmem *>(smem_raw);
+    if (pass_stopped(err)) return;
     const int tid = threadIdx.x;
     const int y0 = blockIdx.y * kTileH, x0 = blockIdx.x * kTileW;
     const int h = g.h, w = g.w;
@@ -779,6 +781,7 @@ __global__ void k_startup(const uint16_t *__restrict__ rgbi, StartupView v,
                           const float *__restrict__ lut, const fx_stage *__restrict__ stages,
                           fx_params p, CombineConst cc, double *__restrict__ cand_out,
                           uint8_t *__restrict__ meta_out, uint32_t *err) {
+    if (pass_stopped(err)) return;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     const int k = blockIdx.y;  // stage hit k+1, centre k-6
     const int w = v.g.w;

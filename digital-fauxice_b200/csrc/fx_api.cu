@@ -125,6 +125,10 @@ struct Slot {
     void *h_out = nullptr;
     size_t h_out_bytes = 0;
     void *h_ctr = nullptr;  // DevCounters copy + error word
+    // cancel word: pinned host memory the pass's stage gates read through
+    // its device mapping (fx_cancel sets it; a new request clears it)
+    volatile uint32_t *cancel_host = nullptr;
+    uint32_t *cancel_dev = nullptr;
     cudaEvent_t chunk_done[16] = {};  // staged downloads (fx_process)
     // request in flight
     bool busy = false;
@@ -134,6 +138,7 @@ struct Slot {
     std::vector<fx_stage> stages;
     bool has_stages = false;
     Geometry g{};
+    bool stage_score = false, stage_changed = false;  // planes staged in h_out
     // device-buffer request (fx_submit_device): caller-owned device memory
     bool device = false;
     const uint16_t *d_in = nullptr;
@@ -149,6 +154,8 @@ struct fx_context {
     bool profile = false;
     bool parallel_walk = true;
     int walk_wave = 0;  // window segments per wave; 0: g_per_wave (three per SM)
+    double walk_sigmas = fx::kDefaultWindowSigmas;  // walk window half-width
+    int64_t list_capacity = 0;  // RNG-dependent list entries per frame; 0: sites / 2
     std::vector<std::vector<cudaEvent_t>> pending;  // recorded, not yet read
     std::vector<std::vector<cudaEvent_t>> spare;
     double profile_ms[fx::kProfileStages] = {0};
@@ -169,6 +176,12 @@ struct fx_context {
 
 namespace fx {
 
+// RNG-dependent list capacity of a frame: the override of
+// fx_set_list_capacity when one is set, else sites / 2 (at least 65536).
+static int64_t amb_capacity(const fx_context *ctx, const Geometry &g) {
+    return ctx->list_capacity > 0 ? ctx->list_capacity : default_amb_capacity(g);
+}
+
 static char g_error[512];
 
 static int fail(fx_context *ctx, int code, const char *fmt, ...) {
@@ -188,7 +201,6 @@ static int fail(fx_context *ctx, int code, const char *fmt, ...) {
     } while (0)
 
 static int ensure_arena(fx_context *ctx, Slot &s, const Geometry &g, int64_t amb_cap) {
-    Arena probe;
     const size_t need = arena_layout(g, amb_cap, nullptr);
     if (s.arena.base && s.arena.bytes >= need) {
         const size_t bytes = s.arena.bytes;
@@ -214,7 +226,6 @@ static int ensure_arena(fx_context *ctx, Slot &s, const Geometry &g, int64_t amb
     s.arena.base = base;
     s.arena.bytes = need;
     arena_layout(g, amb_cap, &s.arena);
-    (void)probe;
     return FX_OK;
 }
 
@@ -242,9 +253,12 @@ static int check_frame(fx_context *ctx, const fx_params *p, int h, int w) {
 
 // Enqueue the whole pass for one frame whose input already sits in
 // s.arena.rgbi (or `d_in`).  Outputs land in the arena (or `d_out`).
+// `cancellable` passes (fx_submit, fx_submit_device) get stage gates that
+// read the slot's cancel word.
 static int enqueue_pass(fx_context *ctx, Slot &s, const Geometry &g, const fx_params &p,
                         const fx_stage *host_stages, uint32_t rng, const uint16_t *d_in,
-                        uint16_t *d_out, uint8_t *d_changed, bool producer_rows) {
+                        uint16_t *d_out, uint8_t *d_changed, bool producer_rows,
+                        bool cancellable = false) {
     Arena &a = s.arena;
     cudaStream_t st = s.stream;
     Marks marks;
@@ -270,13 +284,15 @@ static int enqueue_pass(fx_context *ctx, Slot &s, const Geometry &g, const fx_pa
                                      producer_rows ? a.rows : nullptr, a.err, st));
     }
     marks.mark(1, st);
+    const uint32_t *cancel = cancellable ? s.cancel_dev : nullptr;
+    FX_CUDA(ctx, launch_gate(cancel, a.err, st));
     FX_CUDA(ctx, launch_analysis(d_in, g, ctx->lut, a.stages, p, a.aux, a.hs, a.hwa, a.hwr,
                                  (int64_t)g.prow * g.pitch, a.cand, a.meta, a.err, st, marks));
     // the walk scratch is sized for g_per_wave; a narrower wave uses part of it
     const int wave = (ctx->walk_wave > 0 && ctx->walk_wave < g_per_wave) ? ctx->walk_wave
                                                                          : g_per_wave;
     WriterBuffers wb{a.seg_base, a.seg_amb, a.entries, a.pos, a.extra, a.counters,
-                     a.amb_capacity, a.walk, wave, ctx->parallel_walk};
+                     a.amb_capacity, a.walk, wave, ctx->parallel_walk, ctx->walk_sigmas, cancel};
     FX_CUDA(ctx, launch_writer(g, a.meta, a.cand, d_in, ctx->lut, ctx->high, ctx->low, ctx->ident, a.stages,
                                p, rng, wb, d_out, d_changed, a.err, st, marks));
     return FX_OK;
@@ -284,6 +300,8 @@ static int enqueue_pass(fx_context *ctx, Slot &s, const Geometry &g, const fx_pa
 
 static int error_from_device(fx_context *ctx, uint32_t code) {
     switch (code) {
+    case FX_ERR_CANCELLED:
+        return fail(ctx, (int)code, "the request was cancelled");
     case FX_ERR_NONFINITE_AUX:
         return fail(ctx, (int)code, "auxiliary score input must be a finite HxW plane");
     case FX_ERR_NONFINITE_WORK:
@@ -319,6 +337,9 @@ int context_fail(fx_context *ctx, int code, const char *fmt, ...) {
 
 int context_device_error(fx_context *ctx, uint32_t code) { return error_from_device(ctx, code); }
 
+void context_lock(fx_context *ctx) { ctx->mu.lock(); }
+void context_unlock(fx_context *ctx) { ctx->mu.unlock(); }
+
 // Counters + error word of the slot, after the stream completed.
 static int finish_counters(fx_context *ctx, Slot &s, const void *ctr_copy, uint32_t err,
                            fx_counters *out, bool *overflow) {
@@ -334,6 +355,14 @@ static int finish_counters(fx_context *ctx, Slot &s, const void *ctr_copy, uint3
 
 static Slot &slot0(fx_context *ctx) { return ctx->slots[0]; }
 
+// The synchronous entry points run on slot 0; a request of fx_submit /
+// fx_submit_device may hold it, and its buffers must not move under it.
+static int check_slot0_free(fx_context *ctx) {
+    if (slot0(ctx).busy)
+        return fail(ctx, FX_PENDING, "slot 0 holds a request in flight: wait for it first");
+    return FX_OK;
+}
+
 static int ensure_slots(fx_context *ctx, int n) {
     while ((int)ctx->slots.size() < n) {
         ctx->slots.emplace_back();
@@ -341,6 +370,13 @@ static int ensure_slots(fx_context *ctx, int n) {
         FX_CUDA(ctx, cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking));
         FX_CUDA(ctx, cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming));
         FX_CUDA(ctx, cudaMallocHost(&s.h_ctr, dev_counters_bytes() + 64));  // + err + count
+        void *word = nullptr;
+        FX_CUDA(ctx, cudaHostAlloc(&word, 64, cudaHostAllocMapped));
+        s.cancel_host = static_cast<volatile uint32_t *>(word);
+        *s.cancel_host = 0u;
+        void *dev = nullptr;
+        FX_CUDA(ctx, cudaHostGetDevicePointer(&dev, word, 0));
+        s.cancel_dev = static_cast<uint32_t *>(dev);
     }
     return FX_OK;
 }
@@ -352,6 +388,7 @@ static int run_device(fx_context *ctx, Slot &s, const Geometry &g, const fx_para
                       uint8_t *d_changed, fx_counters *counters, bool producer_rows) {
     int64_t cap = s.arena.base ? s.arena.amb_capacity : default_amb_capacity(g);
     if (cap < default_amb_capacity(g)) cap = default_amb_capacity(g);
+    if (ctx->list_capacity > 0) cap = ctx->list_capacity;
     for (int attempt = 0; attempt < 2; ++attempt) {
         // keep caller-side device pointers stable: the arena may move only
         // when the input/outputs live in it
@@ -404,7 +441,7 @@ FX_API int fx_device_check(int device, char *reason, size_t reason_len) {
     if (cudaGetDeviceProperties(&prop, device) != cudaSuccess)
         return say(FX_ERR_NO_DEVICE, "cannot query the CUDA device");
     if (prop.major != 10 || prop.minor != 0) {
-        char buf[160];
+        char buf[384];
         snprintf(buf, sizeof(buf), "device %s is sm_%d%d; this library is built for sm_100a",
                  prop.name, prop.major, prop.minor);
         return say(FX_ERR_UNSUPPORTED_DEVICE, buf);
@@ -451,6 +488,7 @@ FX_API void fx_context_destroy(fx_context *ctx) {
         if (s.h_in) cudaFreeHost(s.h_in);
         if (s.h_out) cudaFreeHost(s.h_out);
         if (s.h_ctr) cudaFreeHost(s.h_ctr);
+        if (s.cancel_host) cudaFreeHost(const_cast<uint32_t *>(s.cancel_host));
         if (s.done) cudaEventDestroy(s.done);
         for (cudaEvent_t e : s.chunk_done)
             if (e) cudaEventDestroy(e);
@@ -512,9 +550,11 @@ FX_API int fx_producer_rows(fx_context *ctx, const uint16_t *main_rgbi, int32_t 
     std::lock_guard<std::mutex> lock(ctx->mu);
     cudaSetDevice(ctx->device);
     if (!ctx->tables) return fail(ctx, FX_ERR_TABLES, "fx_set_tables has not been called");
+    int rc = check_slot0_free(ctx);
+    if (rc) return rc;
     Slot &s = slot0(ctx);
     const Geometry g = make_geometry(h, w);
-    int rc = ensure_arena(ctx, s, g, default_amb_capacity(g));
+    rc = ensure_arena(ctx, s, g, default_amb_capacity(g));
     if (rc) return rc;
     FX_CUDA(ctx, cudaMemsetAsync(s.arena.err, 0, 16, s.stream));
     FX_CUDA(ctx, cudaMemcpyAsync(s.arena.rgbi, main_rgbi, (size_t)h * w * 8,
@@ -657,10 +697,12 @@ FX_API int fx_process(fx_context *ctx, const fx_frame *f, fx_counters *counters)
     if (rc) return rc;
     if (!f->stages && f->width < 8)
         return fail(ctx, FX_ERR_GEOMETRY, "main RGBI frame has no complete producer cell");
+    rc = check_slot0_free(ctx);
+    if (rc) return rc;
     Slot &s = slot0(ctx);
     const Geometry g = make_geometry(f->height, f->width);
     const size_t px = (size_t)g.h * g.w;
-    int64_t cap = default_amb_capacity(g);
+    int64_t cap = amb_capacity(ctx, g);
     for (int attempt = 0; attempt < 2; ++attempt) {
         rc = ensure_arena(ctx, s, g, cap);
         if (rc) return rc;
@@ -711,6 +753,8 @@ FX_API int fx_process_device(fx_context *ctx, const uint16_t *d_rgbi, int32_t h,
     if (rc) return rc;
     if (!stages && w < 8)
         return fail(ctx, FX_ERR_GEOMETRY, "main RGBI frame has no complete producer cell");
+    rc = check_slot0_free(ctx);
+    if (rc) return rc;
     Slot &s = slot0(ctx);
     cudaStream_t user = reinterpret_cast<cudaStream_t>(stream);
     cudaStream_t saved = s.stream;
@@ -719,7 +763,7 @@ FX_API int fx_process_device(fx_context *ctx, const uint16_t *d_rgbi, int32_t h,
     if (counters) {
         rc = run_device(ctx, s, g, *params, stages, rng, d_rgbi, d_out, d_changed, counters, false);
     } else {
-        rc = ensure_arena(ctx, s, g, default_amb_capacity(g));
+        rc = ensure_arena(ctx, s, g, amb_capacity(ctx, g));
         if (!rc) rc = enqueue_pass(ctx, s, g, *params, stages, rng, d_rgbi, d_out, d_changed, false);
     }
     s.last_stream = s.stream;
@@ -796,9 +840,9 @@ FX_API int fx_reserve_frames(fx_context *ctx, int32_t max_height, int32_t max_wi
     const Geometry g = make_geometry(max_height, max_width);
     for (Slot &s : ctx->slots) {
         if (s.busy) return fail(ctx, FX_ERR_INVALID_ARGUMENT, "a slot is busy: reserve first");
-        const int64_t cap = s.arena.base && s.arena.amb_capacity > default_amb_capacity(g)
+        const int64_t cap = s.arena.base && s.arena.amb_capacity > amb_capacity(ctx, g)
                                 ? s.arena.amb_capacity
-                                : default_amb_capacity(g);
+                                : amb_capacity(ctx, g);
         const int rc = ensure_arena(ctx, s, g, cap);
         if (rc) return rc;
     }
@@ -812,25 +856,49 @@ FX_API int fx_set_slots(fx_context *ctx, int32_t slots) {
     return ensure_slots(ctx, slots);
 }
 
+// Device-to-host copies of a host-buffer request's results into the slot's
+// pinned staging (h_out: RGB16 at 0, score at 6 px, changed at 10 px), then
+// its counters and error word.
+static int stage_host_results(fx_context *ctx, Slot &s) {
+    const Geometry &g = s.g;
+    const size_t px = (size_t)g.h * g.w;
+    char *ho = reinterpret_cast<char *>(s.h_out);
+    FX_CUDA(ctx, cudaMemcpyAsync(ho, s.arena.out, px * 6, cudaMemcpyDeviceToHost, s.stream));
+    if (s.stage_score)
+        FX_CUDA(ctx, cudaMemcpy2DAsync(ho + px * 6, (size_t)g.w * 4,
+                                       s.arena.hs + g.padded_index(0, 0), (size_t)g.pitch * 4,
+                                       (size_t)g.w * 4, g.h, cudaMemcpyDeviceToHost, s.stream));
+    if (s.stage_changed)
+        FX_CUDA(ctx, cudaMemcpyAsync(ho + px * 10, s.arena.changed, px, cudaMemcpyDeviceToHost,
+                                     s.stream));
+    char *hc = reinterpret_cast<char *>(s.h_ctr);
+    FX_CUDA(ctx, cudaMemcpyAsync(hc, s.arena.counters, dev_counters_bytes(),
+                                 cudaMemcpyDeviceToHost, s.stream));
+    FX_CUDA(ctx, cudaMemcpyAsync(hc + dev_counters_bytes(), s.arena.err, 4,
+                                 cudaMemcpyDeviceToHost, s.stream));
+    return FX_OK;
+}
+
+static Slot *free_slot(fx_context *ctx) {
+    for (Slot &s : ctx->slots)
+        if (!s.busy) return &s;
+    return nullptr;
+}
+
 FX_API int fx_submit(fx_context *ctx, const fx_frame *f, int64_t *ticket) {
-    if (!ctx || !f || !f->main_rgbi || !f->rgb_out || !ticket) return FX_ERR_INVALID_ARGUMENT;
+    if (!ctx || !f || !f->main_rgbi || !ticket) return FX_ERR_INVALID_ARGUMENT;
     std::lock_guard<std::mutex> lock(ctx->mu);
     cudaSetDevice(ctx->device);
     int rc = check_frame(ctx, f->params, f->height, f->width);
     if (rc) return rc;
     if (!f->stages && f->width < 8)
         return fail(ctx, FX_ERR_GEOMETRY, "main RGBI frame has no complete producer cell");
-    Slot *slot = nullptr;
-    for (Slot &s : ctx->slots)
-        if (!s.busy) {
-            slot = &s;
-            break;
-        }
+    Slot *slot = free_slot(ctx);
     if (!slot) return fail(ctx, FX_PENDING, "no free slot");
     Slot &s = *slot;
     const Geometry g = make_geometry(f->height, f->width);
     const size_t px = (size_t)g.h * g.w;
-    rc = ensure_arena(ctx, s, g, default_amb_capacity(g));
+    rc = ensure_arena(ctx, s, g, amb_capacity(ctx, g));
     if (rc) return rc;
     const size_t in_bytes = px * 8;
     const size_t out_bytes = px * 6 + px * 4 + px;
@@ -856,24 +924,17 @@ FX_API int fx_submit(fx_context *ctx, const fx_frame *f, int64_t *ticket) {
     s.has_stages = f->stages != nullptr;
     if (s.has_stages) s.stages.assign(f->stages, f->stages + (g.h + 6));
     s.g = g;
+    // no output buffer now: every result stays staged for fx_fetch
+    const bool deferred = f->rgb_out == nullptr;
+    s.stage_score = deferred || f->score_out;
+    s.stage_changed = deferred || f->changed_out;
+    *s.cancel_host = 0u;
     FX_CUDA(ctx, cudaMemcpyAsync(s.arena.rgbi, s.h_in, in_bytes, cudaMemcpyHostToDevice, s.stream));
     rc = enqueue_pass(ctx, s, g, s.params, s.has_stages ? s.stages.data() : nullptr,
-                      f->rng_state, s.arena.rgbi, s.arena.out, s.arena.changed, false);
+                      f->rng_state, s.arena.rgbi, s.arena.out, s.arena.changed, false, true);
     if (rc) return rc;
-    char *ho = reinterpret_cast<char *>(s.h_out);
-    FX_CUDA(ctx, cudaMemcpyAsync(ho, s.arena.out, px * 6, cudaMemcpyDeviceToHost, s.stream));
-    if (f->score_out)
-        FX_CUDA(ctx, cudaMemcpy2DAsync(ho + px * 6, (size_t)g.w * 4,
-                                       s.arena.hs + g.padded_index(0, 0), (size_t)g.pitch * 4,
-                                       (size_t)g.w * 4, g.h, cudaMemcpyDeviceToHost, s.stream));
-    if (f->changed_out)
-        FX_CUDA(ctx, cudaMemcpyAsync(ho + px * 10, s.arena.changed, px, cudaMemcpyDeviceToHost,
-                                     s.stream));
-    char *hc = reinterpret_cast<char *>(s.h_ctr);
-    FX_CUDA(ctx, cudaMemcpyAsync(hc, s.arena.counters, dev_counters_bytes(),
-                                 cudaMemcpyDeviceToHost, s.stream));
-    FX_CUDA(ctx, cudaMemcpyAsync(hc + dev_counters_bytes(), s.arena.err, 4,
-                                 cudaMemcpyDeviceToHost, s.stream));
+    rc = stage_host_results(ctx, s);
+    if (rc) return rc;
     FX_CUDA(ctx, cudaEventRecord(s.done, s.stream));
     s.busy = true;
     s.ticket = ctx->next_ticket++;
@@ -908,16 +969,11 @@ FX_API int fx_submit_device(fx_context *ctx, const uint16_t *d_rgbi, int32_t h, 
     if (rc) return rc;
     if (!stages && w < 8)
         return fail(ctx, FX_ERR_GEOMETRY, "main RGBI frame has no complete producer cell");
-    Slot *slot = nullptr;
-    for (Slot &s : ctx->slots)
-        if (!s.busy) {
-            slot = &s;
-            break;
-        }
+    Slot *slot = free_slot(ctx);
     if (!slot) return fail(ctx, FX_PENDING, "no free slot");
     Slot &s = *slot;
     const Geometry g = make_geometry(h, w);
-    rc = ensure_arena(ctx, s, g, default_amb_capacity(g));
+    rc = ensure_arena(ctx, s, g, amb_capacity(ctx, g));
     if (rc) return rc;
     s.frame = fx_frame{};
     s.frame.height = h;
@@ -933,8 +989,9 @@ FX_API int fx_submit_device(fx_context *ctx, const uint16_t *d_rgbi, int32_t h, 
     s.d_out = d_out;
     s.d_score = d_score;
     s.d_changed = d_changed;
+    *s.cancel_host = 0u;
     rc = enqueue_pass(ctx, s, g, s.params, s.has_stages ? s.stages.data() : nullptr, rng, d_rgbi,
-                      d_out, d_changed, false);
+                      d_out, d_changed, false, true);
     if (rc) return rc;
     rc = copy_device_results(ctx, s);
     if (rc) return rc;
@@ -963,8 +1020,74 @@ FX_API int fx_poll(fx_context *ctx, int64_t ticket) {
     return FX_OK;
 }
 
-FX_API int fx_wait(fx_context *ctx, int64_t ticket, int64_t timeout_ns, fx_counters *counters) {
+FX_API int fx_cancel(fx_context *ctx, int64_t ticket) {
     if (!ctx) return FX_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    Slot *s = find_ticket(ctx, ticket);
+    if (!s) return fail(ctx, FX_ERR_INVALID_ARGUMENT, "unknown ticket");
+    *s->cancel_host = 1u;  // read by the pass's next stage gate
+    return FX_OK;
+}
+
+// Where fx_fetch puts a host request's results (NULL: not wanted).
+struct FetchTargets {
+    uint16_t *rgb;
+    float *score;
+    uint8_t *at_floor;
+    uint8_t *changed;
+};
+
+// The pass of slot s completed with more RNG-dependent channels than its
+// list held (rare): rerun it synchronously with room for all of them.
+static int rerun_with_capacity(fx_context *ctx, Slot &s, fx_counters *counters) {
+    char *hc = reinterpret_cast<char *>(s.h_ctr);
+    const int64_t cap = (int64_t)counters_n_amb(hc) + 1024;
+    int rc = ensure_arena(ctx, s, s.g, cap);
+    if (rc) return rc;
+    if (s.device) {
+        rc = enqueue_pass(ctx, s, s.g, s.params, s.has_stages ? s.stages.data() : nullptr,
+                          s.frame.rng_state, s.d_in, s.d_out, s.d_changed, false, true);
+        if (!rc) rc = copy_device_results(ctx, s);
+    } else {
+        const size_t px = (size_t)s.g.h * s.g.w;
+        FX_CUDA(ctx, cudaMemcpyAsync(s.arena.rgbi, s.h_in, px * 8, cudaMemcpyHostToDevice,
+                                     s.stream));
+        rc = enqueue_pass(ctx, s, s.g, s.params, s.has_stages ? s.stages.data() : nullptr,
+                          s.frame.rng_state, s.arena.rgbi, s.arena.out, s.arena.changed, false,
+                          true);
+        if (!rc) rc = stage_host_results(ctx, s);
+    }
+    if (rc) return rc;
+    if (cudaStreamSynchronize(s.stream) != cudaSuccess)
+        return fail(ctx, FX_ERR_CUDA, "capacity rerun failed");
+    uint32_t err;
+    std::memcpy(&err, hc + dev_counters_bytes(), 4);
+    bool overflow;
+    rc = finish_counters(ctx, s, hc, err, counters, &overflow);
+    if (!rc && overflow) rc = fail(ctx, FX_ERR_INTERNAL, "capacity rerun overflowed");
+    return rc;
+}
+
+// Copy a completed host request's staged results to the caller.
+static void deliver_host_results(Slot &s, const FetchTargets *fetch) {
+    const size_t px = (size_t)s.g.h * s.g.w;
+    const char *ho = reinterpret_cast<const char *>(s.h_out);
+    uint16_t *rgb = fetch ? fetch->rgb : s.frame.rgb_out;
+    float *score = fetch ? fetch->score : s.frame.score_out;
+    uint8_t *changed = fetch ? fetch->changed : s.frame.changed_out;
+    if (rgb) std::memcpy(rgb, ho, px * 6);
+    if (score) std::memcpy(score, ho + px * 6, px * 4);
+    if (changed) std::memcpy(changed, ho + px * 10, px);
+    if (fetch && fetch->at_floor) {
+        // engine.py:175-199: at-floor = score plane == the score floor
+        const float *sp = reinterpret_cast<const float *>(ho + px * 6);
+        const float floor = s.params.score_floor;
+        for (size_t i = 0; i < px; ++i) fetch->at_floor[i] = sp[i] == floor ? 1u : 0u;
+    }
+}
+
+static int wait_ticket(fx_context *ctx, int64_t ticket, int64_t timeout_ns, fx_counters *counters,
+                       const FetchTargets *fetch) {
     const auto start = std::chrono::steady_clock::now();
     for (;;) {
         {
@@ -973,71 +1096,19 @@ FX_API int fx_wait(fx_context *ctx, int64_t ticket, int64_t timeout_ns, fx_count
             Slot *sp = find_ticket(ctx, ticket);
             if (!sp) return fail(ctx, FX_ERR_INVALID_ARGUMENT, "unknown ticket");
             Slot &s = *sp;
+            if (fetch && (s.device || ((fetch->score || fetch->at_floor) && !s.stage_score) ||
+                          (fetch->changed && !s.stage_changed)))
+                return fail(ctx, FX_ERR_INVALID_ARGUMENT,
+                            "fx_fetch: the request did not stage what was asked for");
             const cudaError_t e = cudaEventQuery(s.done);
             if (e == cudaSuccess) {
-                const size_t px = (size_t)s.g.h * s.g.w;
                 char *hc = reinterpret_cast<char *>(s.h_ctr);
                 uint32_t err;
                 std::memcpy(&err, hc + dev_counters_bytes(), 4);
                 bool overflow;
                 int rc = finish_counters(ctx, s, hc, err, counters, &overflow);
-                if (!rc && overflow && s.device) {
-                    // rare: more RNG-dependent channels than the default
-                    // capacity; rerun synchronously with room for all
-                    const int64_t cap = (int64_t)counters_n_amb(hc) + 1024;
-                    rc = ensure_arena(ctx, s, s.g, cap);
-                    if (!rc)
-                        rc = enqueue_pass(ctx, s, s.g, s.params,
-                                          s.has_stages ? s.stages.data() : nullptr,
-                                          s.frame.rng_state, s.d_in, s.d_out, s.d_changed, false);
-                    if (!rc) rc = copy_device_results(ctx, s);
-                    if (!rc && cudaStreamSynchronize(s.stream) != cudaSuccess)
-                        rc = fail(ctx, FX_ERR_CUDA, "retry failed");
-                    std::memcpy(&err, hc + dev_counters_bytes(), 4);
-                    if (!rc) rc = finish_counters(ctx, s, hc, err, counters, &overflow);
-                    if (!rc && overflow) rc = fail(ctx, FX_ERR_INTERNAL, "capacity retry");
-                } else if (!rc && overflow) {
-                    // rare: more RNG-dependent channels than the default
-                    // capacity; rerun synchronously with room for all
-                    fx_frame f = s.frame;
-                    f.main_rgbi = reinterpret_cast<const uint16_t *>(s.h_in);
-                    const int64_t cap = (int64_t)counters_n_amb(hc) + 1024;
-                    rc = ensure_arena(ctx, s, s.g, cap);
-                    if (!rc) {
-                        cudaMemcpyAsync(s.arena.rgbi, s.h_in, px * 8, cudaMemcpyHostToDevice,
-                                        s.stream);
-                        rc = enqueue_pass(ctx, s, s.g, s.params,
-                                          s.has_stages ? s.stages.data() : nullptr, f.rng_state,
-                                          s.arena.rgbi, s.arena.out, s.arena.changed, false);
-                    }
-                    if (!rc) {
-                        char *ho = reinterpret_cast<char *>(s.h_out);
-                        cudaMemcpyAsync(ho, s.arena.out, px * 6, cudaMemcpyDeviceToHost, s.stream);
-                        if (f.score_out)
-                            cudaMemcpy2DAsync(ho + px * 6, (size_t)s.g.w * 4,
-                                              s.arena.hs + s.g.padded_index(0, 0),
-                                              (size_t)s.g.pitch * 4, (size_t)s.g.w * 4, s.g.h,
-                                              cudaMemcpyDeviceToHost, s.stream);
-                        if (f.changed_out)
-                            cudaMemcpyAsync(ho + px * 10, s.arena.changed, px,
-                                            cudaMemcpyDeviceToHost, s.stream);
-                        cudaMemcpyAsync(hc, s.arena.counters, dev_counters_bytes(),
-                                        cudaMemcpyDeviceToHost, s.stream);
-                        cudaMemcpyAsync(hc + dev_counters_bytes(), s.arena.err, 4,
-                                        cudaMemcpyDeviceToHost, s.stream);
-                        if (cudaStreamSynchronize(s.stream) != cudaSuccess)
-                            rc = fail(ctx, FX_ERR_CUDA, "retry failed");
-                        std::memcpy(&err, hc + dev_counters_bytes(), 4);
-                        if (!rc) rc = finish_counters(ctx, s, hc, err, counters, &overflow);
-                        if (!rc && overflow) rc = fail(ctx, FX_ERR_INTERNAL, "capacity retry");
-                    }
-                }
-                if (!rc && !s.device) {
-                    const char *ho = reinterpret_cast<const char *>(s.h_out);
-                    std::memcpy(s.frame.rgb_out, ho, px * 6);
-                    if (s.frame.score_out) std::memcpy(s.frame.score_out, ho + px * 6, px * 4);
-                    if (s.frame.changed_out) std::memcpy(s.frame.changed_out, ho + px * 10, px);
-                }
+                if (!rc && overflow) rc = rerun_with_capacity(ctx, s, counters);
+                if (!rc && !s.device) deliver_host_results(s, fetch);
                 s.busy = false;
                 s.ticket = -1;
                 return rc;
@@ -1054,6 +1125,33 @@ FX_API int fx_wait(fx_context *ctx, int64_t ticket, int64_t timeout_ns, fx_count
         }
         std::this_thread::sleep_for(std::chrono::microseconds(50));
     }
+}
+
+FX_API int fx_wait(fx_context *ctx, int64_t ticket, int64_t timeout_ns, fx_counters *counters) {
+    if (!ctx) return FX_ERR_INVALID_ARGUMENT;
+    return wait_ticket(ctx, ticket, timeout_ns, counters, nullptr);
+}
+
+FX_API int fx_fetch(fx_context *ctx, int64_t ticket, int64_t timeout_ns, uint16_t *rgb_out,
+                    fx_counters *counters, float *score_out, uint8_t *at_floor_out,
+                    uint8_t *changed_out) {
+    if (!ctx) return FX_ERR_INVALID_ARGUMENT;
+    const FetchTargets fetch{rgb_out, score_out, at_floor_out, changed_out};
+    return wait_ticket(ctx, ticket, timeout_ns, counters, &fetch);
+}
+
+FX_API int fx_set_walk_window(fx_context *ctx, double sigmas) {
+    if (!ctx || !(sigmas >= 0.0) || sigmas > 64.0) return FX_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    ctx->walk_sigmas = sigmas;
+    return FX_OK;
+}
+
+FX_API int fx_set_list_capacity(fx_context *ctx, int64_t channels) {
+    if (!ctx || channels < 0 || channels > ((int64_t)1 << 31)) return FX_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    ctx->list_capacity = channels;
+    return FX_OK;
 }
 
 FX_API int fx_profile_enable(fx_context *ctx, int enable) {

@@ -26,6 +26,15 @@ __device__ __forceinline__ void raise_error(uint32_t *err, uint32_t code) {
     if (*reinterpret_cast<volatile uint32_t *>(err) == 0) atomicCAS(err, 0u, code);
 }
 
+// A pass's error block is four words: err[0] the status, err[1] the stop
+// word.  Only the stage gates (k_gate, between kernel groups on the pass's
+// stream) write the stop word, so it is constant while any other kernel of
+// the pass runs and every thread of a kernel sees the same value: a kernel
+// that finds it set returns before its first barrier, all its blocks alike.
+__device__ __forceinline__ bool pass_stopped(const uint32_t *err) {
+    return err[1] != 0u;
+}
+
 // ---------------------------------------------------------------------------
 // Frame geometry and buffers
 // ---------------------------------------------------------------------------
@@ -163,6 +172,8 @@ struct WriterBuffers {
     void *walk_scratch;            // walk_scratch_bytes(capacity, per_wave)
     int per_wave;                  // window blocks per wave (walk_per_wave of the SM count)
     bool parallel_walk;
+    double window_sigmas;          // walk window half-width in standard deviations
+    const uint32_t *cancel;        // host-mapped cancel word read by the stage gates, or null
 };
 
 // Optional CUDA events between kernel groups (measurement only).
@@ -193,10 +204,16 @@ size_t dev_counters_bytes();
 cudaError_t walk_init();
 size_t walk_scratch_bytes(int64_t capacity, int per_wave);
 int walk_per_wave(int sms);
+constexpr double kDefaultWindowSigmas = 4.5;
 cudaError_t launch_walk(const AmbEntry *entries, const uint32_t *pos, const uint32_t *n_ptr,
                         int64_t capacity, uint32_t s0, void *scratch, int per_wave,
-                        bool parallel, uint32_t *extra_after, uint32_t *fallbacks_out,
-                        unsigned long long *stats_out, cudaStream_t stream);
+                        bool parallel, double window_sigmas, uint32_t *extra_after,
+                        uint32_t *fallbacks_out, unsigned long long *stats_out,
+                        const uint32_t *err, cudaStream_t stream);
+// Stage gate: when *cancel (host-mapped) is set, stop the pass: err[1] = 1
+// and err[0] = FX_ERR_CANCELLED unless an error came first.  No launch when
+// `cancel` is null.
+cudaError_t launch_gate(const uint32_t *cancel, uint32_t *err, cudaStream_t stream);
 void counters_to_host(const void *dev_copy, fx_counters *out);
 uint32_t counters_n_amb(const void *dev_copy);
 size_t producer_bytes(int h, int w);
@@ -213,5 +230,7 @@ int context_device(const fx_context *ctx);
 const float *context_lut(const fx_context *ctx);
 int context_fail(fx_context *ctx, int code, const char *fmt, ...);
 int context_device_error(fx_context *ctx, uint32_t code);
+void context_lock(fx_context *ctx);  // the context's call lock (fx_set_tables holds it)
+void context_unlock(fx_context *ctx);
 
 }  // namespace fx

@@ -10,9 +10,12 @@
 // this file is loaded, and the call itself makes no cudaMalloc, cudaFree or
 // other allocating call.
 //
-// The array lives in this translation unit alone so it is only reserved in
-// processes that use this entry point (the runtime loads a module lazily,
-// the first time one of its symbols is used).
+// When the array is reserved depends on how the CUDA runtime loads modules.
+// Under lazy loading (CUDA_MODULE_LOADING=LAZY, the default since CUDA 12.2)
+// the module is loaded, and the 24 MiB reserved, by the first
+// cudaGetSymbolAddress of this entry point, so only processes that call it
+// pay for it.  Under CUDA_MODULE_LOADING=EAGER every context of the process
+// reserves it when the context is created.
 #include <cstring>
 #include <mutex>
 
@@ -35,6 +38,28 @@ static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBy
 static void *g_static_ptr[kStaticMaxDevices];
 static std::mutex g_static_mu[kStaticMaxDevices];
 
+// Holds the context's call lock for the whole call, so fx_set_tables cannot
+// rewrite the LUT while this call's kernels read it and no other call on the
+// context overwrites its error text; restores the caller's current device.
+class StaticCallScope {
+  public:
+    explicit StaticCallScope(fx_context *ctx) : ctx_(ctx) {
+        context_lock(ctx_);
+        restore_ = cudaGetDevice(&saved_) == cudaSuccess;
+    }
+    ~StaticCallScope() {
+        if (restore_) cudaSetDevice(saved_);
+        context_unlock(ctx_);
+    }
+    StaticCallScope(const StaticCallScope &) = delete;
+    StaticCallScope &operator=(const StaticCallScope &) = delete;
+
+  private:
+    fx_context *ctx_;
+    int saved_ = 0;
+    bool restore_ = false;
+};
+
 }  // namespace fx
 
 using namespace fx;
@@ -43,6 +68,8 @@ FX_API int fx_producer_rows_static(fx_context *ctx, const uint16_t *d_main_rgbi,
                                    int32_t w, float *d_rows, fx_stage *d_stages, void *stream) {
     if (!ctx || !d_main_rgbi || !d_rows || !d_stages || h < 1 || w < 8)
         return FX_ERR_INVALID_ARGUMENT;
+    // lock order: the context's lock, then the device's scratch lock
+    StaticCallScope scope(ctx);
     const int device = context_device(ctx);
     if (device < 0 || device >= kStaticMaxDevices)
         return context_fail(ctx, FX_ERR_INVALID_ARGUMENT, "device index outside the static table");
@@ -67,6 +94,11 @@ FX_API int fx_producer_rows_static(fx_context *ctx, const uint16_t *d_main_rgbi,
         e = cudaGetSymbolAddress(&p, g_static_scratch);
         if (e != cudaSuccess || !p) {
             cudaGetLastError();
+            if (e == cudaErrorMemoryAllocation)
+                return context_fail(ctx, FX_ERR_OUT_OF_MEMORY,
+                                    "the device has no room for the %zu MiB static producer "
+                                    "scratch (reserved when the module loads)",
+                                    kStaticScratchBytes >> 20);
             return context_fail(ctx, FX_ERR_CUDA, "cudaGetSymbolAddress failed: %s",
                                 cudaGetErrorString(e));
         }

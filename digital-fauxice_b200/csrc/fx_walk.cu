@@ -35,17 +35,17 @@ constexpr int kWinRing = 3;                         // staged chunks in flight
 constexpr uint32_t kCompactEvery = 512;             // block compaction period (steady state)
 constexpr uint32_t kNone = 0xFFFFFFFFu;
 constexpr uint32_t kSerialBelow = 4 * kSegLen;      // short chains: one serial walk
-// Window half-width in standard deviations of the predicted entry count.  A
-// count outside its window costs one exact serial walk of that segment
-// (about 40 us) and never changes a result; at 4.5 sigma that happens for
-// about 7e-6 of the segments.
-constexpr double kWindowSigmas = 4.5;
+// The window half-width is kDefaultWindowSigmas (4.5) standard deviations of
+// the predicted entry count, plus 16.  A count outside its window costs one
+// exact serial walk of that segment (about 40 us) and never changes a
+// result; at 4.5 sigma that happens for about 7e-6 of the segments.
+// fx_set_walk_window narrows it, so tests can force such misses.
 
 struct WalkState {
     uint32_t e_wave;     // exact E at the start of the current wave
-    uint32_t fallbacks;  // segments resolved by an exact serial walk
     uint32_t waves;
-    uint32_t pad;
+    uint32_t fallbacks;  // segments resolved by an exact serial walk
+    uint32_t packed;     // segments whose settled phase ran two candidates per lane
     unsigned long long candidate_steps;  // window-walk work, for diagnostics
     unsigned long long window_sum;       // candidates started
     unsigned long long survivor_sum;     // candidates left at segment ends
@@ -91,8 +91,9 @@ __device__ __forceinline__ uint4 intervals(const AmbEntry &e) {
 // probability p).
 __global__ void k_seg_prob(const AmbEntry *__restrict__ entries, const uint32_t *__restrict__ n_ptr,
                            int64_t capacity, double *__restrict__ seg_mu,
-                           double *__restrict__ seg_var) {
+                           double *__restrict__ seg_var, const uint32_t *__restrict__ err) {
     __shared__ double s_mu[8], s_var[8];
+    if (pass_stopped(err)) return;
     const uint32_t n = (uint32_t)min((int64_t)*n_ptr, capacity);
     const uint32_t i0 = blockIdx.x * kSegLen;
     if (i0 >= n) return;
@@ -324,9 +325,11 @@ __global__ void __launch_bounds__(kWinThreads, kWinBlocksPerSM)
              const double *__restrict__ seg_mu, const double *__restrict__ seg_var,
              const WalkState *__restrict__ st, uint32_t wave, uint32_t per_wave, uint32_t t0,
              SegWindow *__restrict__ windows, uint32_t *__restrict__ table,
-             SegList *__restrict__ lists, WalkState *stats, uint32_t serial_below) {
+             SegList *__restrict__ lists, WalkState *stats, uint32_t serial_below,
+             double sigmas, const uint32_t *__restrict__ err) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     WindowSmem &S = *reinterpret_cast<WindowSmem *>(smem_raw);
+    if (pass_stopped(err)) return;
     const uint32_t n = (uint32_t)min((int64_t)*n_ptr, capacity);
     if (n < serial_below) return;  // the chain is walked serially instead
     const uint32_t seg0 = wave * per_wave;
@@ -356,7 +359,7 @@ __global__ void __launch_bounds__(kWinThreads, kWinBlocksPerSM)
     __syncthreads();
     const uint32_t e0 = st->e_wave;
     const uint32_t before = i0 - seg0 * kSegLen;  // channels since the wave start
-    const double half = kWindowSigmas * sqrt(S.pred[1]) + 16.0;
+    const double half = sigmas * sqrt(S.pred[1]) + 16.0;
     const double center = S.pred[0];
     int64_t lo = (int64_t)floor(center - half), hi = (int64_t)ceil(center + half);
     lo = lo < 0 ? 0 : lo;
@@ -507,6 +510,7 @@ __global__ void __launch_bounds__(kWinThreads, kWinBlocksPerSM)
     };
 
     uint32_t steps = 0;
+    bool packed = false;  // the settled phase ran two candidates per lane
     // Three staged chunks: chunk c+2 is fetched into the buffer of chunk c-1
     // right after the barrier that ends every warp's work on chunk c-1.
     stage(i0, 0);
@@ -558,6 +562,7 @@ __global__ void __launch_bounds__(kWinThreads, kWinBlocksPerSM)
             if (done >= next_compact || c0 + r == iw) {
                 merge_and_compact(slots);
                 slots = window_slots(live);
+                packed |= live <= (uint32_t)kWinThreads && slots == 2;
                 next_compact = live <= (uint32_t)kWinThreads ? (iw - i0)
                                                              : min(2 * next_compact, done + kCompactEvery);
             }
@@ -604,6 +609,7 @@ __global__ void __launch_bounds__(kWinThreads, kWinBlocksPerSM)
         list->count = (live <= (uint32_t)kListMax) ? live : 0xFFFFu;
         atomicAdd(&stats->window_sum, (unsigned long long)count);
         atomicAdd(&stats->survivor_sum, (unsigned long long)live);
+        if (packed) atomicAdd(&stats->packed, 1u);
     }
     for (int o = 16; o > 0; o >>= 1) steps += __shfl_down_sync(0xFFFFFFFFu, steps, o);
     if ((tid & 31) == 0 && steps) atomicAdd(&stats->candidate_steps, (unsigned long long)steps);
@@ -658,9 +664,10 @@ __global__ void __launch_bounds__(kResolveThreads)
               uint32_t wave, uint32_t per_wave, uint32_t t0,
               const SegWindow *__restrict__ windows, const uint32_t *__restrict__ table,
               const SegList *__restrict__ lists, uint32_t *__restrict__ e_in_exact,
-              uint32_t serial_below) {
+              uint32_t serial_below, const uint32_t *__restrict__ err) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ResolveSmem &S = *reinterpret_cast<ResolveSmem *>(smem_raw);
+    if (pass_stopped(err)) return;
     const uint32_t n = (uint32_t)min((int64_t)*n_ptr, capacity);
     if (n < serial_below) return;
     const uint32_t segs = (n + kSegLen - 1) / kSegLen;
@@ -782,9 +789,11 @@ __global__ void __launch_bounds__(kRewalkWarps * 32)
     k_rewalk(const AmbEntry *__restrict__ entries, const uint32_t *__restrict__ pos,
              const uint32_t *__restrict__ n_ptr, int64_t capacity, uint32_t parallel_seg_len,
              const uint32_t *__restrict__ e_in_exact, uint32_t t0,
-             uint32_t *__restrict__ extra_after, uint32_t serial_below) {
+             uint32_t *__restrict__ extra_after, uint32_t serial_below,
+             const uint32_t *__restrict__ err) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     RewalkSmem &S = *reinterpret_cast<RewalkSmem *>(smem_raw);
+    if (pass_stopped(err)) return;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t n = (uint32_t)min((int64_t)*n_ptr, capacity);
     // a short chain (or the serial mode) is one segment walked from E = 0
@@ -927,8 +936,9 @@ cudaError_t walk_init() {
 // warp instead of the speculative windows.
 cudaError_t launch_walk(const AmbEntry *entries, const uint32_t *pos, const uint32_t *n_ptr,
                         int64_t capacity, uint32_t s0, void *scratch, int per_wave,
-                        bool parallel, uint32_t *extra_after, uint32_t *fallbacks_out,
-                        unsigned long long *stats_out, cudaStream_t stream) {
+                        bool parallel, double window_sigmas, uint32_t *extra_after,
+                        uint32_t *fallbacks_out, unsigned long long *stats_out,
+                        const uint32_t *err, cudaStream_t stream) {
     const int64_t segs_max = walk_max_segments(capacity);
     char *p = reinterpret_cast<char *>(scratch);
     auto take = [&](size_t bytes) {
@@ -949,24 +959,25 @@ cudaError_t launch_walk(const AmbEntry *entries, const uint32_t *pos, const uint
     const uint32_t segs = (uint32_t)segs_max;
     if (parallel) {
         const uint32_t waves = (segs + per_wave - 1) / per_wave;
-        k_seg_prob<<<segs, 256, 0, stream>>>(entries, n_ptr, capacity, mu, var);
+        k_seg_prob<<<segs, 256, 0, stream>>>(entries, n_ptr, capacity, mu, var, err);
         for (uint32_t w = 0; w < waves; ++w) {
             const uint32_t blocks = min((uint32_t)per_wave, segs - w * per_wave);
             k_window<<<blocks, kWinThreads, sizeof(WindowSmem), stream>>>(
                 entries, pos, n_ptr, capacity, mu, var, st, w, per_wave, t0, windows, table,
-                lists, st, serial_below);
+                lists, st, serial_below, window_sigmas, err);
             k_resolve<<<1, kResolveThreads, resolve_smem_bytes(), stream>>>(
                 entries, pos, n_ptr, capacity, st, w, per_wave, t0, windows, table, lists, e_in,
-                serial_below);
+                serial_below, err);
         }
     }
     constexpr uint32_t kRewalkPerBlock = kRewalkWarps * kRewalkLanes;
     k_rewalk<<<(segs + kRewalkPerBlock - 1) / kRewalkPerBlock, kRewalkWarps * 32, sizeof(RewalkSmem),
                stream>>>(entries, pos, n_ptr, capacity, kSegLen, e_in, t0, extra_after,
-                         serial_below);
+                         serial_below, err);
+    // fallbacks_out[0] = segments walked exactly, fallbacks_out[1] = packed segments
     if (fallbacks_out)
-        cudaMemcpyAsync(fallbacks_out, &st->fallbacks, sizeof(uint32_t), cudaMemcpyDeviceToDevice,
-                        stream);
+        cudaMemcpyAsync(fallbacks_out, &st->fallbacks, 2 * sizeof(uint32_t),
+                        cudaMemcpyDeviceToDevice, stream);
     if (stats_out)
         cudaMemcpyAsync(stats_out, &st->candidate_steps, 3 * sizeof(unsigned long long),
                         cudaMemcpyDeviceToDevice, stream);

@@ -36,6 +36,7 @@ struct DevCounters {
     uint32_t startup_base, startup_amb, startup_extra;
     uint32_t n_amb;
     uint32_t walk_fallbacks;
+    uint32_t walk_packed;              // written together with walk_fallbacks
     unsigned long long walk_stats[3];  // candidate steps, window sum, survivor sum
     uint32_t su_base[6], su_amb[6];    // per startup row, for the last block's prefix
     uint32_t su_done;                  // startup rows summed
@@ -113,8 +114,10 @@ __device__ __forceinline__ void load_meta(const uint8_t *meta, int64_t first, in
 }
 
 __global__ void k_seg_sums(const uint8_t *__restrict__ meta, int64_t sites,
-                           uint32_t *__restrict__ seg_base, uint32_t *__restrict__ seg_amb) {
+                           uint32_t *__restrict__ seg_base, uint32_t *__restrict__ seg_amb,
+                           const uint32_t *__restrict__ err) {
     __shared__ uint32_t scratch[kSegThreads / 32];
+    if (pass_stopped(err)) return;
     const int64_t first = (int64_t)blockIdx.x * kSegment + threadIdx.x * kPer;
     uint8_t m[kPer];
     load_meta(meta, first, sites, m);
@@ -130,8 +133,9 @@ __global__ void k_seg_sums(const uint8_t *__restrict__ meta, int64_t sites,
 
 // Exclusive scan of the per-segment sums; entry [n] holds the totals.
 __global__ void k_seg_scan(uint32_t *__restrict__ seg_base, uint32_t *__restrict__ seg_amb,
-                           int64_t n) {
+                           int64_t n, const uint32_t *__restrict__ err) {
     __shared__ uint32_t ws[32];
+    if (pass_stopped(err)) return;
     uint32_t carry_b = 0, carry_a = 0;
     for (int64_t base = 0; base < n; base += 1024) {
         const int64_t i = base + threadIdx.x;
@@ -319,8 +323,9 @@ __device__ void copy_intervals(const ChannelView &cv, AmbEntry &e, uint32_t *err
 __global__ void __launch_bounds__(kSegThreads)
     k_amb(const uint8_t *__restrict__ meta, int64_t sites, const uint32_t *__restrict__ seg_base,
           const uint32_t *__restrict__ seg_amb, uint32_t *__restrict__ site_of,
-          uint32_t *__restrict__ pos_out, int64_t capacity) {
+          uint32_t *__restrict__ pos_out, int64_t capacity, const uint32_t *__restrict__ err) {
     __shared__ uint32_t ws[kSegThreads / 32];
+    if (pass_stopped(err)) return;
     const int64_t first = (int64_t)blockIdx.x * kSegment + threadIdx.x * kPer;
     uint8_t m[kPer];
     load_meta(meta, first, sites, m);
@@ -357,6 +362,7 @@ __global__ void k_coef(AmbEntry *__restrict__ entries, const uint32_t *__restric
                        const uint32_t *__restrict__ site_of, const uint8_t *__restrict__ meta,
                        const double *__restrict__ cand, int w, const uint16_t *__restrict__ rgbi,
                        const float *__restrict__ lut, fx_params p, uint32_t *err) {
+    if (pass_stopped(err)) return;
     const uint32_t n = (uint32_t)min((int64_t)*n_amb_ptr, capacity);
     const DitherConst dc = dither_const(p);
     const int64_t su = 6 * (int64_t)w;
@@ -409,9 +415,11 @@ __global__ void k_coef(AmbEntry *__restrict__ entries, const uint32_t *__restric
 // at the row's ends).
 __global__ void k_startup_counts(const uint8_t *__restrict__ meta, int w,
                                  const uint32_t *__restrict__ extra_after, uint32_t s0,
-                                 DevCounters *ctr, int64_t capacity) {
+                                 DevCounters *ctr, int64_t capacity,
+                                 const uint32_t *__restrict__ err) {
     __shared__ unsigned long long scratch[8];
     __shared__ bool last;
+    if (pass_stopped(err)) return;
     const int k = blockIdx.x;  // startup row 0..5
     unsigned long long att = 0, base = 0, amb = 0;
     for (int x = threadIdx.x; x < w; x += blockDim.x) {
@@ -532,6 +540,7 @@ __global__ void __launch_bounds__(kSegThreads, 5)
     __shared__ unsigned long long s_sums[kSegThreads / 32][4];
     __shared__ Affine s_jump[kJumpDigits][64];
     __shared__ uint32_t s_ref[kSegment], s_p[kSegment], s_a[kSegment];
+    if (pass_stopped(err)) return;  // cancelled: the output stays untouched
     for (int i = threadIdx.x; i < 256; i += kSegThreads) {
         hi[i] = g_high[i];
         lo[i] = g_low[i];
@@ -680,6 +689,7 @@ __global__ void __launch_bounds__(kSegThreads, 5)
 __global__ void k_final(const uint32_t *__restrict__ seg_base, const uint32_t *__restrict__ seg_amb,
                         int64_t segments, const uint32_t *__restrict__ extra_after, uint32_t s0,
                         DevCounters *ctr, uint32_t *err, int64_t capacity) {
+    if (pass_stopped(err)) return;
     const uint32_t p_total = seg_base[segments];
     const uint32_t a_total = seg_amb[segments];
     const uint32_t e_total = extra_before(extra_after, a_total, capacity);
@@ -705,28 +715,49 @@ cudaError_t launch_writer(const Geometry &g, const uint8_t *meta, const double *
     const int64_t segs = g.segments;
     DevCounters *ctr = reinterpret_cast<DevCounters *>(b.counters);
     cudaMemsetAsync(ctr, 0, sizeof(DevCounters), stream);
-    k_seg_sums<<<(unsigned)segs, kSegThreads, 0, stream>>>(meta, g.sites, b.seg_base, b.seg_amb);
-    k_seg_scan<<<1, 1024, 0, stream>>>(b.seg_base, b.seg_amb, segs);
+    cudaError_t e = launch_gate(b.cancel, err, stream);
+    if (e != cudaSuccess) return e;
+    k_seg_sums<<<(unsigned)segs, kSegThreads, 0, stream>>>(meta, g.sites, b.seg_base, b.seg_amb,
+                                                           err);
+    k_seg_scan<<<1, 1024, 0, stream>>>(b.seg_base, b.seg_amb, segs, err);
     // the site list lives in extra_after until the walk writes the counts
     k_amb<<<(unsigned)segs, kSegThreads, 0, stream>>>(meta, g.sites, b.seg_base, b.seg_amb,
-                                                      b.extra_after, b.pos, b.capacity);
+                                                      b.extra_after, b.pos, b.capacity, err);
     const uint32_t *n_amb = b.seg_amb + segs;
     k_coef<<<1184, 256, 0, stream>>>(b.entries, b.pos, n_amb, b.capacity, b.extra_after, meta,
                                      cand, g.w, rgbi, lut, p, err);
     marks.mark(5, stream);
-    cudaError_t e = launch_walk(b.entries, b.pos, n_amb, b.capacity, s0, b.walk_scratch,
-                                b.per_wave, b.parallel_walk, b.extra_after, &ctr->walk_fallbacks,
-                                ctr->walk_stats, stream);
+    e = launch_gate(b.cancel, err, stream);
+    if (e != cudaSuccess) return e;
+    e = launch_walk(b.entries, b.pos, n_amb, b.capacity, s0, b.walk_scratch, b.per_wave,
+                    b.parallel_walk, b.window_sigmas, b.extra_after, &ctr->walk_fallbacks,
+                    ctr->walk_stats, err, stream);
     if (e != cudaSuccess) return e;
     marks.mark(6, stream);
+    e = launch_gate(b.cancel, err, stream);
+    if (e != cudaSuccess) return e;
     k_startup_counts<<<6, 256, 0, stream>>>(meta, g.w, b.extra_after, s0 & kLcgMask, ctr,
-                                            b.capacity);
+                                            b.capacity, err);
     k_apply<<<(unsigned)segs, kSegThreads, 0, stream>>>(
         meta, cand, g.sites, g.w, rgbi, lut, high, low, ident, stages, p, b.seg_base, b.seg_amb,
         b.extra_after, s0 & kLcgMask, rgb_out, changed_out, ctr, err, b.capacity);
     k_final<<<1, 1, 0, stream>>>(b.seg_base, b.seg_amb, segs, b.extra_after, s0 & kLcgMask,
                                  ctr, err, b.capacity);
     marks.mark(7, stream);
+    return cudaGetLastError();
+}
+
+// One thread: a cancel request seen here stops every later kernel of the pass.
+__global__ void k_gate(const volatile uint32_t *cancel, uint32_t *err) {
+    if (*cancel && err[1] == 0u) {
+        err[1] = 1u;
+        atomicCAS(err, 0u, (uint32_t)FX_ERR_CANCELLED);
+    }
+}
+
+cudaError_t launch_gate(const uint32_t *cancel, uint32_t *err, cudaStream_t stream) {
+    if (!cancel) return cudaSuccess;
+    k_gate<<<1, 1, 0, stream>>>(cancel, err);
     return cudaGetLastError();
 }
 
@@ -749,6 +780,7 @@ void counters_to_host(const void *dev_copy, fx_counters *out) {
     out->walk_candidate_steps = (int64_t)c.walk_stats[0];
     out->walk_candidates = (int64_t)c.walk_stats[1];
     out->walk_survivors = (int64_t)c.walk_stats[2];
+    out->walk_packed_segments = (int64_t)c.walk_packed;
 }
 
 uint32_t counters_n_amb(const void *dev_copy) {

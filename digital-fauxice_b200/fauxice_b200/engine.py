@@ -243,6 +243,65 @@ def run_frame(ctx: _lib.Context, main: np.ndarray, params: _lib.FxParams,
     return FrameOutcome(out, counters, score, changed, digest)
 
 
+_CANCEL_POLL_S = 0.0005  # how often a running pass checks the cancellation callback
+
+
+def run_frame_cancellable(ctx: _lib.Context, main: np.ndarray, params: _lib.FxParams,
+                          stages: np.ndarray | None, rng_state: int, diagnostics: bool,
+                          cancelled: CancellationCallback) -> FrameOutcome:
+    """One frame through fx_submit / fx_fetch, polling ``cancelled`` while
+    the device works.
+
+    The reference polls its callback between phases (engine.py:103-106); here
+    the pass itself is the long phase, so the callback is polled while it
+    runs and a True answer is handed to the device with fx_cancel: the pass
+    stops at its next stage boundary, and nothing is copied to the caller.
+    """
+
+    import ctypes
+
+    px = np.ascontiguousarray(main, dtype=np.uint16)
+    h, w = px.shape[:2]
+    if stages is not None:
+        stages = np.ascontiguousarray(stages, dtype=_lib.STAGE_DTYPE)
+        if stages.shape != (h + 6,):
+            raise ValueError("stage table must hold height + 6 entries")
+    # rgb_out NULL: the results stay staged in the library until fx_fetch
+    frame = _lib.FxFrame(
+        main_rgbi=px.ctypes.data, height=h, width=w, params=ctypes.pointer(params),
+        stages=stages.ctypes.data if stages is not None else None,
+        rng_state=int(rng_state) & 0xFFFFFF, rgb_out=None, score_out=None, changed_out=None)
+    lib = _lib.load()
+
+    def check(status: int) -> None:
+        if status:
+            try:
+                ctx.check(status)
+            except _lib.LibraryError as error:
+                raise_library_error(error)
+
+    with ctx.lock:
+        ticket = ctypes.c_int64()
+        check(lib.fx_submit(ctx.handle, ctypes.byref(frame), ctypes.byref(ticket)))
+        while True:
+            status = lib.fx_poll(ctx.handle, ticket.value)
+            if status != _lib.FX_PENDING:
+                break
+            if cancelled():
+                lib.fx_cancel(ctx.handle, ticket.value)
+                # releases the slot; the staged results are dropped
+                lib.fx_fetch(ctx.handle, ticket.value, -1, None, None, None, None, None)
+                raise ProcessingCancelled("portable correction was cancelled")
+            time.sleep(_CANCEL_POLL_S)
+        out = np.empty((h, w, 3), np.uint16)
+        score = np.empty((h, w), np.float32) if diagnostics else None
+        changed = np.empty((h, w), np.uint8) if diagnostics else None
+        counters = _lib.FxCounters()
+        check(lib.fx_fetch(ctx.handle, ticket.value, -1, _lib.ptr(out), ctypes.byref(counters),
+                           _lib.ptr(score), None, _lib.ptr(changed)))
+    return FrameOutcome(out, counters, score, changed)
+
+
 def replay_result(outcome: FrameOutcome) -> StreamingReplayResult:
     c = outcome.counters
     h, w = outcome.output.shape[:2]
@@ -328,8 +387,12 @@ def process_b200(
     height = int(main_pixels.shape[0])
     _notify(progress, ProcessingPhase.RECONSTRUCTION, 0, height)
     params = DEFAULT_PROFILE.hot_path_parameters().to_c()
-    outcome = run_frame(ctx, main_pixels, params, None, NIKON_PE_INITIAL_STATE,
-                        export_diagnostics)
+    if cancelled is None:
+        outcome = run_frame(ctx, main_pixels, params, None, NIKON_PE_INITIAL_STATE,
+                            export_diagnostics)
+    else:
+        outcome = run_frame_cancellable(ctx, main_pixels, params, None, NIKON_PE_INITIAL_STATE,
+                                        export_diagnostics, cancelled)
     replay = replay_result(outcome)
     _notify(progress, ProcessingPhase.RECONSTRUCTION, height, height, replay.attempted_pixels,
             replay.written_pixels)

@@ -44,10 +44,15 @@ SMALL_CROP = DefectSpec(discs=40, disc_radius=(2, 12), scratches=6, scratch_leng
 # Native frame: ~3000 discs r~U[1,20], 60 scratches of length U[50,2000] (~0.5%).
 NATIVE_FRAME = DefectSpec(discs=3000, disc_radius=(1, 20), scratches=60,
                           scratch_length=(50, 2000))
-# Heavy damage: 5% coverage incl. 200 blobs r~U[20,60] whose IR keeps only
-# 1-10% (scores saturate at the floor) plus dense crossing scratches.
+# Dense damage for small stress frames: about 27% of a full frame's pixels,
+# with floor-saturating blobs, many discs and long scratches.
 HEAVY_FRAME = DefectSpec(discs=9000, disc_radius=(1, 20), scratches=600,
                          scratch_length=(200, 4000), blobs=200)
+# Heavy damage at full size: about 5% of the pixels, most of it 200 blobs of
+# radius U[20,60] whose IR keeps only 1-10% (scores saturate at the floor),
+# plus long crossing scratches and some discs.
+HEAVY_FULL = DefectSpec(discs=120, disc_radius=(1, 20), scratches=40,
+                        scratch_length=(1000, 4000), blobs=200)
 
 
 def scaled_spec(spec: DefectSpec, height: int, width: int) -> DefectSpec:
@@ -191,6 +196,14 @@ def heavy_frame(seed: int, *, height: int = FULL_FRAME[0],
     """Heavy-damage frame (~5% coverage with floor-saturating blobs)."""
 
     main = make_frame(seed, height, width, scaled_spec(HEAVY_FRAME, height, width))
+    return main, make_prepass(main)
+
+
+def heavy_full_frame(index: int, base_seed: int = 200) -> tuple[np.ndarray, np.ndarray]:
+    """Frame ``index`` of the heavy-damage batch: a full 5782x3946 frame at
+    about 5% coverage (HEAVY_FULL), seed base+index."""
+
+    main = make_frame(base_seed + index, FULL_FRAME[0], FULL_FRAME[1], HEAVY_FULL)
     return main, make_prepass(main)
 
 

@@ -98,6 +98,8 @@ typedef struct fx_counters {
                                (no reference counterpart) */
     int64_t walk_fallbacks; /* walk segments resolved by the exact serial path */
     int64_t walk_candidate_steps, walk_candidates, walk_survivors; /* walk work */
+    int64_t walk_packed_segments; /* segments whose settled phase ran two
+                                     candidates per lane (walk diagnostics) */
 } fx_counters;
 
 /* One frame for fx_process / fx_submit.  Host pointers. */
@@ -162,7 +164,11 @@ FX_API int fx_producer_rows(fx_context *ctx, const uint16_t *main_rgbi, int32_t 
  * `stream` (a cudaStream_t, NULL for the legacy default stream) and the call
  * returns after it finishes.  The scratch is shared by all calls on one
  * device, so calls are serialized; the first call on a device reserves the
- * array and should come before any stream capture. */
+ * array (under the CUDA runtime's default lazy module loading; with
+ * CUDA_MODULE_LOADING=EAGER every context reserves it at creation) and
+ * should come before any stream capture.  FX_ERR_OUT_OF_MEMORY when the
+ * device has no room left for the array.  The call holds the context's lock
+ * and leaves the caller's current device as it found it. */
 FX_API int fx_producer_rows_static(fx_context *ctx, const uint16_t *d_main_rgbi, int32_t height,
                                    int32_t width, float *d_rows, fx_stage *d_stages, void *stream);
 
@@ -216,6 +222,10 @@ FX_API int fx_output_digest(fx_context *ctx, uint8_t *digest32);
  * fx_set_slots and before submitting.  FX_ERR_OUT_OF_MEMORY when the device
  * cannot hold them. */
 FX_API int fx_reserve_frames(fx_context *ctx, int32_t max_height, int32_t max_width);
+/* Submit a host-buffer frame.  A frame with rgb_out NULL keeps its results
+ * (RGB16 output, score plane, changed mask) staged in pinned memory until
+ * fx_fetch; otherwise fx_wait copies them into the frame's own buffers.
+ * FX_PENDING when every slot is busy. */
 FX_API int fx_submit(fx_context *ctx, const fx_frame *frame, int64_t *ticket);
 /* fx_submit for a frame already in device memory: the pass is enqueued on
  * a free slot's stream and writes d_rgb_out / d_score_out / d_changed_out
@@ -228,6 +238,39 @@ FX_API int fx_submit_device(fx_context *ctx, const uint16_t *d_rgbi, int32_t hei
                             uint8_t *d_changed_out, int64_t *ticket);
 FX_API int fx_poll(fx_context *ctx, int64_t ticket);
 FX_API int fx_wait(fx_context *ctx, int64_t ticket, int64_t timeout_ns, fx_counters *counters);
+/* Cooperative cancellation of a request in flight, the device-side form of
+ * the `cancelled` callback the reference polls between phases
+ * (engine.py:103-106, checked by tests/test_engine.py:46-73).  Sets the
+ * request's cancel word; the pass reads it at its next stage boundary
+ * (after the producer, the analysis, the chain scan and the walk) and every
+ * later kernel returns at once, so a device output buffer is left untouched
+ * unless the last boundary had already passed.  fx_wait / fx_fetch then
+ * return FX_ERR_CANCELLED (or FX_OK when the pass had already finished) and
+ * release the slot; host buffers are written only on FX_OK. */
+FX_API int fx_cancel(fx_context *ctx, int64_t ticket);
+/* fx_wait for an fx_submit ticket that delivers the results into the
+ * buffers given here, any of which may be NULL: the RGB16 output, the
+ * counters, the score plane, the at-floor mask (score == the profile's
+ * score floor, engine.py:175-199) and the changed mask.  The planes must
+ * have been staged (a frame submitted with rgb_out NULL stages all of
+ * them); FX_ERR_INVALID_ARGUMENT otherwise, or for a device-buffer ticket. */
+FX_API int fx_fetch(fx_context *ctx, int64_t ticket, int64_t timeout_ns, uint16_t *rgb_out,
+                    fx_counters *counters, float *score_out, uint8_t *at_floor_out,
+                    uint8_t *changed_out);
+
+/* Test knobs, no reference counterpart.  Neither changes a result, only
+ * which code path produces it; both exist so the tests can drive the rare
+ * paths of the writer.
+ * fx_set_walk_window: half-width of the speculative walk's candidate
+ * windows in standard deviations of the predicted count (default 4.5, plus
+ * 16 candidates).  Narrow windows make entry counts fall outside them, so
+ * the affected segments are walked by the exact serial fallback
+ * (fx_counters.walk_fallbacks counts them).
+ * fx_set_list_capacity: entries of the RNG-dependent channel list each pass
+ * reserves (0, the default: half the frame's chain sites).  A frame with
+ * more such channels reruns with room for all of them. */
+FX_API int fx_set_walk_window(fx_context *ctx, double sigmas);
+FX_API int fx_set_list_capacity(fx_context *ctx, int64_t channels);
 
 /* Device time per pipeline stage, from CUDA events recorded on the frame's
  * stream between kernel groups (measurement only; no reference

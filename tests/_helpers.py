@@ -12,7 +12,8 @@ from fauxice_b200 import contracts
 from fauxice_b200 import streaming as b200_streaming
 
 # Golden job cases cheap enough for the CPU oracle in the default suite.
-SLOW_JOBS = {"native_full", "batch_0", "batch_1", "batch_2", "batch_3", "batch_4"}
+SLOW_JOBS = {"native_full", "batch_0", "batch_1", "batch_2", "batch_3", "batch_4",
+             "heavy_full_0", "heavy_full_1"}
 
 
 def sha(array: np.ndarray) -> str:

@@ -212,6 +212,9 @@ JOB_CASES = {
     "heavy_1024": ((lambda: generated(201, 1024, 1024, "heavy")), "cpu-fast"),
     "native_full": ((lambda: synthetic.native_frame(2)), "cpu-fast"),
     **{f"batch_{i}": ((lambda i=i: synthetic.batch_frame(i)), "cpu-fast") for i in range(5)},
+    # heavy-damage full frames (about 5% coverage, 200 floor-saturating blobs)
+    **{f"heavy_full_{i}": ((lambda i=i: synthetic.heavy_full_frame(i)), "cpu-fast")
+       for i in range(2)},
 }
 
 # Streaming-replay cases with explicit parameters

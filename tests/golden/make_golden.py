@@ -2,7 +2,8 @@
 """Generate tests/golden/reference_results.json by running the reference.
 
 This script imports the reference package portable_digital_ice from
-``--reference`` (default /root/reference/src) and records, for every case in
+``--reference`` (or the FAUXICE_REFERENCE_SRC environment variable: the
+reference checkout's ``src`` directory) and records, for every case in
 cases.py, the reference's output digest, replay counters, startup receipt,
 diagnostics digests and prelude records.  It is run once, in a container
 where the reference is importable; the tests then need only the JSON file.
@@ -33,10 +34,13 @@ def sha(array: np.ndarray) -> str:
 
 def main() -> int:
     parser = argparse.ArgumentParser()
-    parser.add_argument("--reference", default="/root/reference/src")
+    parser.add_argument("--reference", default=os.environ.get("FAUXICE_REFERENCE_SRC"),
+                        help="the reference checkout's src directory")
     parser.add_argument("--only", default=None)
     parser.add_argument("--skip-slow", action="store_true")
     args = parser.parse_args()
+    if not args.reference:
+        parser.error("give --reference or set FAUXICE_REFERENCE_SRC")
     os.environ.setdefault("NUMBA_CACHE_DIR", "/tmp/fauxice_numba_cache")
     os.environ.setdefault("PYTHONDONTWRITEBYTECODE", "1")
     sys.dont_write_bytecode = True

@@ -2,7 +2,8 @@
 """Generate tests/golden/routing_golden.json by running the reference routing.
 
 Loads ``hybrid/src/fauxce_hybrid/routing.py`` of the reference from
-``--reference`` (default /root/reference) by file path (the module needs only
+``--reference`` (or the FAUXICE_REFERENCE environment variable: the
+reference checkout's root directory) by file path (the module needs only
 numpy and scipy) and records, for every case of route_cases.py, either the
 raised exception (type and message) or the SHA-256 of the canonical JSON
 census, the SHA-256 of the three planes (provisional labels, synthesis mask,
@@ -37,8 +38,11 @@ def sha(data: bytes) -> str:
 
 def main() -> int:
     parser = argparse.ArgumentParser()
-    parser.add_argument("--reference", default="/root/reference")
+    parser.add_argument("--reference", default=os.environ.get("FAUXICE_REFERENCE"),
+                        help="the reference checkout's root directory")
     args = parser.parse_args()
+    if not args.reference:
+        parser.error("give --reference or set FAUXICE_REFERENCE")
     path = os.path.join(args.reference, "hybrid", "src", "fauxce_hybrid", "routing.py")
     spec = importlib.util.spec_from_file_location("reference_routing", path)
     ref = importlib.util.module_from_spec(spec)

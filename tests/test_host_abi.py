@@ -49,7 +49,18 @@ def test_struct_layouts_match_the_oracle():
     assert ctypes.sizeof(_lib.FxParams) == ctypes.sizeof(ox.OxParams)
     assert _lib.STAGE_DTYPE.itemsize == ox.STAGE_DTYPE.itemsize
     # fx_counters carries walk diagnostics beyond the reference's counters
-    assert ctypes.sizeof(_lib.FxCounters) == ctypes.sizeof(ox.OxCounters) + 5 * 8
+    assert ctypes.sizeof(_lib.FxCounters) == ctypes.sizeof(ox.OxCounters) + 6 * 8
+
+
+def test_request_entry_points_reject_bad_arguments():
+    """fx_cancel, fx_fetch and the two test knobs refuse a null context or an
+    out-of-range value without touching a device."""
+
+    lib = _lib.load()
+    assert lib.fx_cancel(None, 1) == 1
+    assert lib.fx_fetch(None, 1, 0, None, None, None, None, None) == 1
+    assert lib.fx_set_walk_window(None, 4.5) == 1
+    assert lib.fx_set_list_capacity(None, 0) == 1
 
 
 def test_frame_bytes_estimate_is_sane():

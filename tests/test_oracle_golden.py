@@ -71,11 +71,14 @@ def test_oracle_matches_reference_jobs(name, golden):
 
 
 @pytest.mark.slow
-def test_oracle_matches_reference_native_full_frame(golden):
-    """A full 5782x3946 frame against the reference's cpu-fast run."""
+@pytest.mark.parametrize("name", ["native_full", "heavy_full_0"])
+def test_oracle_matches_reference_full_frame(name, golden):
+    """Full 5782x3946 frames (the native frame and a heavy-damage frame at
+    about 5% coverage) against the reference's cpu-fast runs."""
 
-    expected = golden["jobs"]["native_full"]
-    main, prepass = cases.JOB_CASES["native_full"][0]()
+    expected = golden["jobs"][name]
+    main, prepass = cases.JOB_CASES[name][0]()
+    assert sha(main.astype("<u2")) == expected["input_sha256"], "input recipe drifted"
     res = ox.process(main, prepass)
     assert oracle_mismatches(expected, res) == []
 
