@@ -14,8 +14,13 @@ replay, dither writer, emit and counters.
   --impl reference  times the CPU restatement of the reference path
          (oracle/, OpenMP over all host cores) on the same workload.
 
-Multi-GPU (torchrun): every rank processes its own frames (replicas; frames
-are independent jobs), no collective on the data path.
+Multi-GPU: one process per GPU.  Under torchrun the ranks come from the
+environment; ``--gpus N`` without one relaunches this script under
+torch.distributed.run itself.  Rank r processes its own frame (seed 2 + r;
+frames are independent jobs), with no collective on the data path: the
+only collectives are the barriers around the timed region and the maximum
+of the ranks' elapsed times.  ``--plan-only`` prints the per-rank work plan
+after those collectives and exits (no GPU work; gloo on a CPU machine).
 """
 
 from __future__ import annotations
@@ -24,6 +29,7 @@ import argparse
 import ctypes
 import json
 import os
+import socket
 import statistics
 import subprocess
 import sys
@@ -48,8 +54,10 @@ SEED = 2
 STENCIL_BYTES_PER_PIXEL = 33
 WALK_BYTES_PER_CHANNEL = 36
 BATCH_FRAMES = 16          # uneven sizes, seeds 100..115
-SERVE_RATES = (2.0, 8.0, 32.0)
-STENCIL_PROFILE = os.path.join(ROOT, "profiles", "k_stencil_native_frame.md")
+HEAVY_FRAMES = 8           # full 5782x3946 frames at ~5% coverage, seeds 200..207
+SERVE_RATES = (2.0, 8.0, 32.0, 400.0)  # the last one above the GPU's capacity
+# DRAM bytes and warp instructions per k_stencil launch from an ncu capture
+NCU_COUNTERS = os.path.join(ROOT, "profiles", "ncu_counters.json")
 
 
 WALK_BLOCKS_PER_SM = 3   # window-walk segments per SM in one wave (kWinBlocksPerSM)
@@ -67,16 +75,18 @@ def launches_per_frame(h: int, w: int, per_wave: int) -> int:
     return 15 + 2 * waves
 
 
-def stencil_traffic():
-    """DRAM bytes per k_stencil launch from the committed ncu summary."""
+def ncu_counter(kernel: str, name: str):
+    """A counter of one kernel's committed ncu capture (None if absent)."""
 
     try:
-        for line in open(STENCIL_PROFILE):
-            if line.startswith("traffic_bytes_per_launch:"):
-                return int(line.split(":")[1].strip())
-    except OSError:
-        pass
-    return None
+        with open(NCU_COUNTERS) as handle:
+            return json.load(handle)[kernel][name]
+    except (OSError, KeyError, ValueError):
+        return None
+
+
+def stencil_traffic():
+    return ncu_counter("k_stencil", "dram_bytes_per_launch")
 
 
 def issue_roofline(stencil_ms: float, device: int):
@@ -103,30 +113,13 @@ def issue_roofline(stencil_ms: float, device: int):
     return {"bound": "issue", "warp_instructions_per_launch": inst,
             "achieved": round(achieved, 1), "peak": round(peak, 1), "unit": "G warp-inst/s",
             "frac": round(achieved / peak, 4),
-            "source": "instructions from profiles/k_stencil_native_frame.md (ncu), "
+            "source": "instructions from the ncu capture in profiles/ncu_counters.json, "
                       "time from this run's CUDA events, peak = 4 x SMs x max SM clock"}
 
 
 def stencil_warp_instructions():
-    """Warp instructions per k_stencil launch from the committed ncu summary."""
-
-    try:
-        for line in open(STENCIL_PROFILE):
-            if line.startswith("| warp instructions |"):
-                return float(line.split("|")[2].split()[0]) * 1e9  # "1.298 G (...)"
-    except (OSError, ValueError, IndexError):
-        pass
-    return None
-
-
-def generate_batch(count: int):
-    """Frames of the batched workload, generated in spawn workers (before
-    any CUDA call in this process)."""
-
-    import multiprocessing as mp
-
-    with mp.get_context("spawn").Pool(min(count, os.cpu_count() or 1)) as pool:
-        return pool.map(_batch_frame, range(count))
+    value = ncu_counter("k_stencil", "warp_instructions_per_launch")
+    return float(value) if value is not None else None
 
 
 def _batch_frame(index: int):
@@ -136,6 +129,49 @@ def _batch_frame(index: int):
     from fauxice_b200 import synthetic
 
     return synthetic.batch_frame(index)[0]
+
+
+def _heavy_frame(index: int):
+    for _p in (ROOT, os.path.join(ROOT, "digital-fauxice_b200")):
+        if _p not in sys.path:
+            sys.path.insert(0, _p)
+    from fauxice_b200 import synthetic
+
+    return synthetic.heavy_full_frame(index)[0]
+
+
+def _serving_frame(spec):
+    for _p in (ROOT, os.path.join(ROOT, "digital-fauxice_b200")):
+        if _p not in sys.path:
+            sys.path.insert(0, _p)
+    from fauxice_b200 import synthetic
+
+    seed, h, w, coverage = spec
+    return synthetic.coverage_frame(seed, h, w, coverage)
+
+
+def generate(fn, items):
+    """Frames generated in spawn workers (before any CUDA call here)."""
+
+    import multiprocessing as mp
+
+    with mp.get_context("spawn").Pool(min(len(items), os.cpu_count() or 1)) as pool:
+        return pool.map(fn, items)
+
+
+def serving_pool_specs(seed: int = 500):
+    """The serving pool: 4 full frames, 4 of 2892x1973 and 8 crops of
+    U[256, 2048]^2, each with its own defect coverage drawn from
+    U[0.1%, 3%] (seed, height, width, coverage)."""
+
+    rng = np.random.default_rng(seed)
+    specs = []
+    for k, (h, w) in enumerate([(5782, 3946)] * 4 + [(2892, 1973)] * 4):
+        specs.append((seed + k, h, w, float(rng.uniform(0.001, 0.03))))
+    for k in range(8):
+        h, w = (int(v) for v in rng.integers(256, 2049, size=2))
+        specs.append((seed + 8 + k, h, w, float(rng.uniform(0.001, 0.03))))
+    return specs
 
 
 def parse():
@@ -150,9 +186,38 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched and serving runs")
     ap.add_argument("--batch-steps", type=int, default=3)
+    ap.add_argument("--no-heavy", action="store_true", help="skip the heavy-damage batch")
     ap.add_argument("--serve-seconds", type=float, default=6.0,
                     help="arrival window per request rate (the workload's 120 s, shortened)")
+    ap.add_argument("--serve-rates", default=",".join(f"{r:g}" for r in SERVE_RATES),
+                    help="comma-separated Poisson request rates per second")
+    ap.add_argument("--plan-only", action="store_true",
+                    help="print each rank's work plan after the collectives; no GPU work")
     return ap.parse_args()
+
+
+def free_port() -> int:
+    with socket.socket() as sock:
+        sock.bind(("127.0.0.1", 0))
+        return sock.getsockname()[1]
+
+
+def launch_command(gpus: int, argv: list[str], port: int) -> list[str]:
+    """This script relaunched as ``gpus`` ranks, one process per GPU."""
+
+    return [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+            f"--nproc-per-node={gpus}", "--master-addr=127.0.0.1", f"--master-port={port}",
+            os.path.abspath(__file__), *argv]
+
+
+def rank_plan(rank: int, world: int) -> dict:
+    """What rank ``rank`` processes: its own native frame (seed 2 + rank)
+    for the timed plain path."""
+
+    from fauxice_b200 import replicas
+
+    seeds = replicas.shard(list(range(SEED, SEED + world)), rank, world)
+    return {"rank": rank, "frame_seeds": seeds}
 
 
 def load_peaks():
@@ -221,7 +286,7 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def dist_setup():
+def dist_setup(plan_only: bool = False):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -231,9 +296,28 @@ def dist_setup():
         import torch
         import torch.distributed as dist
 
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        backend = "gloo" if plan_only or not torch.cuda.is_available() else "nccl"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     return world, rank, local
+
+
+def run_plan(world: int, rank: int) -> None:
+    """The plan of every rank, gathered after the timed region's collectives."""
+
+    plan = rank_plan(rank, world)
+    barrier(world)
+    slowest = max_over_ranks(0.5 + rank, world)
+    plans = [plan]
+    if world > 1:
+        import torch.distributed as dist
+
+        plans = [None] * world
+        dist.all_gather_object(plans, plan)
+    if rank == 0:
+        print(json.dumps({"world": world, "plans": plans, "max_over_ranks": slowest}),
+              flush=True)
 
 
 def max_over_ranks(value: float, world: int) -> float:
@@ -324,14 +408,15 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
-def run_b200(args, world, rank, local, frames=None):
+def run_b200(args, world, rank, local, frames=None, heavy=None, pool=None):
     import torch
 
     from fauxice_b200 import _lib, engine, synthetic
     from fauxice_b200.profile import DEFAULT_PROFILE, NIKON_PE_INITIAL_STATE
 
     torch.cuda.set_device(local)
-    main, prepass = synthetic.native_frame(SEED)
+    seed = rank_plan(rank, world)["frame_seeds"][0]  # rank r: its own frame, seed 2 + r
+    main, prepass = synthetic.native_frame(seed)
     h, w = main.shape[:2]
     lib = _lib.load()
     ctx = engine.context(local)
@@ -357,11 +442,11 @@ def run_b200(args, world, rank, local, frames=None):
     out_host = d_out.cpu().numpy().view(np.uint16)
     digest = hashlib.sha256(out_host.astype("<u2").tobytes()).hexdigest()
     golden = json.load(open(os.path.join(ROOT, "tests", "golden", "reference_results.json")))
-    expect = golden["jobs"]["native_full"]
+    expect = golden["jobs"]["native_full"]  # the seed-2 frame: rank 0's
     bit_exact = (digest == expect["output_sha256"]
                  and counters.attempted == expect["attempted_pixels"]
                  and counters.public_advances == expect["public_rng_advances"]
-                 and counters.final_state == expect["final_rng_state"])
+                 and counters.final_state == expect["final_rng_state"]) if seed == SEED else None
 
     ctx.check(lib.fx_profile_enable(ctx.handle, 1))
     ctx.check(lib.fx_profile_read(ctx.handle, None, None, 1))
@@ -430,7 +515,7 @@ def run_b200(args, world, rank, local, frames=None):
             t0 = time.perf_counter()
             result = engine.process_b200(job)
             times.append(time.perf_counter() - t0)
-        e2e_ok = result.replay.output_sha256 == expect["output_sha256"]
+        e2e_ok = result.replay.output_sha256 == digest
         e2e_s = max_over_ranks(sum(times) / len(times), world)
         e2e = {"value": round(world * mp / e2e_s, 3), "unit": "MP/s",
                "h2d_bytes_per_step": int(main.nbytes), "d2h_bytes_per_step": int(h * w * 6),
@@ -459,11 +544,12 @@ def run_b200(args, world, rank, local, frames=None):
             "data": "synthetic",
             "config": {
                 "workload": "plain single-frame path, native 5782x3946 RGBI uint16 frame "
-                            "(seed 2, ~0.5% defects), inputs resident in HBM",
+                            "(seed 2 + rank; 3000 discs and 60 scratches touching ~6% of "
+                            "the pixels), inputs resident in HBM",
                 "frames_per_step": 1,
                 "l2": "inputs 182.5 MB per frame > 126 MB L2; no flush",
                 "parallelism": f"replicas x{world}",
-                "bit_exact_vs_reference": bool(bit_exact),
+                "bit_exact_vs_reference": bit_exact,
             },
             "latency_ms": {"p50": round(lat[len(lat) // 2], 3),
                            "p99": round(lat[min(len(lat) - 1, int(0.99 * len(lat)))], 3)},
@@ -481,7 +567,11 @@ def run_b200(args, world, rank, local, frames=None):
         }
         if frames is not None:
             line["batched"] = run_batched(ctx, frames, args, golden)
-            line["serving"] = run_serving(ctx, frames, args)
+            line["e2e_batched"] = run_e2e_batched(frames, line["batched"])
+        if heavy is not None:
+            line["heavy_batched"] = run_heavy(ctx, heavy, args, golden, line.get("batched"))
+        if pool is not None:
+            line["serving"] = run_serving(ctx, pool, args)
         if not args.no_routing:
             line["routing"] = run_routing(ctx, d_in, h, w)
         print(json.dumps(line), flush=True)
@@ -585,15 +675,14 @@ def run_batched(ctx, frames, args, golden):
                                              waves=(0, 148))
     best, med = timed(as_jobs(outs), slots)
     same = all(torch.equal(a, b) for a, b in zip(outs, plain_out))
-    ref_ok = []
-    for i in range(5):
-        host = outs[i].cpu().numpy().view(np.uint16)
-        digest = hashlib.sha256(host.astype("<u2").tobytes()).hexdigest()
-        ref_ok.append(digest == golden["jobs"][f"batch_{i}"]["output_sha256"])
+    digests = [hashlib.sha256(o.cpu().numpy().view(np.uint16).astype("<u2").tobytes()).hexdigest()
+               for o in outs]
+    ref_ok = [digests[i] == golden["jobs"][f"batch_{i}"]["output_sha256"] for i in range(5)]
     batch.set_walk_wave(ctx, 0)
     return {
+        "_digests": digests,
         "workload": f"{len(frames)} frames cycling 5782x3946, 3946x5782, 2892x1973, 1024x768, "
-                    "4000x2700 (seeds 100-115, ~0.5% defects), device-resident",
+                    "4000x2700 (seeds 100-115, native defect density), device-resident",
         "value": round(mp / med, 1), "unit": "MP/s", "megapixels": round(mp, 2),
         "ms_per_step": round(1000 * med, 2), "steps": args.batch_steps,
         "plain_same_mix": {"value": round(mp / plain_med, 1), "unit": "MP/s",
@@ -608,55 +697,165 @@ def run_batched(ctx, frames, args, golden):
     }
 
 
-def run_serving(ctx, frames, args):
-    """Requests at Poisson rates 2, 8 and 32 per second over a shortened
-    window; sizes 50% 5782x3946, 30% 2892x1973, 20% seeded crops of
-    U[256, 2048]^2 from the batch frames; inputs in pinned host memory."""
+def run_heavy(ctx, frames, args, golden, batched):
+    """Config 4, heavy damage: 8 full 5782x3946 frames at ~5% coverage
+    (200 floor-saturating blobs, crossing scratches; seeds 200-207),
+    device-resident, one at a time and batched with the slot count the mix
+    tuned; every batched output equals its single-frame output, and frames
+    0-1 equal the reference's recorded results."""
+
+    import hashlib
 
     import torch
 
-    from fauxice_b200 import serve
+    from fauxice_b200 import batch
 
-    full = [f for f in frames if f.shape[:2] == (5782, 3946)]
-    half = [f for f in frames if f.shape[:2] == (2892, 1973)]
-    rng = np.random.default_rng(500)
-    crops = []
-    for k in range(6):
-        src = frames[k % len(frames)]
-        ch, cw = (int(v) for v in rng.integers(256, 2049, size=2))
-        ch, cw = min(ch, src.shape[0]), min(cw, src.shape[1])
-        y = int(rng.integers(0, src.shape[0] - ch + 1))
-        x = int(rng.integers(0, src.shape[1] - cw + 1))
-        crops.append(np.ascontiguousarray(src[y:y + ch, x:x + cw]))
-    pinned = lambda a: torch.from_numpy(np.ascontiguousarray(a).view(np.int16)).pin_memory()
-    pools = [[pinned(f) for f in full], [pinned(f) for f in half], [pinned(f) for f in crops]]
+    d_in = [torch.from_numpy(np.ascontiguousarray(f).view(np.int16)).to("cuda") for f in frames]
+    plain_out = [torch.empty((f.shape[0], f.shape[1], 3), dtype=torch.int16, device="cuda")
+                 for f in frames]
+    outs = [torch.empty_like(o) for o in plain_out]
+    mp = sum(f.shape[0] * f.shape[1] for f in frames) / 1e6
+    jobs = lambda dst: [batch.DeviceFrame(d.data_ptr(), f.shape[0], f.shape[1], o.data_ptr())
+                        for f, d, o in zip(frames, d_in, dst)]
+    slots = batched["slots"] if batched else 4
+    wave = batched["walk_wave"] if batched and isinstance(batched["walk_wave"], int) else 0
+
+    def timed(dst, n_slots):
+        times = []
+        for _ in range(args.batch_steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            counters = batch.run_device_batch(ctx, jobs(dst), slots=n_slots)
+            torch.cuda.synchronize()
+            times.append(time.perf_counter() - t0)
+        return sorted(times)[len(times) // 2], counters
+
+    batch.set_walk_wave(ctx, 0)
+    batch.run_device_batch(ctx, jobs(plain_out), slots=1)  # warm
+    plain_med, _ = timed(plain_out, 1)
+    batch.set_walk_wave(ctx, wave)
+    med, counters = timed(outs, slots)
+    batch.set_walk_wave(ctx, 0)
+    same = all(torch.equal(a, b) for a, b in zip(outs, plain_out))
+    ref_ok = []
+    for i in range(2):
+        host = outs[i].cpu().numpy().view(np.uint16)
+        digest = hashlib.sha256(host.astype("<u2").tobytes()).hexdigest()
+        ref_ok.append(digest == golden["jobs"][f"heavy_full_{i}"]["output_sha256"])
+    return {
+        "workload": f"{len(frames)} full 5782x3946 heavy-damage frames (~5% coverage incl. "
+                    "200 blobs r U[20,60] with IR x U[0.01,0.1], crossing scratches; seeds "
+                    "200-207), device-resident",
+        "value": round(mp / med, 1), "unit": "MP/s", "megapixels": round(mp, 2),
+        "ms_per_step": round(1000 * med, 2), "steps": args.batch_steps,
+        "plain_same_mix": {"value": round(mp / plain_med, 1), "unit": "MP/s",
+                           "ms_per_step": round(1000 * plain_med, 2), "slots": 1},
+        "slots": slots, "walk_wave": wave or "default",
+        "attempted_pixels": int(sum(c.attempted for c in counters)),
+        "rng_dependent_channels": int(sum(c.rng_dependent for c in counters)),
+        "timing": "host clock around the whole batch, synchronize on both sides",
+        "bit_exact_vs_single_frame": bool(same),
+        "bit_exact_vs_reference_frames_0_1": bool(all(ref_ok)),
+    }
+
+
+def run_e2e_batched(frames, batched):
+    """The batched mix through the public host-buffer API: 16 jobs of host
+    numpy frames into process_batch (validation, prepass, staged uploads,
+    passes, downloads and output SHA-256 digests all inside the timed
+    region), with the slot count the device-resident run tuned."""
+
+    from fauxice_b200 import batch, synthetic
+
+    digests = batched.pop("_digests")
+    jobs = [make_job(f, synthetic.make_prepass(f)) for f in frames]
+    batch.process_batch(jobs[:2], slots=batched["slots"])  # warm the host staging
+    t0 = time.perf_counter()
+    results = batch.process_batch(jobs, slots=batched["slots"])
+    elapsed = time.perf_counter() - t0
+    mp = sum(f.shape[0] * f.shape[1] for f in frames) / 1e6
+    exact = all(r.replay.output_sha256 == d for r, d in zip(results, digests))
+    return {"value": round(mp / elapsed, 1), "unit": "MP/s", "ms_per_step": round(1e3 * elapsed, 1),
+            "frames": len(frames), "slots": batched["slots"],
+            "h2d_bytes_per_step": int(sum(f.nbytes for f in frames)),
+            "d2h_bytes_per_step": int(sum(f.shape[0] * f.shape[1] * 6 for f in frames)),
+            "bit_exact_vs_device_batch": bool(exact),
+            "api": "fauxice_b200.batch.process_batch(jobs) (host numpy in/out, output SHA-256 "
+                   "per frame on a thread pool)"}
+
+
+def run_serving(ctx, pool, args):
+    """Requests at Poisson rates over a shortened window; sizes 50% 5782x3946,
+    30% 2892x1973, 20% crops of U[256, 2048]^2, each pool frame with its own
+    defect coverage from U[0.1%, 3%]; inputs in pinned host memory.
+
+    Admission by device memory, latency from arrival to the output in host
+    memory, every output compared on the device with the same frame's
+    single-frame output."""
+
+    import torch
+
+    from fauxice_b200 import _lib, serve
+    from fauxice_b200.profile import DEFAULT_PROFILE, NIKON_PE_INITIAL_STATE
+
+    lib = _lib.load()
+    params = DEFAULT_PROFILE.hot_path_parameters().to_c()
+    frames, specs = pool
+    pinned, expected = [], []
+    for f in frames:
+        h, w = f.shape[:2]
+        pinned.append(torch.from_numpy(np.ascontiguousarray(f).view(np.int16)).pin_memory())
+        d_in = pinned[-1].to("cuda")
+        out = torch.empty((h, w, 3), dtype=torch.int16, device="cuda")
+        ctx.check(lib.fx_process_device(ctx.handle, d_in.data_ptr(), h, w, ctypes.byref(params),
+                                        None, NIKON_PE_INITIAL_STATE, out.data_ptr(), None, None,
+                                        None, None))
+        expected.append(out)
+    torch.cuda.synchronize()
+    groups = [[k for k, s in enumerate(specs) if (s[1], s[2]) == (5782, 3946)],
+              [k for k, s in enumerate(specs) if (s[1], s[2]) == (2892, 1973)],
+              [k for k, s in enumerate(specs) if (s[1], s[2]) not in ((5782, 3946), (2892, 1973))]]
+    rates = [float(r) for r in args.serve_rates.split(",") if r]
     out = {"workload": "Poisson arrivals, 50% 5782x3946 / 30% 2892x1973 / 20% crops "
-                       f"U[256,2048]^2, {args.serve_seconds:g} s per rate (of the 120 s "
-                       "workload), latency from arrival to device completion, 4 slots",
-           "rates": {}}
-    for r_i, rate in enumerate(SERVE_RATES):
+                       "U[256,2048]^2, per-frame defect coverage U[0.1%,3%] (pool of 16 "
+                       f"frames), {args.serve_seconds:g} s per rate (of the 120 s workload); "
+                       "admission by free HBM (fx_frame_bytes), up to 12 in flight; latency "
+                       "from arrival to the RGB16 output in pinned host memory; every output "
+                       "compared on the device with its frame's single-frame output",
+           "pool_coverage": [round(s[3], 4) for s in specs], "rates": {}}
+    for r_i, rate in enumerate(rates):
         arrivals = serve.poisson_arrivals(rate, args.serve_seconds, seed=600 + r_i)
         pick = np.random.default_rng(700 + r_i)
         requests = []
         for t in arrivals:
             u = pick.random()
-            pool = pools[0] if u < 0.5 else (pools[1] if u < 0.8 else pools[2])
-            requests.append(serve.Request(float(t), pool[int(pick.integers(0, len(pool)))]))
-        report = serve.serve(ctx, requests, slots=4)
+            group = groups[0] if u < 0.5 else (groups[1] if u < 0.8 else groups[2])
+            k = group[int(pick.integers(0, len(group)))]
+            requests.append(serve.Request(float(t), pinned[k], expected[k]))
+        report = serve.serve(ctx, requests, max_slots=12)
         out["rates"][f"{rate:g}/s"] = report.summary()
     return out
 
 
 def main():
     args = parse()
-    world, rank, local = dist_setup()
-    if args.impl == "reference":
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # one process per GPU: relaunch under torch.distributed.run
+        sys.exit(subprocess.call(launch_command(args.gpus, sys.argv[1:], free_port())))
+    world, rank, local = dist_setup(args.plan_only)
+    if args.plan_only:
+        run_plan(world, rank)
+    elif args.impl == "reference":
         run_reference(args, world, rank)
     else:
-        frames = None
+        frames = heavy = pool = None
         if world == 1 and not args.no_batch:
-            frames = generate_batch(BATCH_FRAMES)
-        run_b200(args, world, rank, local, frames)
+            frames = generate(_batch_frame, list(range(BATCH_FRAMES)))
+            if not args.no_heavy:
+                heavy = generate(_heavy_frame, list(range(HEAVY_FRAMES)))
+            specs = serving_pool_specs()
+            pool = (generate(_serving_frame, specs), specs)
+        run_b200(args, world, rank, local, frames, heavy, pool)
     if world > 1:
         import torch.distributed as dist
 

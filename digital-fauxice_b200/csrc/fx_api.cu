@@ -587,6 +587,26 @@ static int copy_threads() {
     return n >= 8 ? 8 : (n > 0 ? (int)n : 1);
 }
 
+// memcpy of a large buffer split over the copy threads (one host thread
+// cannot saturate the memory bus; frames here are 100-200 MB).
+static void parallel_memcpy(void *dst, const void *src, size_t bytes) {
+    const int nt = bytes < ((size_t)8 << 20) ? 1 : copy_threads();
+    if (nt == 1) {
+        std::memcpy(dst, src, bytes);
+        return;
+    }
+    const size_t part = (bytes + nt - 1) / nt;
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nt; ++t)
+        pool.emplace_back([=] {
+            const size_t off = (size_t)t * part;
+            if (off < bytes)
+                std::memcpy(static_cast<char *>(dst) + off, static_cast<const char *>(src) + off,
+                            std::min(part, bytes - off));
+        });
+    for (std::thread &th : pool) th.join();
+}
+
 static int ensure_pinned(fx_context *ctx, void **buf, size_t *have, size_t need) {
     if (*have >= need) return FX_OK;
     if (*buf) cudaFreeHost(*buf);
@@ -879,10 +899,23 @@ static int stage_host_results(fx_context *ctx, Slot &s) {
     return FX_OK;
 }
 
-static Slot *free_slot(fx_context *ctx) {
-    for (Slot &s : ctx->slots)
-        if (!s.busy) return &s;
-    return nullptr;
+// A free slot for a frame of geometry g: the one with the smallest arena
+// that already holds the frame, else one without an arena, else any free
+// slot (whose arena then grows: a cudaFree, which waits for the whole
+// device, so serving and batching keep to the first two cases).
+static Slot *free_slot(fx_context *ctx, const Geometry &g) {
+    const size_t need = arena_layout(g, amb_capacity(ctx, g), nullptr);
+    Slot *fit = nullptr, *empty = nullptr, *any = nullptr;
+    for (Slot &s : ctx->slots) {
+        if (s.busy) continue;
+        if (!any) any = &s;
+        if (!s.arena.base) {
+            if (!empty) empty = &s;
+        } else if (s.arena.bytes >= need && (!fit || s.arena.bytes < fit->arena.bytes)) {
+            fit = &s;
+        }
+    }
+    return fit ? fit : (empty ? empty : any);
 }
 
 FX_API int fx_submit(fx_context *ctx, const fx_frame *f, int64_t *ticket) {
@@ -893,10 +926,10 @@ FX_API int fx_submit(fx_context *ctx, const fx_frame *f, int64_t *ticket) {
     if (rc) return rc;
     if (!f->stages && f->width < 8)
         return fail(ctx, FX_ERR_GEOMETRY, "main RGBI frame has no complete producer cell");
-    Slot *slot = free_slot(ctx);
+    const Geometry g = make_geometry(f->height, f->width);
+    Slot *slot = free_slot(ctx, g);
     if (!slot) return fail(ctx, FX_PENDING, "no free slot");
     Slot &s = *slot;
-    const Geometry g = make_geometry(f->height, f->width);
     const size_t px = (size_t)g.h * g.w;
     rc = ensure_arena(ctx, s, g, amb_capacity(ctx, g));
     if (rc) return rc;
@@ -916,7 +949,7 @@ FX_API int fx_submit(fx_context *ctx, const fx_frame *f, int64_t *ticket) {
         FX_CUDA(ctx, cudaMallocHost(&s.h_out, out_bytes));
         s.h_out_bytes = out_bytes;
     }
-    std::memcpy(s.h_in, f->main_rgbi, in_bytes);
+    parallel_memcpy(s.h_in, f->main_rgbi, in_bytes);
     s.device = false;
     s.frame = *f;
     s.params = *f->params;
@@ -969,10 +1002,10 @@ FX_API int fx_submit_device(fx_context *ctx, const uint16_t *d_rgbi, int32_t h, 
     if (rc) return rc;
     if (!stages && w < 8)
         return fail(ctx, FX_ERR_GEOMETRY, "main RGBI frame has no complete producer cell");
-    Slot *slot = free_slot(ctx);
+    const Geometry g = make_geometry(h, w);
+    Slot *slot = free_slot(ctx, g);
     if (!slot) return fail(ctx, FX_PENDING, "no free slot");
     Slot &s = *slot;
-    const Geometry g = make_geometry(h, w);
     rc = ensure_arena(ctx, s, g, amb_capacity(ctx, g));
     if (rc) return rc;
     s.frame = fx_frame{};
@@ -1075,9 +1108,9 @@ static void deliver_host_results(Slot &s, const FetchTargets *fetch) {
     uint16_t *rgb = fetch ? fetch->rgb : s.frame.rgb_out;
     float *score = fetch ? fetch->score : s.frame.score_out;
     uint8_t *changed = fetch ? fetch->changed : s.frame.changed_out;
-    if (rgb) std::memcpy(rgb, ho, px * 6);
-    if (score) std::memcpy(score, ho + px * 6, px * 4);
-    if (changed) std::memcpy(changed, ho + px * 10, px);
+    if (rgb) parallel_memcpy(rgb, ho, px * 6);
+    if (score) parallel_memcpy(score, ho + px * 6, px * 4);
+    if (changed) parallel_memcpy(changed, ho + px * 10, px);
     if (fetch && fetch->at_floor) {
         // engine.py:175-199: at-floor = score plane == the score floor
         const float *sp = reinterpret_cast<const float *>(ho + px * 6);

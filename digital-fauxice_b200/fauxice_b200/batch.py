@@ -20,8 +20,11 @@ scans leave most SMs to the others).
 from __future__ import annotations
 
 import ctypes
+import hashlib
+import os
 import time
 from collections import deque
+from concurrent.futures import ThreadPoolExecutor
 from dataclasses import dataclass
 from typing import Iterable, Sequence
 
@@ -155,13 +158,21 @@ def tune_slots(ctx: _lib.Context, frames: Sequence[DeviceFrame],
     return choice, timings
 
 
+def _sha256(array: np.ndarray) -> bytes:
+    # little-endian uint16 bytes in row-major order, hashed in place (hashlib
+    # releases the GIL for large buffers, so several frames hash at once)
+    return hashlib.sha256(memoryview(array).cast("B")).digest()
+
+
 def process_batch(jobs: Sequence, *, slots: int = 4, export_diagnostics: bool = False,
-                  device: int = 0) -> list[ProcessingResult]:
+                  device: int = 0, hash_workers: int | None = None) -> list[ProcessingResult]:
     """Process many jobs with up to ``slots`` frames in flight.
 
     Every job is validated (and its prepass record checked) before any is
     submitted, so a bad job fails the call before device work starts.  Each
     result equals :func:`fauxice_b200.engine.process_b200` on the same job.
+    The output digests (the replay result's output_sha256) are computed on
+    ``hash_workers`` threads while later frames are still on the device.
     """
 
     for job in jobs:
@@ -179,7 +190,8 @@ def process_batch(jobs: Sequence, *, slots: int = 4, export_diagnostics: bool = 
     floor = DEFAULT_PROFILE.score_floor()
 
     inflight: deque[tuple[int, int, object]] = deque()
-    results: list[ProcessingResult | None] = [None] * len(jobs)
+    finished: list[tuple[int, FrameOutcome, object]] = []
+    hasher = ThreadPoolExecutor(hash_workers or min(8, os.cpu_count() or 1))
 
     def finish_oldest() -> None:
         index, ticket, keep = inflight.popleft()
@@ -187,11 +199,8 @@ def process_batch(jobs: Sequence, *, slots: int = 4, export_diagnostics: bool = 
         status = lib.fx_wait(ctx.handle, ticket, -1, ctypes.byref(counters))
         _check(ctx, status)
         _, out, score, changed = keep
-        outcome = FrameOutcome(out, counters, score, changed)
-        diagnostics = make_diagnostics(outcome, floor) if export_diagnostics else None
-        results[index] = ProcessingResult(output_rgb16=out, replay=replay_result(outcome),
-                                          profile_id=DEFAULT_PROFILE.profile_id,
-                                          diagnostics=diagnostics)
+        finished.append((index, FrameOutcome(out, counters, score, changed),
+                         hasher.submit(_sha256, out)))
 
     for index, job in enumerate(jobs):
         px = np.ascontiguousarray(job.acquisition.main.pixels, dtype=np.uint16)
@@ -216,6 +225,17 @@ def process_batch(jobs: Sequence, *, slots: int = 4, export_diagnostics: bool = 
             _check(ctx, status)
             inflight.append((index, ticket.value, (px, out, score, changed)))
             break
-    while inflight:
-        finish_oldest()
+    try:
+        while inflight:
+            finish_oldest()
+        results: list[ProcessingResult | None] = [None] * len(jobs)
+        for index, outcome, digest in finished:
+            outcome.digest = digest.result()
+            diagnostics = make_diagnostics(outcome, floor) if export_diagnostics else None
+            results[index] = ProcessingResult(output_rgb16=outcome.output,
+                                              replay=replay_result(outcome),
+                                              profile_id=DEFAULT_PROFILE.profile_id,
+                                              diagnostics=diagnostics)
+    finally:
+        hasher.shutdown(wait=True)
     return results  # type: ignore[return-value]

@@ -1,18 +1,30 @@
 """Serving: requests of mixed sizes admitted as they arrive (continuous batching).
 
-No counterpart in the reference.  A request is one RGBI frame in host
-memory.  Device memory is sized once, before the run, for the largest
-request: every library slot (fx_reserve_frames) and one input/output buffer
-pair per slot; the run fails up front with MemoryError when free HBM cannot
-hold them.  The loop admits requests in arrival order while a buffer pair is
-free, so frames that arrive while others run are processed alongside them:
-each upload is queued on a copy stream, the frame is submitted with
-fx_submit_device once its upload has landed, and completions are polled.
-Latency runs from arrival to the moment the completion is seen.  Results
-equal one-frame processing: every request is an independent job.
+No counterpart in the reference, which processes one job per call.  A
+request is one RGBI frame in host memory.  The loop admits requests in
+arrival order while the device has room for them, so frames that arrive
+while others run are processed alongside them, each in its own library slot
+(its own stream and device buffers):
 
-Device memory for inputs and outputs is plumbing (torch tensors); the
-processing itself is the library's.
+* admission is by device memory: a request needs its pass buffers
+  (``fx_frame_bytes(h, w)``, the same estimate the reference's CUDA backend
+  checks against free memory, cuda_backend/engine.py:168-224) plus its input
+  and output planes.  A slot whose buffers already hold the frame is reused
+  (no new memory); otherwise a slot without buffers takes it if the bytes
+  fit the budget (the free HBM reported by ``fx_mem_info`` at the start,
+  less a reserve).  Slot buffers are never freed while frames are in
+  flight: a ``cudaFree`` would wait for the whole device.
+* a request's upload is queued on a copy stream; the frame is submitted
+  with ``fx_submit_device`` once the upload has landed; when the pass is
+  done its RGB16 output is copied back into pinned host memory on a second
+  copy stream.  The loop never blocks on a copy.
+* latency runs from arrival to the moment the output is in host memory.
+* optionally, each output is compared on the device, bit for bit, with the
+  output of the same frame processed alone (kept resident for the check);
+  the count of differing values is read once, after the run.
+
+Device memory for inputs and outputs is plumbing (torch tensors from its
+caching allocator); the processing itself is the library's.
 """
 
 from __future__ import annotations
@@ -35,6 +47,8 @@ class Request:
     arrival_s: float  # seconds after the start of the run
     pixels: object    # H x W x 4 uint16 in host memory: a numpy array, or a
                       # pinned torch int16 tensor (then the upload is a DMA)
+    expected: object = None  # the frame's RGB16 output processed alone: a
+                             # device int16 tensor (H, W, 3), for verification
 
 
 @dataclass
@@ -50,23 +64,43 @@ class Completion:
     def latency_s(self) -> float:
         return self.done_s - self.arrival_s
 
+    @property
+    def queued_s(self) -> float:
+        return self.admitted_s - self.arrival_s
+
 
 @dataclass
 class ServeReport:
     completions: list[Completion] = field(default_factory=list)
     wall_s: float = 0.0
     megapixels: float = 0.0
+    max_in_flight: int = 0
+    peak_bytes: int = 0        # slot buffers + planes of the requests in flight
+    budget_bytes: int = 0
+    slots_used: int = 0        # library slots that got device buffers
+    verified: int = 0          # outputs compared with their single-frame output
+    mismatches: int = 0        # differing uint16 values over all verified outputs
 
-    def percentile_ms(self, q: float) -> float:
-        lat = np.array([c.latency_s for c in self.completions]) * 1e3
+    def percentile_ms(self, q: float, attr: str = "latency_s") -> float:
+        lat = np.array([getattr(c, attr) for c in self.completions]) * 1e3
         return float(np.percentile(lat, q)) if lat.size else float("nan")
 
     def summary(self) -> dict:
-        return {"requests": len(self.completions), "wall_s": round(self.wall_s, 3),
-                "mp_per_s": round(self.megapixels / self.wall_s, 1) if self.wall_s else None,
-                "p50_ms": round(self.percentile_ms(50), 2),
-                "p95_ms": round(self.percentile_ms(95), 2),
-                "p99_ms": round(self.percentile_ms(99), 2)}
+        out = {"requests": len(self.completions), "wall_s": round(self.wall_s, 3),
+               "mp_per_s": round(self.megapixels / self.wall_s, 1) if self.wall_s else None,
+               "p50_ms": round(self.percentile_ms(50), 2),
+               "p95_ms": round(self.percentile_ms(95), 2),
+               "p99_ms": round(self.percentile_ms(99), 2),
+               "queue_p50_ms": round(self.percentile_ms(50, "queued_s"), 2),
+               "queue_p99_ms": round(self.percentile_ms(99, "queued_s"), 2),
+               "max_in_flight": self.max_in_flight,
+               "peak_device_bytes": self.peak_bytes,
+               "budget_bytes": self.budget_bytes,
+               "slots_used": self.slots_used}
+        if self.verified:
+            out["verified"] = self.verified
+            out["bit_exact"] = self.mismatches == 0 and self.verified == len(self.completions)
+        return out
 
 
 def poisson_arrivals(rate_per_s: float, duration_s: float, seed: int) -> np.ndarray:
@@ -81,17 +115,56 @@ def poisson_arrivals(rate_per_s: float, duration_s: float, seed: int) -> np.ndar
         times.append(t)
 
 
-def serve(ctx: _lib.Context, requests: Sequence[Request], *, slots: int = 4,
-          reserve_bytes: int = 2 << 30, keep_outputs: bool = False) -> ServeReport:
+def frame_bytes(height: int, width: int) -> int:
+    """Device bytes of one pass's buffers (fx_frame_bytes)."""
+
+    return int(_lib.load().fx_frame_bytes(int(height), int(width)))
+
+
+class SlotModel:
+    """The library's slot choice, mirrored on the host: the free slot with
+    the smallest buffers that hold the frame, else a slot without buffers.
+    Tracks which buffer sizes exist so admission knows whether a request
+    needs new device memory."""
+
+    def __init__(self, slots: int) -> None:
+        self.free_sizes: list[int] = []   # buffers of idle slots
+        self.empty = slots                 # slots without buffers
+        self.allocated = 0                 # bytes of all slot buffers
+
+    def choose(self, need: int) -> tuple[str, int] | None:
+        fits = [s for s in self.free_sizes if s >= need]
+        if fits:
+            return "reuse", min(fits)
+        if self.empty:
+            return "new", need
+        return None
+
+    def take(self, kind: str, size: int) -> None:
+        if kind == "reuse":
+            self.free_sizes.remove(size)
+        else:
+            self.empty -= 1
+            self.allocated += size
+
+    def give_back(self, size: int) -> None:
+        self.free_sizes.append(size)
+
+
+def serve(ctx: _lib.Context, requests: Sequence[Request], *, max_slots: int = 12,
+          budget_bytes: int | None = None, reserve_bytes: int = 8 << 30,
+          keep_outputs: bool = False) -> ServeReport:
     """Run the request loop in real time; requests must be sorted by arrival.
 
-    Before the clock starts, every library slot is sized for the largest
-    request (fx_reserve_frames) and each of ``slots`` device buffer pairs
-    (input RGBI, output RGB16) is allocated at that size, so nothing is
-    allocated or freed while frames are in flight.  A request is admitted as
-    soon as a buffer pair is free: its upload is queued on a copy stream and
-    the frame is submitted when the upload's event has completed, so the loop
-    never blocks on a copy and keeps polling arrivals and completions.
+    ``max_slots`` bounds the requests in flight; device memory bounds them
+    too: ``budget_bytes`` (default: the free HBM at the start less
+    ``reserve_bytes``) must hold every slot's buffers plus the input and
+    output planes of the requests in flight.  A request that carries its
+    ``expected`` output is checked against it on the device, after its
+    output's copy to host memory has been queued (off the latency path).
+    The context should hold no slot buffers yet (a fresh context, or one
+    whose slots this loop sized before): the host's model of the slots
+    starts empty.
     """
 
     import torch
@@ -100,25 +173,31 @@ def serve(ctx: _lib.Context, requests: Sequence[Request], *, slots: int = 4,
     report = ServeReport()
     if not requests:
         return report
-    batch.set_slots(ctx, slots)
-    max_h = max(int(r.pixels.shape[0]) for r in requests)
-    max_w = max(int(r.pixels.shape[1]) for r in requests)
-    batch.reserve_frames(ctx, max_h, max_w)
-    pair_bytes = slots * max_h * max_w * 14
-    free, total = ctypes.c_size_t(), ctypes.c_size_t()
-    with ctx.lock:
-        if (lib.fx_mem_info(ctx.handle, ctypes.byref(free), ctypes.byref(total)) == 0
-                and free.value < pair_bytes + reserve_bytes):
-            raise MemoryError(f"{slots} buffer pairs for {max_h}x{max_w} frames need "
-                              f"{pair_bytes} bytes; {free.value} are free")
+    batch.set_slots(ctx, max_slots)
+    if budget_bytes is None:
+        free, total = ctypes.c_size_t(), ctypes.c_size_t()
+        with ctx.lock:
+            ctx.check(lib.fx_mem_info(ctx.handle, ctypes.byref(free), ctypes.byref(total)))
+        budget_bytes = int(free.value) - reserve_bytes
+    report.budget_bytes = int(budget_bytes)
+    largest = max(frame_bytes(*r.pixels.shape[:2]) + 14 * int(r.pixels.shape[0])
+                  * int(r.pixels.shape[1]) for r in requests)
+    if largest > budget_bytes:
+        raise MemoryError(f"the largest request needs {largest} bytes of device memory; the "
+                          f"budget is {budget_bytes}")
     params = DEFAULT_PROFILE.hot_path_parameters().to_c()
-    ins = [torch.empty(max_h * max_w * 4, dtype=torch.int16, device="cuda") for _ in range(slots)]
-    outs = [torch.empty(max_h * max_w * 3, dtype=torch.int16, device="cuda") for _ in range(slots)]
-    free_pairs: deque[int] = deque(range(slots))
-    copy_stream = torch.cuda.Stream()
+    model = SlotModel(max_slots)
+    max_out = max(int(r.pixels.shape[0]) * int(r.pixels.shape[1]) * 3 for r in requests)
+    host_out = [torch.empty(max_out, dtype=torch.int16).pin_memory() for _ in range(max_slots)]
+    free_host = deque(range(max_slots))
+    up_stream, down_stream = torch.cuda.Stream(), torch.cuda.Stream()
+    check_stream = torch.cuda.Stream()
+    mismatches = torch.zeros((), dtype=torch.int64, device="cuda")
     waiting: deque[int] = deque()
-    staging: deque[tuple] = deque()  # (index, pair, event, admitted): uploads in flight, in order
-    inflight: dict[int, tuple] = {}  # ticket -> (index, admitted, pair)
+    staging: deque[dict] = deque()    # uploads in flight, in admission order
+    inflight: dict[int, dict] = {}    # ticket -> request state
+    downloads: deque[dict] = deque()  # outputs on their way to host memory
+    in_use_bytes = 0                  # planes of the requests in flight
     torch.cuda.synchronize()
     nxt = 0
     start = time.perf_counter()
@@ -126,63 +205,99 @@ def serve(ctx: _lib.Context, requests: Sequence[Request], *, slots: int = 4,
     def now() -> float:
         return time.perf_counter() - start
 
-    while nxt < len(requests) or waiting or staging or inflight:
+    while nxt < len(requests) or waiting or staging or inflight or downloads:
         t = now()
         while nxt < len(requests) and requests[nxt].arrival_s <= t:
             waiting.append(nxt)
             nxt += 1
-        # admission: a free buffer pair takes the next request's upload
-        while waiting and free_pairs:
-            i = waiting.popleft()
-            pair = free_pairs.popleft()
+        # admission, in arrival order: a slot (reused or new) and room
+        while waiting and free_host:
+            i = waiting[0]
+            h, w = (int(v) for v in requests[i].pixels.shape[:2])
+            planes = 14 * h * w
+            choice = model.choose(frame_bytes(h, w))
+            if choice is None:
+                break
+            kind, size = choice
+            extra = size if kind == "new" else 0
+            if model.allocated + extra + in_use_bytes + planes > budget_bytes:
+                break
+            waiting.popleft()
+            model.take(kind, size)
+            in_use_bytes += planes
             src = requests[i].pixels
             if isinstance(src, np.ndarray):
                 src = torch.from_numpy(np.ascontiguousarray(src, dtype=np.uint16).view(np.int16))
-            h, w = int(src.shape[0]), int(src.shape[1])
-            with torch.cuda.stream(copy_stream):
-                ins[pair][: h * w * 4].view(h, w, 4).copy_(src, non_blocking=True)
-                done = torch.cuda.Event()
-                done.record(copy_stream)
-            staging.append((i, pair, done, now()))
+            with torch.cuda.stream(up_stream):
+                d_in = torch.empty((h, w, 4), dtype=torch.int16, device="cuda")
+                d_out = torch.empty((h, w, 3), dtype=torch.int16, device="cuda")
+                d_in.copy_(src.view(h, w, 4), non_blocking=True)
+                landed = torch.cuda.Event()
+                landed.record(up_stream)
+            staging.append({"i": i, "h": h, "w": w, "d_in": d_in, "d_out": d_out,
+                            "event": landed, "admitted": now(), "size": size,
+                            "planes": planes, "host": free_host.popleft()})
+        report.max_in_flight = max(report.max_in_flight,
+                                   len(staging) + len(inflight) + len(downloads))
+        report.peak_bytes = max(report.peak_bytes, model.allocated + in_use_bytes)
         # submission: uploads that have landed go to a library slot
-        while staging and staging[0][2].query():
-            i, pair, _, admitted = staging[0]
-            src = requests[i].pixels
-            h, w = int(src.shape[0]), int(src.shape[1])
+        while staging and staging[0]["event"].query():
+            st = staging[0]
             ticket = ctypes.c_int64()
             with ctx.lock:
                 status = lib.fx_submit_device(
-                    ctx.handle, ctypes.c_void_p(ins[pair].data_ptr()), h, w,
+                    ctx.handle, ctypes.c_void_p(st["d_in"].data_ptr()), st["h"], st["w"],
                     ctypes.byref(params), None, NIKON_PE_INITIAL_STATE,
-                    ctypes.c_void_p(outs[pair].data_ptr()), None, None, ctypes.byref(ticket))
+                    ctypes.c_void_p(st["d_out"].data_ptr()), None, None, ctypes.byref(ticket))
             if status == batch.FX_PENDING:
                 break
             batch._check(ctx, status)
             staging.popleft()
-            inflight[ticket.value] = (i, admitted, pair)
-        # completions
-        finished = False
+            inflight[ticket.value] = st
+        # finished passes: counters, then the output's copy to host memory
         for ticket in list(inflight):
             with ctx.lock:
                 status = lib.fx_poll(ctx.handle, ticket)
             if status == batch.FX_PENDING:
                 continue
+            st = inflight.pop(ticket)
             counters = _lib.FxCounters()
-            status = lib.fx_wait(ctx.handle, ticket, -1, ctypes.byref(counters))
-            batch._check(ctx, status)
+            batch._check(ctx, lib.fx_wait(ctx.handle, ticket, -1, ctypes.byref(counters)))
+            st["counters"] = counters
+            n = st["h"] * st["w"] * 3
+            with torch.cuda.stream(down_stream):
+                host_out[st["host"]][:n].copy_(st["d_out"].view(-1), non_blocking=True)
+                st["event"] = torch.cuda.Event()
+                st["event"].record(down_stream)
+            expected = requests[st["i"]].expected
+            if expected is not None:
+                # the pass is complete (fx_wait returned): no stream order needed
+                with torch.cuda.stream(check_stream):
+                    mismatches.add_((st["d_out"] != expected.view(st["h"], st["w"], 3)).sum())
+                st["d_out"].record_stream(check_stream)
+                report.verified += 1
+            downloads.append(st)
+        finished = False
+        while downloads and downloads[0]["event"].query():
+            st = downloads.popleft()
             done_t = now()
-            i, admitted, pair = inflight.pop(ticket)
-            h, w = (int(v) for v in requests[i].pixels.shape[:2])
+            i, h, w = st["i"], st["h"], st["w"]
             output = None
             if keep_outputs:
-                output = outs[pair][: h * w * 3].view(h, w, 3).cpu().numpy().view(np.uint16)
-            free_pairs.append(pair)
-            report.completions.append(Completion(i, requests[i].arrival_s, admitted, done_t,
-                                                 counters, output))
+                n = h * w * 3
+                output = host_out[st["host"]][:n].numpy().view(np.uint16).reshape(h, w, 3).copy()
+            free_host.append(st["host"])
+            model.give_back(st["size"])
+            in_use_bytes -= st["planes"]
+            report.completions.append(Completion(i, requests[i].arrival_s, st["admitted"],
+                                                 done_t, st["counters"], output))
             report.megapixels += h * w / 1e6
             finished = True
         if not finished:
             time.sleep(0.0001)
     report.wall_s = now()
+    report.slots_used = max_slots - model.empty
+    check_stream.synchronize()
+    report.mismatches = int(mismatches.item())
     report.completions.sort(key=lambda c: c.index)
     return report

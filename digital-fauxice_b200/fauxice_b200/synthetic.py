@@ -48,6 +48,8 @@ NATIVE_FRAME = DefectSpec(discs=3000, disc_radius=(1, 20), scratches=60,
 # with floor-saturating blobs, many discs and long scratches.
 HEAVY_FRAME = DefectSpec(discs=9000, disc_radius=(1, 20), scratches=600,
                          scratch_length=(200, 4000), blobs=200)
+# Fraction of a frame's pixels the NATIVE_FRAME defects touch (measured).
+NATIVE_COVERAGE = 0.06
 # Heavy damage at full size: about 5% of the pixels, most of it 200 blobs of
 # radius U[20,60] whose IR keeps only 1-10% (scores saturate at the floor),
 # plus long crossing scratches and some discs.
@@ -205,6 +207,23 @@ def heavy_full_frame(index: int, base_seed: int = 200) -> tuple[np.ndarray, np.n
 
     main = make_frame(base_seed + index, FULL_FRAME[0], FULL_FRAME[1], HEAVY_FULL)
     return main, make_prepass(main)
+
+
+def coverage_frame(seed: int, height: int, width: int, coverage: float) -> np.ndarray:
+    """A frame from the native generator with its defect counts scaled to a
+    target coverage, the fraction of pixels a defect touches: the serving
+    workload draws each request's coverage from U[0.1%, 3%].  The native
+    spec's counts touch about 6% of a frame (NATIVE_COVERAGE, measured on
+    this generator), and coverage grows about linearly with the counts in
+    this range."""
+
+    base = scaled_spec(NATIVE_FRAME, height, width)
+    factor = coverage / NATIVE_COVERAGE
+    spec = DefectSpec(discs=max(1, int(round(base.discs * factor))),
+                      disc_radius=base.disc_radius,
+                      scratches=max(1, int(round(base.scratches * factor))),
+                      scratch_length=base.scratch_length)
+    return make_frame(seed, height, width, spec)
 
 
 def crop_origins(height: int, width: int, size: int, count: int, base_seed: int = 1000):

@@ -23,3 +23,20 @@ def test_report_percentiles_and_throughput():
     assert s["requests"] == 4 and s["mp_per_s"] == 50.0
     assert s["p50_ms"] == 25.0
     assert s["p50_ms"] <= s["p95_ms"] <= s["p99_ms"] <= 40.0
+
+
+def test_slot_model_reuses_the_smallest_fitting_buffers():
+    model = serve.SlotModel(2)
+    assert model.choose(100) == ("new", 100)
+    model.take("new", 100)
+    assert model.choose(300) == ("new", 300)
+    model.take("new", 300)
+    assert model.allocated == 400 and model.empty == 0
+    assert model.choose(50) is None  # both slots busy
+    model.give_back(300)
+    model.give_back(100)
+    assert model.choose(50) == ("reuse", 100)
+    assert model.choose(200) == ("reuse", 300)
+    assert model.choose(400) is None  # no slot holds it and none is empty
+    model.take("reuse", 100)
+    assert model.free_sizes == [300] and model.allocated == 400
