@@ -191,6 +191,8 @@ def parse():
                     help="arrival window per request rate (the workload's 120 s, shortened)")
     ap.add_argument("--serve-rates", default=",".join(f"{r:g}" for r in SERVE_RATES),
                     help="comma-separated Poisson request rates per second")
+    ap.add_argument("--stencil-tile", type=int, default=0,
+                    help="stencil tile rows of the plain path (8 or 16; 0: library default)")
     ap.add_argument("--plan-only", action="store_true",
                     help="print each rank's work plan after the collectives; no GPU work")
     return ap.parse_args()
@@ -420,6 +422,7 @@ def run_b200(args, world, rank, local, frames=None, heavy=None, pool=None):
     h, w = main.shape[:2]
     lib = _lib.load()
     ctx = engine.context(local)
+    ctx.check(lib.fx_set_stencil_tile(ctx.handle, args.stencil_tile))
     params = DEFAULT_PROFILE.hot_path_parameters().to_c()
     d_in = torch.from_numpy(main.view(np.int16)).to(f"cuda:{local}")
     d_out = torch.empty((h, w, 3), dtype=torch.int16, device=f"cuda:{local}")
@@ -668,17 +671,23 @@ def run_batched(ctx, frames, args, golden):
             times.append(time.perf_counter() - t0)
         return min(times), sorted(times)[len(times) // 2]
 
+    import tempfile
+
     batch.set_walk_wave(ctx, 0)
     batch.run_device_batch(ctx, as_jobs(plain_out), slots=1)  # warm
     plain_best, plain_med = timed(as_jobs(plain_out), 1)
-    (slots, wave), tuning = batch.tune_slots(ctx, as_jobs(outs), candidates=(2, 4, 8),
-                                             waves=(0, 148))
+    with tempfile.TemporaryDirectory() as tmp:  # always measured here, never from a cache
+        entry, _ = batch.autotune(ctx, as_jobs(outs), candidates=(2, 4, 8), waves=(0, 148),
+                                  tiles=(8, 16), cache_path=os.path.join(tmp, "tuning.json"),
+                                  retune=True)
+    slots, wave, tile = entry["slots"], entry["walk_wave"], entry["stencil_tile"]
     best, med = timed(as_jobs(outs), slots)
     same = all(torch.equal(a, b) for a, b in zip(outs, plain_out))
     digests = [hashlib.sha256(o.cpu().numpy().view(np.uint16).astype("<u2").tobytes()).hexdigest()
                for o in outs]
     ref_ok = [digests[i] == golden["jobs"][f"batch_{i}"]["output_sha256"] for i in range(5)]
     batch.set_walk_wave(ctx, 0)
+    batch.set_stencil_tile(ctx, 0)
     return {
         "_digests": digests,
         "workload": f"{len(frames)} frames cycling 5782x3946, 3946x5782, 2892x1973, 1024x768, "
@@ -687,9 +696,11 @@ def run_batched(ctx, frames, args, golden):
         "ms_per_step": round(1000 * med, 2), "steps": args.batch_steps,
         "plain_same_mix": {"value": round(mp / plain_med, 1), "unit": "MP/s",
                            "ms_per_step": round(1000 * plain_med, 2), "slots": 1},
-        "slots": slots, "walk_wave": wave or f"default ({WALK_BLOCKS_PER_SM} per SM)",
-        "tuning_ms": {f"slots={k[0]},wave={k[1] or 'default'}": round(1000 * v, 1)
-                      for k, v in tuning.items()},
+        "slots": slots, "walk_wave": wave, "stencil_tile": tile,
+        "tuning_ms": {f"slots={k.split(',')[0]},wave={k.split(',')[1]},tile={k.split(',')[2]}": v
+                      for k, v in entry["timings_ms"].items()},
+        "autotuner": "fauxice_b200.batch.autotune (slots x walk wave x stencil tile; JSON cache "
+                     "keyed by device and frame shapes; remeasured for this run)",
         "timing": "host clock around the whole batch, synchronize on both sides (frames run on "
                   "several library streams)",
         "bit_exact_vs_single_frame": bool(same),
@@ -718,7 +729,8 @@ def run_heavy(ctx, frames, args, golden, batched):
     jobs = lambda dst: [batch.DeviceFrame(d.data_ptr(), f.shape[0], f.shape[1], o.data_ptr())
                         for f, d, o in zip(frames, d_in, dst)]
     slots = batched["slots"] if batched else 4
-    wave = batched["walk_wave"] if batched and isinstance(batched["walk_wave"], int) else 0
+    wave = batched["walk_wave"] if batched else 0
+    tile = batched["stencil_tile"] if batched else 0
 
     def timed(dst, n_slots):
         times = []
@@ -734,8 +746,10 @@ def run_heavy(ctx, frames, args, golden, batched):
     batch.run_device_batch(ctx, jobs(plain_out), slots=1)  # warm
     plain_med, _ = timed(plain_out, 1)
     batch.set_walk_wave(ctx, wave)
+    batch.set_stencil_tile(ctx, tile)
     med, counters = timed(outs, slots)
     batch.set_walk_wave(ctx, 0)
+    batch.set_stencil_tile(ctx, 0)
     same = all(torch.equal(a, b) for a, b in zip(outs, plain_out))
     ref_ok = []
     for i in range(2):
@@ -750,7 +764,7 @@ def run_heavy(ctx, frames, args, golden, batched):
         "ms_per_step": round(1000 * med, 2), "steps": args.batch_steps,
         "plain_same_mix": {"value": round(mp / plain_med, 1), "unit": "MP/s",
                            "ms_per_step": round(1000 * plain_med, 2), "slots": 1},
-        "slots": slots, "walk_wave": wave or "default",
+        "slots": slots, "walk_wave": wave, "stencil_tile": tile or 8,
         "attempted_pixels": int(sum(c.attempted for c in counters)),
         "rng_dependent_channels": int(sum(c.rng_dependent for c in counters)),
         "timing": "host clock around the whole batch, synchronize on both sides",

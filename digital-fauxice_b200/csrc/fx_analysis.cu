@@ -39,12 +39,14 @@ __device__ __forceinline__ float aux_value(const uint2 raw, const fx_stage &st, 
 // One padded row segment of the history planes (streaming.py:111-147,
 // 201-233), with the auxiliary plane computed on the way: each thread
 // computes the aux of its own column (the edge threads also their outer
-// neighbour's, for the horizontal minimum) and writes it once for the real
-// pixels.  Rows above the image take the pseudo row, rows below repeat the
-// last row, columns outside are zero.
+// neighbour's, for the horizontal minimum).  History planes: rows above the
+// image take the pseudo row, rows below repeat the last row, columns outside
+// are zero.  The auxiliary plane is written padded too, but edge-replicated
+// (the decision bars clamp their indices, streaming.py:166-198): padded
+// (y, x) holds the aux of (clamp(y), clamp(x)).
 __global__ void __launch_bounds__(256)
     k_planes(const uint16_t *__restrict__ rgbi, Geometry g, const float *__restrict__ lut,
-             const fx_stage *__restrict__ stages, fx_params p, float *__restrict__ aux,
+             const fx_stage *__restrict__ stages, fx_params p, float *__restrict__ auxp,
              float *__restrict__ hs, float *__restrict__ hwa, float *__restrict__ hwr,
              int64_t plane, uint32_t *err) {
     __shared__ float s_aux[256 + 2];  // aux of columns x-1 .. x+256 of the segment
@@ -56,13 +58,20 @@ __global__ void __launch_bounds__(256)
     const int r = y < 0 ? 0 : (y < g.h ? y : g.h - 1);
     const int64_t row0 = (int64_t)r * g.w;
     const fx_stage ast = stages[r];  // stage y+1 (stage_parameters.py:207-212)
-    const bool own = live && px < g.pitch && x >= 0 && x < g.w;
+    const bool inside = x >= 0 && x < g.w;
+    const bool own = live && px < g.pitch && inside;
     uint2 raw = make_uint2(0u, 0u);
     float a = 0.0f;
-    if (own) {
-        raw = reinterpret_cast<const uint2 *>(rgbi)[row0 + x];
-        a = aux_value(raw, ast, p.visible_channel, lut, err);
-        if (y >= 0 && y < g.h) aux[row0 + x] = a;
+    if (px < g.pitch) {
+        // the aux of (clamp(y), clamp(x)), for the edge-replicated plane
+        const int xc = x < 0 ? 0 : (x < g.w ? x : g.w - 1);
+        const uint2 rc = reinterpret_cast<const uint2 *>(rgbi)[row0 + xc];
+        const float ac = aux_value(rc, ast, p.visible_channel, lut, err);
+        auxp[(int64_t)py * g.pitch + px] = ac;
+        if (own) {
+            raw = rc;
+            a = ac;
+        }
     }
     s_aux[threadIdx.x + 1] = a;
     if (threadIdx.x == 0 || threadIdx.x == blockDim.x - 1) {
@@ -187,6 +196,26 @@ __device__ __forceinline__ void q69_q21(S3 s3, S5 s5, S7 s7, S9 s9, double &q69,
     q21 = t21 * (double)(float)(1.0 / 21.0);
 }
 
+// The two halves of q69_q21, each in the same operation order.
+template <class S5, class S7, class S9>
+__device__ __forceinline__ double q69_only(S5 s5, S7 s7, S9 s9) {
+    double t69 = (double)s5(8) + (double)s5(0);
+    t69 += (double)s7(1);
+    t69 += (double)s7(7);
+#pragma unroll
+    for (int x = 2; x < 7; ++x) t69 += (double)s9(x);
+    return t69 * (double)(float)(1.0 / 69.0);
+}
+
+template <class S3, class S5>
+__device__ __forceinline__ double q21_only(S3 s3, S5 s5) {
+    double t21 = (double)s3(6) + (double)s3(2);
+    t21 += (double)s5(3);
+    t21 += (double)s5(4);
+    t21 += (double)s5(5);
+    return t21 * (double)(float)(1.0 / 21.0);
+}
+
 template <class B>
 __device__ __forceinline__ double q16_wa(B b16) {
     double t = (double)b16(4) + (double)b16(3);
@@ -213,13 +242,27 @@ __device__ __forceinline__ double q16_rgb(A at) {
     return total * (double)(float)(1.0 / 16.0);
 }
 
-// recovered_rgb_candidates (reconstruction.py:425-462), UNNORMALIZED_SUM.
-__device__ __forceinline__ float rgb_candidate(double avg, float weight) {
-    if (weight > 0.0f) {
-        const double reciprocal = 1.0 / (double)weight;
-        return (float)(avg * reciprocal);
+// recovered_rgb_candidates (reconstruction.py:425-462), UNNORMALIZED_SUM:
+// C_k = f32(Q_k * (1.0 / f64(W_k))) when W_k > 0, else f32(Q_k).  The
+// reciprocal depends only on the weight, so it is computed once per weight
+// and shared by the three channels (the same value every time).
+struct Reciprocals {
+    double r[3];
+    bool pos[3];
+};
+
+__device__ __forceinline__ Reciprocals weight_reciprocals(const float weights[4]) {
+    Reciprocals o;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        o.pos[k] = weights[k] > 0.0f;
+        o.r[k] = o.pos[k] ? 1.0 / (double)weights[k] : 0.0;
     }
-    return (float)avg;
+    return o;
+}
+
+__device__ __forceinline__ float rgb_candidate(double avg, const Reciprocals &rc, int k) {
+    return rc.pos[k] ? (float)(avg * rc.r[k]) : (float)avg;
 }
 
 // The combiner's and writer's float32 profile constants, widened once on the
@@ -388,94 +431,118 @@ __device__ uint8_t classify_site(const double cand[3], const float orig[3], bool
 // The stencil
 // ---------------------------------------------------------------------------
 
-constexpr int PR = kTileH + 10;   // history tile rows (y0-5 .. y0+TH+4)
-constexpr int PC = kTileW + 10;   // history tile cols (x0-5 .. x0+TW+4)
-constexpr int RR = kTileH + 8;    // rgb / decision tile rows (y0-4 ..)
-constexpr int RC = kTileW + 8;    // rgb / decision tile cols (x0-4 ..)
-constexpr int CR = kTileH + 2;    // record rows (y0-1 .. y0+TH)
-constexpr int CC = kTileW + 10;   // column-sum cols (x0-5 .. x0+TW+4)
-constexpr int RECC = kTileW + 2;  // record cols (x0-1 .. x0+TW)
-constexpr int kStencilThreads = kTileH * kTileW;
+// Tile geometry for a tile of TH pixel rows by 32 pixel columns.  Every plane
+// tile is staged with 16-byte cp.async copies from a 16-byte aligned origin:
+// padded column x0 (x0 a multiple of 32, the pitch a multiple of 32 floats),
+// 44 floats (11 vectors) per row.
+template <int TH>
+struct Tile {
+    static constexpr int TW = 32;
+    static constexpr int THREADS = TH * TW;
+    static constexpr int PR = TH + 10;   // history tile rows (y0-5 .. y0+TH+4)
+    static constexpr int PC = TW + 10;   // history tile cols used (x0-5 .. x0+TW+4)
+    static constexpr int RR = TH + 8;    // rgb / decision tile rows (y0-4 ..)
+    static constexpr int RC = TW + 8;    // rgb / decision tile cols used (x0-4 ..)
+    static constexpr int CR = TH + 2;    // record rows (y0-1 .. y0+TH)
+    static constexpr int CC = TW + 10;   // column-sum cols (x0-5 .. x0+TW+4)
+    static constexpr int RECC = TW + 2;  // record cols (x0-1 .. x0+TW)
+    static constexpr int SW = 44;        // staged floats per row (11 x 16 bytes)
+    static constexpr int RO = 1;         // staged column of rgb / decision col 0
+    static constexpr int WA_RUN = TH == 8 ? 5 : 6;  // score / waux column-sum run
+    static constexpr int RGB_RUN = 4;               // rgb column-sum run
+    static constexpr int BLOCKS_PER_SM = TH == 8 ? 4 : 2;
+};
 
+template <int TH>
 struct StencilSmem {
-    float hs[PR][PC];
-    float hwa[PR][PC];
-    float hwr[3][RR][RC];
-    float cs[2][5][CR][CC];       // [score|waux][S3,S5,S7,S9,B16]
-    float rcs[3][4][kTileH][RC];  // [channel][S3,S5,S7,S9]
-    Record rec[CR][RECC];
+    using T = Tile<TH>;
+    float hs[T::PR][T::SW];
+    float hwa[T::PR][T::SW];
+    float hwr[3][T::RR][T::SW];                 // staged column j: logical col j - RO
+    float cs[2][5][T::CR][T::CC];               // [score|waux][S3,S5,S7,S9,B16]
+    float rcs[3][4][TH][T::RC];                 // [channel][S3,S5,S7,S9]
+    Record rec[T::CR][T::RECC];
     union {
-        // aux at clamped (y0-4+r, x0-4+c): decision masks and point aux,
+        // aux at clamped (y0-4+r, x0-5+j): decision masks and point aux,
         // dead once the records are built
-        float auxt[RR][RC];
+        float auxt[T::RR][T::SW];
         struct {  // the attempted-pixel list of the per-pixel phase
-            uint32_t wcount[kStencilThreads / 32];
+            uint32_t wcount[T::THREADS / 32];
             int n_attempted;
-            uint16_t attempted[kStencilThreads];  // thread index of each attempted pixel
+            uint16_t attempted[T::THREADS];  // thread index of each attempted pixel
         } dec;
     };
-    unsigned long long rowlow[RR];  // bit c: auxt[r][c] below the decision threshold
-    uint32_t collow[RC];            // bit r: the same, by column
-    uint32_t rowbal[kTileH];        // bit x: pixel (row, x) of the tile is attempted
+    unsigned long long rowlow[T::RR];  // bit c: aux (row r, col c) below the threshold
+    uint32_t collow[T::RC];            // bit r: the same, by column
+    uint32_t rowbal[TH];               // bit x: pixel (row, x) of the tile is attempted
 };
-// four blocks per SM: 228 KB less 1 KB reserved per block
-static_assert(sizeof(StencilSmem) <= 57344, "the stencil tile keeps four blocks per SM");
-static_assert(kTileW == 32, "one warp per pixel row of the stencil tile");
-static_assert(sizeof(float) * RR * RC >= 4 * (kStencilThreads / 32 + 1) + 2 * kStencilThreads,
+// four 8-row blocks per SM (228 KB less 1 KB reserved per block); two 16-row
+static_assert(sizeof(StencilSmem<8>) <= 57344, "the 8-row tile keeps four blocks per SM");
+static_assert(sizeof(StencilSmem<16>) <= 115712, "the 16-row tile keeps two blocks per SM");
+static_assert(Tile<8>::RR <= 32 && Tile<16>::RR <= 32, "column masks are 32 bits");
+static_assert(sizeof(float) * Tile<16>::RR * Tile<16>::SW >=
+                  4 * (Tile<16>::THREADS / 32 + 1) + 2 * Tile<16>::THREADS,
               "the attempted list fits in the aux tile");
+static_assert(sizeof(float) * Tile<8>::RR * Tile<8>::SW >=
+                  4 * (Tile<8>::THREADS / 32 + 1) + 2 * Tile<8>::THREADS,
+              "the attempted list fits in the aux tile");
+static_assert(kTileH % 16 == 0, "padded planes cover whole tiles of either height");
 
-__global__ void __launch_bounds__(kStencilThreads, 4)
+template <int TH>
+__global__ void __launch_bounds__(Tile<TH>::THREADS, Tile<TH>::BLOCKS_PER_SM)
     k_stencil(const uint16_t *__restrict__ rgbi, Geometry g, const float *__restrict__ lut,
               const fx_stage *__restrict__ stages, fx_params p, CombineConst cc,
-              const float *__restrict__ aux, const float *__restrict__ hs,
+              const float *__restrict__ auxp, const float *__restrict__ hs,
               const float *__restrict__ hwa, const float *__restrict__ hwr, int64_t plane,
               double *__restrict__ cand_out, uint8_t *__restrict__ meta_out, uint32_t *err) {
+    using T = Tile<TH>;
+    constexpr int PR = T::PR, RR = T::RR, RC = T::RC, CR = T::CR, CC = T::CC;
+    constexpr int RECC = T::RECC, RO = T::RO, NT = T::THREADS;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    StencilSmem &S = *reinterpret_cast<StencilSmem *>(smem_raw);
+    StencilSmem<TH> &S = *reinterpret_cast<StencilSmem<TH> *>(smem_raw);
     if (pass_stopped(err)) return;
     const int tid = threadIdx.x;
-    const int y0 = blockIdx.y * kTileH, x0 = blockIdx.x * kTileW;
+    const int y0 = blockIdx.y * TH, x0 = blockIdx.x * T::TW;
     const int h = g.h, w = g.w;
 
     // ---- stage the tile ---------------------------------------------------
-    // Every element goes through cp.async, so all of a thread's requests
-    // are in flight at once; one wait then covers the whole tile.
-    auto cp4 = [](void *dst, const void *src) {
-        const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(src));
-    };
-    for (int i = tid; i < PR * PC; i += kStencilThreads) {
-        const int r = i / PC, c = i % PC;
-        const int64_t o = (int64_t)(y0 + r) * g.pitch + (x0 + c);  // padded (y0-5+r, x0-5+c)
-        cp4(&S.hs[r][c], hs + o);
-        cp4(&S.hwa[r][c], hwa + o);
+    // 16-byte copies, 11 per staged row: rows 0..PR-1 score, PR..2PR-1 waux
+    // (padded rows y0..), then 3 x RR rgb rows and RR aux rows (padded rows
+    // y0+1..).  All requests are in flight at once; one wait covers them.
+    {
+        constexpr int kRows = 2 * PR + 4 * RR, kVec = T::SW / 4;
+        const int64_t col = x0;
+        for (int i = tid; i < kRows * kVec; i += NT) {
+            const int row = i / kVec, v = i % kVec;
+            const float *src;
+            float *dst;
+            if (row < 2 * PR) {
+                const int r = row < PR ? row : row - PR;
+                src = (row < PR ? hs : hwa) + (int64_t)(y0 + r) * g.pitch + col;
+                dst = row < PR ? S.hs[r] : S.hwa[r];
+            } else {
+                const int q = row - 2 * PR, k = q / RR, r = q % RR;  // k 0..2 rgb, 3 aux
+                src = (k < 3 ? hwr + k * plane : auxp) + (int64_t)(y0 + 1 + r) * g.pitch + col;
+                dst = k < 3 ? S.hwr[k][r] : S.auxt[r];
+            }
+            const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst + 4 * v);
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src + 4 * v));
+        }
+        asm volatile("cp.async.commit_group;\n" ::);
+        asm volatile("cp.async.wait_group 0;\n" ::);
     }
-    for (int i = tid; i < 3 * RR * RC; i += kStencilThreads) {
-        const int ch = i / (RR * RC), rem = i % (RR * RC);
-        const int r = rem / RC, c = rem % RC;
-        cp4(&S.hwr[ch][r][c], hwr + ch * plane + (int64_t)(y0 + 1 + r) * g.pitch + (x0 + 1 + c));
-    }
-    for (int i = tid; i < RR * RC; i += kStencilThreads) {
-        const int r = i / RC, c = i % RC;
-        int yy = y0 - 4 + r, xx = x0 - 4 + c;
-        yy = yy < 0 ? 0 : (yy > h - 1 ? h - 1 : yy);
-        xx = xx < 0 ? 0 : (xx > w - 1 ? w - 1 : xx);
-        cp4(&S.auxt[r][c], aux + (int64_t)yy * w + xx);
-    }
-    asm volatile("cp.async.commit_group;\n" ::);
-    asm volatile("cp.async.wait_group 0;\n" ::);
     const float thr = p.decision_threshold;
     __syncthreads();
 
     // ---- decision masks and vertical column sums ---------------------------
     if (tid < RR) {
         unsigned long long m = 0;
-        for (int c = 0; c < RC; ++c) m |= (unsigned long long)(S.auxt[tid][c] < thr) << c;
+        for (int c = 0; c < RC; ++c) m |= (unsigned long long)(S.auxt[tid][c + RO] < thr) << c;
         S.rowlow[tid] = m;
     } else if (tid >= 32 && tid < 32 + RC) {
         const int c = tid - 32;
         uint32_t m = 0;
-        for (int r = 0; r < RR; ++r) m |= (uint32_t)(S.auxt[r][c] < thr) << r;
+        for (int r = 0; r < RR; ++r) m |= (uint32_t)(S.auxt[r][c + RO] < thr) << r;
         S.collow[c] = m;
     }
     __syncthreads();
@@ -484,7 +551,7 @@ __global__ void __launch_bounds__(kStencilThreads, 4)
     // It needs only the aux masks, the point score and the stage gates, so it
     // comes first: a tile without an attempted pixel stops here, and the
     // others build only the records their attempted pixels read.
-    const int dty = tid / kTileW, dtx = tid % kTileW;
+    const int dty = tid / T::TW, dtx = tid % T::TW;
     bool eligible = false;
     {
         const int y = y0 + dty, x = x0 + dtx;
@@ -508,7 +575,7 @@ __global__ void __launch_bounds__(kStencilThreads, 4)
                 eligible = false;
             if (!eligible) meta_out[6 * (int64_t)w + (int64_t)y * w + x] = 0;
         }
-        // a warp is one pixel row of the tile (kTileW == 32)
+        // a warp is one pixel row of the tile (32 columns)
         const uint32_t bal = __ballot_sync(0xFFFFFFFFu, eligible);
         if (dtx == 0) S.rowbal[dty] = bal;
     }
@@ -516,19 +583,21 @@ __global__ void __launch_bounds__(kStencilThreads, 4)
 
     // One work item is a vertical run of column sums in one column: the
     // samples are loaded and widened once and shared by the run's chains.
-    // Items 0..167: score / waux planes, runs of 5 record rows; items
-    // 168..407: the three RGB planes, runs of 4 pixel rows.
-    constexpr int kWaItems = 2 * CC * 2, kRgbItems = 3 * RC * 2;
-    for (int it = tid; it < kWaItems + kRgbItems; it += kStencilThreads) {
+    // Items below kWaItems: score / waux planes, runs of WA_RUN record rows;
+    // the rest: the three RGB planes, runs of RGB_RUN pixel rows.
+    constexpr int WR = T::WA_RUN, GR = T::RGB_RUN;
+    static_assert(CR % WR == 0 && TH % GR == 0, "runs tile the rows");
+    constexpr int kWaItems = 2 * CC * (CR / WR), kRgbItems = 3 * RC * (TH / GR);
+    for (int it = tid; it < kWaItems + kRgbItems; it += NT) {
         if (it < kWaItems) {
-            const int src = it / (2 * CC), rem = it % (2 * CC);
-            const int c = rem % CC, r0 = (rem / CC) * 5;  // lanes on consecutive columns
-            const float(*pl)[PC] = src ? S.hwa : S.hs;
-            double v[13];
+            const int src = it / (CC * (CR / WR)), rem = it % (CC * (CR / WR));
+            const int c = rem % CC, r0 = (rem / CC) * WR;  // lanes on consecutive columns
+            const float(*pl)[T::SW] = src ? S.hwa : S.hs;
+            double v[WR + 8];
 #pragma unroll
-            for (int k = 0; k < 13; ++k) v[k] = (double)pl[r0 + k][c];
+            for (int k = 0; k < WR + 8; ++k) v[k] = (double)pl[r0 + k][c];
 #pragma unroll
-            for (int j = 0; j < 5; ++j) {
+            for (int j = 0; j < WR; ++j) {
                 const ColumnSums cs = column_sums_wide(v + j);
                 S.cs[src][0][r0 + j][c] = cs.s3;
                 S.cs[src][1][r0 + j][c] = cs.s5;
@@ -538,13 +607,13 @@ __global__ void __launch_bounds__(kStencilThreads, 4)
             }
         } else {
             const int q = it - kWaItems;
-            const int ch = q / (2 * RC), rem = q % (2 * RC);
-            const int c = rem % RC, r0 = (rem / RC) * 4;
-            double v[12];
+            const int ch = q / (RC * (TH / GR)), rem = q % (RC * (TH / GR));
+            const int c = rem % RC, r0 = (rem / RC) * GR;
+            double v[GR + 8];
 #pragma unroll
-            for (int k = 0; k < 12; ++k) v[k] = (double)S.hwr[ch][r0 + k][c];
+            for (int k = 0; k < GR + 8; ++k) v[k] = (double)S.hwr[ch][r0 + k][c + RO];
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
+            for (int j = 0; j < GR; ++j) {
                 const ColumnSums cs = column_sums_wide(v + j);
                 S.rcs[ch][0][r0 + j][c] = cs.s3;
                 S.rcs[ch][1][r0 + j][c] = cs.s5;
@@ -556,16 +625,16 @@ __global__ void __launch_bounds__(kStencilThreads, 4)
     __syncthreads();
 
     // ---- feature records (streaming.py:236-308) ---------------------------
-    for (int i = tid; i < CR * RECC; i += kStencilThreads) {
+    for (int i = tid; i < CR * RECC; i += NT) {
         const int r = i / RECC, c = i % RECC;
         {   // read by an attempted pixel: record row r is the centre row of
             // pixel row r-1 and the cross neighbour of pixel rows r and r-2
             unsigned long long need = 0;
-            if (r >= 1 && r <= kTileH) {
+            if (r >= 1 && r <= TH) {
                 const unsigned long long b = S.rowbal[r - 1];
                 need |= b | (b << 1) | (b << 2);
             }
-            if (r < kTileH) need |= (unsigned long long)S.rowbal[r] << 1;
+            if (r < TH) need |= (unsigned long long)S.rowbal[r] << 1;
             if (r >= 2) need |= (unsigned long long)S.rowbal[r - 2] << 1;
             if (!((need >> c) & 1ull)) continue;
         }
@@ -606,7 +675,7 @@ __global__ void __launch_bounds__(kStencilThreads, 4)
                 }
             }
             if (point_score > 0.0f) {
-                rec.a[3] = S.auxt[r + 3][c + 3];  // xx is inside the row here
+                rec.a[3] = S.auxt[r + 3][c + 3 + RO];  // xx is inside the row here
             } else {
                 rec.a[3] = 0.0f;
                 rec.fb |= 8u;
@@ -626,7 +695,7 @@ __global__ void __launch_bounds__(kStencilThreads, 4)
         __syncthreads();
         uint32_t base = 0, total = 0;
 #pragma unroll
-        for (int k = 0; k < kStencilThreads / 32; ++k) {
+        for (int k = 0; k < NT / 32; ++k) {
             const uint32_t c = S.dec.wcount[k];
             base += k < (tid >> 5) ? c : 0u;
             total += c;
@@ -640,7 +709,7 @@ __global__ void __launch_bounds__(kStencilThreads, 4)
     const int listed = S.dec.n_attempted;
     if (tid >= listed) return;
     const int me = S.dec.attempted[tid];
-    const int ty = me / kTileW, tx = me % kTileW;
+    const int ty = me / T::TW, tx = me % T::TW;
     const int y = y0 + ty, x = x0 + tx;
     const int64_t site = 6 * (int64_t)w + (int64_t)y * w + x;
     const uint2 raw = reinterpret_cast<const uint2 *>(rgbi)[(int64_t)y * w + x];
@@ -679,23 +748,32 @@ __global__ void __launch_bounds__(kStencilThreads, 4)
         weights[3] = S.hs[ty + 5][tx + 5];  // point score
     }
 
-    // RGB candidates (reconstruction.py:425-462)
+    // RGB candidates (reconstruction.py:425-462), one weight at a time: its
+    // reciprocal serves the three channels
     float cand[3][3];
 #pragma unroll
-    for (int ch = 0; ch < 3; ++ch) {
-        const float(*s3)[RC] = S.rcs[ch][0];
-        const float(*s5)[RC] = S.rcs[ch][1];
-        const float(*s7)[RC] = S.rcs[ch][2];
-        const float(*s9)[RC] = S.rcs[ch][3];
-        double q69, q21;
-        q69_q21([&](int k) { return s3[ty][tx + k]; }, [&](int k) { return s5[ty][tx + k]; },
-                [&](int k) { return s7[ty][tx + k]; }, [&](int k) { return s9[ty][tx + k]; }, q69,
-                q21);
-        const float(*pl)[RC] = S.hwr[ch];
-        const double q16 = q16_rgb([&](int i, int j) { return pl[ty + 3 + i][tx + 3 + j]; });
-        cand[0][ch] = rgb_candidate(q69, weights[0]);
-        cand[1][ch] = rgb_candidate(q21, weights[1]);
-        cand[2][ch] = rgb_candidate(q16, weights[2]);
+    for (int k = 0; k < 3; ++k) {
+        const bool pos = weights[k] > 0.0f;
+        const double recip = pos ? 1.0 / (double)weights[k] : 0.0;
+#pragma unroll
+        for (int ch = 0; ch < 3; ++ch) {
+            const float(*s3)[RC] = S.rcs[ch][0];
+            const float(*s5)[RC] = S.rcs[ch][1];
+            const float(*s7)[RC] = S.rcs[ch][2];
+            const float(*s9)[RC] = S.rcs[ch][3];
+            const float(*pl)[T::SW] = S.hwr[ch];
+            double q;
+            if (k == 0)
+                q = q69_only([&](int j) { return s5[ty][tx + j]; },
+                             [&](int j) { return s7[ty][tx + j]; },
+                             [&](int j) { return s9[ty][tx + j]; });
+            else if (k == 1)
+                q = q21_only([&](int j) { return s3[ty][tx + j]; },
+                             [&](int j) { return s5[ty][tx + j]; });
+            else
+                q = q16_rgb([&](int i, int j) { return pl[ty + 3 + i][tx + 3 + j + RO]; });
+            cand[k][ch] = pos ? (float)(q * recip) : (float)q;
+        }
     }
     double combined[3];
     if (!combine(cand, orig, weights, feats, records, ws.coarse, p, cc, combined)) {
@@ -730,10 +808,11 @@ __device__ __forceinline__ float su_plane(const StartupView &v, const float *pl,
     return pl[v.g.padded_index(y, x)];
 }
 
-// Raw decision history (startup.py:119-126) at padded column xp = x + 4.
+// Raw decision history (startup.py:119-126) at padded column xp = x + 4,
+// read from the edge-replicated padded aux plane.
 __device__ __forceinline__ float su_raw(const StartupView &v, int y, int xp) {
     const int w = v.g.w;
-    const float *src = v.aux + (int64_t)(y < 0 ? 0 : y) * w;
+    const float *src = v.aux + v.g.padded_index(y < 0 ? 0 : y, 0);
     if (xp < 4) return src[0];
     if (xp < 4 + w) return src[xp - 4];
     return y >= 0 ? src[w - 1] : 0.0f;
@@ -814,6 +893,7 @@ __global__ void k_startup(const uint16_t *__restrict__ rgbi, StartupView v,
         meta_out[site] = 0;
         return;
     }
+    const Reciprocals rcp = weight_reciprocals(weights);
     float cand[3][3];
 #pragma unroll
     for (int ch = 0; ch < 3; ++ch) {
@@ -831,9 +911,9 @@ __global__ void k_startup(const uint16_t *__restrict__ rgbi, StartupView v,
                 [&](int kk) { return cs[kk].s7; }, [&](int kk) { return cs[kk].s9; }, q69, q21);
         const double q16 = q16_rgb(
             [&](int i, int j) { return su_plane(v, pl, center - 1 + i, x - 1 + j); });
-        cand[0][ch] = rgb_candidate(q69, weights[0]);
-        cand[1][ch] = rgb_candidate(q21, weights[1]);
-        cand[2][ch] = rgb_candidate(q16, weights[2]);
+        cand[0][ch] = rgb_candidate(q69, rcp, 0);
+        cand[1][ch] = rgb_candidate(q21, rcp, 1);
+        cand[2][ch] = rgb_candidate(q16, rcp, 2);
     }
     const int records = p.cross_neighbor ? 5 : 1;
     if (records == 5) {
@@ -869,7 +949,8 @@ __global__ void k_startup(const uint16_t *__restrict__ rgbi, StartupView v,
 cudaError_t launch_analysis(const uint16_t *rgbi, const Geometry &g, const float *lut,
                             const fx_stage *stages, const fx_params &p, float *aux, float *hs,
                             float *hwa, float *hwr, int64_t plane, double *cand, uint8_t *meta,
-                            uint32_t *err, cudaStream_t stream, const Marks &marks) {
+                            uint32_t *err, cudaStream_t stream, const Marks &marks,
+                            int tile_rows) {
     const CombineConst cc = combine_const(p);
     {
         dim3 block(256), grid((g.pitch + 255) / 256, g.prow);
@@ -877,9 +958,13 @@ cudaError_t launch_analysis(const uint16_t *rgbi, const Geometry &g, const float
                                              err);
     }
     marks.mark(2, stream);
-    {
-        dim3 grid(g.tw, g.th);
-        k_stencil<<<grid, kStencilThreads, sizeof(StencilSmem), stream>>>(
+    if (tile_rows == 16) {
+        dim3 grid(g.tw, g.hp / 16);
+        k_stencil<16><<<grid, Tile<16>::THREADS, sizeof(StencilSmem<16>), stream>>>(
+            rgbi, g, lut, stages, p, cc, aux, hs, hwa, hwr, plane, cand, meta, err);
+    } else {
+        dim3 grid(g.tw, g.hp / 8);
+        k_stencil<8><<<grid, Tile<8>::THREADS, sizeof(StencilSmem<8>), stream>>>(
             rgbi, g, lut, stages, p, cc, aux, hs, hwa, hwr, plane, cand, meta, err);
     }
     marks.mark(3, stream);
@@ -892,7 +977,6 @@ cudaError_t launch_analysis(const uint16_t *rgbi, const Geometry &g, const float
     return cudaGetLastError();
 }
 
-size_t stencil_smem_bytes() { return sizeof(StencilSmem); }
 
 cudaError_t producer_init();
 cudaError_t writer_init();
@@ -900,8 +984,12 @@ cudaError_t writer_init();
 // Opt in to the dynamic shared memory the tiled kernels use (once per
 // device, with the device current).
 cudaError_t analysis_init() {
-    cudaError_t e = cudaFuncSetAttribute(k_stencil, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)sizeof(StencilSmem));
+    cudaError_t e = cudaFuncSetAttribute(k_stencil<8>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)sizeof(StencilSmem<8>));
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_stencil<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)sizeof(StencilSmem<16>));
     if (e != cudaSuccess) return e;
     e = walk_init();
     if (e != cudaSuccess) return e;

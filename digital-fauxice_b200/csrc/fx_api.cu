@@ -69,7 +69,7 @@ static size_t arena_layout(const Geometry &g, int64_t amb_cap, Arena *a) {
     const int64_t plane = (int64_t)g.prow * g.pitch;
     const size_t o_rgbi = take(px * 8);
     const size_t o_stages = take((g.h + 6) * sizeof(fx_stage));
-    const size_t o_aux = take(px * 4);
+    const size_t o_aux = take(plane * 4);  // padded, edge-replicated
     const size_t o_hs = take(plane * 4);
     const size_t o_hwa = take(plane * 4);
     const size_t o_hwr = take(3 * plane * 4);
@@ -155,6 +155,7 @@ struct fx_context {
     bool parallel_walk = true;
     int walk_wave = 0;  // window segments per wave; 0: g_per_wave (three per SM)
     double walk_sigmas = fx::kDefaultWindowSigmas;  // walk window half-width
+    int stencil_rows = 8;  // stencil tile height: 8 (four blocks per SM) or 16 (two)
     int64_t list_capacity = 0;  // RNG-dependent list entries per frame; 0: sites / 2
     std::vector<std::vector<cudaEvent_t>> pending;  // recorded, not yet read
     std::vector<std::vector<cudaEvent_t>> spare;
@@ -287,7 +288,8 @@ static int enqueue_pass(fx_context *ctx, Slot &s, const Geometry &g, const fx_pa
     const uint32_t *cancel = cancellable ? s.cancel_dev : nullptr;
     FX_CUDA(ctx, launch_gate(cancel, a.err, st));
     FX_CUDA(ctx, launch_analysis(d_in, g, ctx->lut, a.stages, p, a.aux, a.hs, a.hwa, a.hwr,
-                                 (int64_t)g.prow * g.pitch, a.cand, a.meta, a.err, st, marks));
+                                 (int64_t)g.prow * g.pitch, a.cand, a.meta, a.err, st, marks,
+                                 ctx->stencil_rows));
     // the walk scratch is sized for g_per_wave; a narrower wave uses part of it
     const int wave = (ctx->walk_wave > 0 && ctx->walk_wave < g_per_wave) ? ctx->walk_wave
                                                                          : g_per_wave;
@@ -869,6 +871,22 @@ FX_API int fx_reserve_frames(fx_context *ctx, int32_t max_height, int32_t max_wi
     return FX_OK;
 }
 
+FX_API int fx_release_idle_slots(fx_context *ctx, int64_t *released_bytes) {
+    if (!ctx) return FX_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    cudaSetDevice(ctx->device);
+    int64_t freed = 0;
+    for (Slot &s : ctx->slots) {
+        if (s.busy || !s.arena.base) continue;
+        FX_CUDA(ctx, cudaStreamSynchronize(s.stream));
+        FX_CUDA(ctx, cudaFree(s.arena.base));
+        freed += (int64_t)s.arena.bytes;
+        s.arena = Arena();
+    }
+    if (released_bytes) *released_bytes = freed;
+    return FX_OK;
+}
+
 FX_API int fx_set_slots(fx_context *ctx, int32_t slots) {
     if (!ctx || slots < 1 || slots > 64) return FX_ERR_INVALID_ARGUMENT;
     std::lock_guard<std::mutex> lock(ctx->mu);
@@ -900,22 +918,22 @@ static int stage_host_results(fx_context *ctx, Slot &s) {
 }
 
 // A free slot for a frame of geometry g: the one with the smallest arena
-// that already holds the frame, else one without an arena, else any free
-// slot (whose arena then grows: a cudaFree, which waits for the whole
-// device, so serving and batching keep to the first two cases).
+// that already holds the frame, else one without an arena, else the free
+// slot with the largest arena (which then grows: a cudaFree, which waits
+// for the whole device).
 static Slot *free_slot(fx_context *ctx, const Geometry &g) {
     const size_t need = arena_layout(g, amb_capacity(ctx, g), nullptr);
-    Slot *fit = nullptr, *empty = nullptr, *any = nullptr;
+    Slot *fit = nullptr, *empty = nullptr, *largest = nullptr;
     for (Slot &s : ctx->slots) {
         if (s.busy) continue;
-        if (!any) any = &s;
         if (!s.arena.base) {
             if (!empty) empty = &s;
-        } else if (s.arena.bytes >= need && (!fit || s.arena.bytes < fit->arena.bytes)) {
-            fit = &s;
+            continue;
         }
+        if (s.arena.bytes >= need && (!fit || s.arena.bytes < fit->arena.bytes)) fit = &s;
+        if (!largest || s.arena.bytes > largest->arena.bytes) largest = &s;
     }
-    return fit ? fit : (empty ? empty : any);
+    return fit ? fit : (empty ? empty : largest);
 }
 
 FX_API int fx_submit(fx_context *ctx, const fx_frame *f, int64_t *ticket) {
@@ -1177,6 +1195,13 @@ FX_API int fx_set_walk_window(fx_context *ctx, double sigmas) {
     if (!ctx || !(sigmas >= 0.0) || sigmas > 64.0) return FX_ERR_INVALID_ARGUMENT;
     std::lock_guard<std::mutex> lock(ctx->mu);
     ctx->walk_sigmas = sigmas;
+    return FX_OK;
+}
+
+FX_API int fx_set_stencil_tile(fx_context *ctx, int32_t rows) {
+    if (!ctx || (rows != 0 && rows != 8 && rows != 16)) return FX_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    ctx->stencil_rows = rows == 0 ? 8 : rows;
     return FX_OK;
 }
 

@@ -16,7 +16,8 @@ constexpr uint32_t kLcgMask = 0x00FFFFFFu;
 // rng.py:135: float32 bits 0x337fffff widened = (2^24 - 1) * 2^-48.
 constexpr double kNormalization = 0x1.fffffep-25;
 constexpr int kPad = 5;          // history-plane border (rows/cols)
-constexpr int kTileH = 8;        // stencil tile rows
+constexpr int kTileH = 16;       // padded planes cover whole 16-row tiles (the
+                                 // stencil runs 8- or 16-row tiles)
 constexpr int kTileW = 32;       // stencil tile cols
 constexpr int kSegment = 1024;   // chain sites per scan segment
 constexpr int kSegThreads = 256; // threads per segment block
@@ -41,7 +42,7 @@ __device__ __forceinline__ bool pass_stopped(const uint32_t *err) {
 
 struct Geometry {
     int h, w;              // logical frame
-    int th, tw;            // tiles
+    int th, tw;            // kTileH x kTileW blocks covering the frame
     int hp, wp;            // rows/cols rounded up to whole tiles
     int prow;              // padded rows = hp + 2*kPad
     int pitch;             // floats per padded row (>= wp + 2*kPad, multiple of 32)
@@ -190,7 +191,8 @@ cudaError_t analysis_init();
 cudaError_t launch_analysis(const uint16_t *rgbi, const Geometry &g, const float *lut,
                             const fx_stage *stages, const fx_params &p, float *aux, float *hs,
                             float *hwa, float *hwr, int64_t plane, double *cand, uint8_t *meta,
-                            uint32_t *err, cudaStream_t stream, const Marks &marks);
+                            uint32_t *err, cudaStream_t stream, const Marks &marks,
+                            int tile_rows);
 cudaError_t writer_identity_table(const float *lut, const uint32_t *hi, const uint32_t *lo,
                                   uint16_t *ident, uint32_t *bad, cudaStream_t stream);
 cudaError_t launch_writer(const Geometry &g, const uint8_t *meta, const double *cand,

@@ -33,6 +33,7 @@ constexpr uint32_t kSegLen = 4096;                  // channels per walk segment
 constexpr int kWinChunk = 256;                      // channels staged per chunk
 constexpr int kWinRing = 3;                         // staged chunks in flight
 constexpr uint32_t kCompactEvery = 512;             // block compaction period (steady state)
+constexpr uint32_t kSettledCompactEvery = 512;      // the same once at most 256 are left
 constexpr uint32_t kNone = 0xFFFFFFFFu;
 constexpr uint32_t kSerialBelow = 4 * kSegLen;      // short chains: one serial walk
 // The window half-width is kDefaultWindowSigmas (4.5) standard deviations of
@@ -309,12 +310,13 @@ __device__ __forceinline__ void walk_span(const uint4 *r4, uint32_t r, uint32_t 
 
 // Slots per lane for `live` candidates.  Warp w holds list positions
 // [w * slots * 32, (w + 1) * slots * 32).  Above kWinThreads candidates every
-// warp walks; at most kWinThreads left (no further compaction), more than
-// half of them are packed two per lane into at most four warps: two slots
-// in four warps measured 1.48x the candidate-step rate of one slot in eight
-// (three blocks per SM, 4096 channels).
+// warp walks; at most kWinThreads left (the settled phase), more than 32 of
+// them are packed two per lane into the fewest warps: two slots in four
+// warps measured 1.48x the candidate-step rate of one slot in eight (three
+// blocks per SM, 4096 channels), and warps with no candidate left do not
+// step.
 __device__ __forceinline__ int window_slots(uint32_t live) {
-    if (live <= (uint32_t)kWinThreads) return live > (uint32_t)kWinThreads / 2u ? 2 : 1;
+    if (live <= (uint32_t)kWinThreads) return live > 32u ? 2 : 1;
     const uint32_t s = (live + kWinThreads - 1u) / kWinThreads;
     return s > (uint32_t)kWinSlots ? kWinSlots : (int)s;
 }
@@ -563,8 +565,11 @@ __global__ void __launch_bounds__(kWinThreads, kWinBlocksPerSM)
                 merge_and_compact(slots);
                 slots = window_slots(live);
                 packed |= live <= (uint32_t)kWinThreads && slots == 2;
-                next_compact = live <= (uint32_t)kWinThreads ? (iw - i0)
-                                                             : min(2 * next_compact, done + kCompactEvery);
+                // settled: compact every kSettledCompactEvery channels, so
+                // warps drop out as duplicates merge
+                next_compact = live <= (uint32_t)kWinThreads
+                                   ? min(iw - i0, done + kSettledCompactEvery)
+                                   : min(2 * next_compact, done + kCompactEvery);
             }
         }
         b = (b + 1) % kWinRing;

@@ -152,9 +152,11 @@ SIGNATURES = {
     "fx_poll": ([_P, ctypes.c_int64], ctypes.c_int),
     "fx_wait": ([_P, ctypes.c_int64, ctypes.c_int64, ctypes.POINTER(FxCounters)], ctypes.c_int),
     "fx_cancel": ([_P, ctypes.c_int64], ctypes.c_int),
+    "fx_release_idle_slots": ([_P, ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
     "fx_fetch": ([_P, ctypes.c_int64, ctypes.c_int64, _P, ctypes.POINTER(FxCounters), _P, _P, _P],
                  ctypes.c_int),
     "fx_set_walk_window": ([_P, ctypes.c_double], ctypes.c_int),
+    "fx_set_stencil_tile": ([_P, ctypes.c_int32], ctypes.c_int),
     "fx_set_list_capacity": ([_P, ctypes.c_int64], ctypes.c_int),
     "fx_mem_info": ([_P, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)],
                     ctypes.c_int),

@@ -13,14 +13,18 @@ scans leave most SMs to the others).
 * :func:`process_batch` -- :class:`ProcessingJob` objects in, reference-shaped
   :class:`ProcessingResult` objects out (host buffers), same validation and
   fail-closed behaviour as :func:`fauxice_b200.engine.process_b200`.
-* :func:`tune_slots` -- picks the slot count that maximises throughput on a
-  sample of the workload (the batching autotuner).
+* :func:`tune_slots` -- picks the slot count, walk wave and stencil tile
+  height that maximise throughput on a sample of the workload (the batching
+  autotuner); :func:`autotune` caches that choice as JSON, keyed by device
+  and frame shapes.  Every choice computes the same bits; only the time
+  differs.
 """
 
 from __future__ import annotations
 
 import ctypes
 import hashlib
+import json
 import os
 import time
 from collections import deque
@@ -88,6 +92,13 @@ def set_walk_wave(ctx: _lib.Context, segments: int) -> None:
         _check(ctx, _lib.load().fx_set_walk_wave(ctx.handle, int(segments)))
 
 
+def set_stencil_tile(ctx: _lib.Context, rows: int) -> None:
+    """Stencil tile height: 8 rows (four blocks per SM) or 16 (two)."""
+
+    with ctx.lock:
+        _check(ctx, _lib.load().fx_set_stencil_tile(ctx.handle, int(rows)))
+
+
 def run_device_batch(ctx: _lib.Context, frames: Sequence[DeviceFrame], *, slots: int = 4,
                      params: _lib.FxParams | None = None) -> list[_lib.FxCounters]:
     """Process device-resident frames with up to ``slots`` in flight.
@@ -136,26 +147,98 @@ def run_device_batch(ctx: _lib.Context, frames: Sequence[DeviceFrame], *, slots:
 
 def tune_slots(ctx: _lib.Context, frames: Sequence[DeviceFrame],
                candidates: Iterable[int] = (1, 2, 4, 8), waves: Iterable[int] = (0,),
-               repeats: int = 1) -> tuple[tuple[int, int], dict]:
-    """Time the sample batch at each (slots, walk wave) pair; leave the best
-    walk wave set and return it with the measured seconds of every pair
-    (after one warm-up run that allocates the slots' buffers)."""
+               repeats: int = 1, tiles: Iterable[int] = (8,)) -> tuple[tuple[int, ...], dict]:
+    """Time the sample batch at each (slots, walk wave, stencil tile)
+    combination; leave the best walk wave and tile set and return the
+    choice with the measured seconds of every combination (after one
+    warm-up run that allocates the slots' buffers).  The choice is a
+    (slots, wave) pair when only one tile height is tried, else
+    (slots, wave, tile)."""
 
-    candidates, waves = tuple(candidates), tuple(waves)
-    timings: dict[tuple[int, int], float] = {}
+    candidates, waves, tiles = tuple(candidates), tuple(waves), tuple(tiles)
+    timings: dict[tuple[int, ...], float] = {}
     run_device_batch(ctx, frames, slots=max(candidates))
-    for wave in waves:
-        set_walk_wave(ctx, wave)
-        for slots in candidates:
-            best = float("inf")
-            for _ in range(repeats):
-                t0 = time.perf_counter()
-                run_device_batch(ctx, frames, slots=slots)
-                best = min(best, time.perf_counter() - t0)
-            timings[(slots, wave)] = best
+    import torch
+
+    for tile in tiles:
+        set_stencil_tile(ctx, tile)
+        for wave in waves:
+            set_walk_wave(ctx, wave)
+            for slots in candidates:
+                best = float("inf")
+                for _ in range(repeats):
+                    torch.cuda.synchronize()
+                    t0 = time.perf_counter()
+                    run_device_batch(ctx, frames, slots=slots)
+                    torch.cuda.synchronize()
+                    best = min(best, time.perf_counter() - t0)
+                key = (slots, wave) if len(tiles) == 1 else (slots, wave, tile)
+                timings[key] = best
     choice = min(timings, key=timings.get)
     set_walk_wave(ctx, choice[1])
+    set_stencil_tile(ctx, choice[2] if len(choice) > 2 else tiles[0])
     return choice, timings
+
+
+def tuning_cache_path() -> str:
+    """Where autotune keeps its choices: FAUXICE_B200_TUNING, else
+    $XDG_CACHE_HOME (or ~/.cache)/fauxice_b200/tuning.json."""
+
+    path = os.environ.get("FAUXICE_B200_TUNING")
+    if path:
+        return path
+    base = os.environ.get("XDG_CACHE_HOME") or os.path.join(os.path.expanduser("~"), ".cache")
+    return os.path.join(base, "fauxice_b200", "tuning.json")
+
+
+def tuning_key(device: int, frames: Sequence[DeviceFrame]) -> str:
+    """Device name, SM count and the sorted set of frame shapes."""
+
+    import torch
+
+    props = torch.cuda.get_device_properties(device)
+    shapes = sorted({(f.height, f.width) for f in frames})
+    return (f"{props.name}|sm{props.major}{props.minor}|{props.multi_processor_count}SM|"
+            + ",".join(f"{h}x{w}" for h, w in shapes))
+
+
+def autotune(ctx: _lib.Context, frames: Sequence[DeviceFrame], *,
+             candidates: Iterable[int] = (2, 4, 8), waves: Iterable[int] = (0, 148),
+             tiles: Iterable[int] = (8, 16), cache_path: str | None = None,
+             retune: bool = False) -> tuple[dict, bool]:
+    """The batching configuration for this device and these frame shapes:
+    from the JSON cache when an entry exists (and ``retune`` is off), else
+    measured with :func:`tune_slots` over every combination and stored.
+    Applies the walk wave and stencil tile to the context and returns
+    ({"slots", "walk_wave", "stencil_tile", "timings_ms"}, from_cache)."""
+
+    path = cache_path or tuning_cache_path()
+    key = tuning_key(ctx.device, frames)
+    cache: dict = {}
+    try:
+        with open(path) as handle:
+            cache = json.load(handle)
+    except (OSError, ValueError):
+        cache = {}
+    entry = None if retune else cache.get(key)
+    from_cache = entry is not None
+    if entry is None:
+        choice, timings = tune_slots(ctx, frames, candidates=candidates, waves=waves,
+                                     tiles=tuple(tiles))
+        if len(choice) == 2:
+            choice = (*choice, tuple(tiles)[0])
+        entry = {"slots": choice[0], "walk_wave": choice[1], "stencil_tile": choice[2],
+                 "timings_ms": {",".join(str(v) for v in k): round(1e3 * t, 2)
+                                for k, t in timings.items()}}
+        cache[key] = entry
+        os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
+        tmp = path + ".tmp"
+        with open(tmp, "w") as handle:
+            json.dump(cache, handle, indent=1, sort_keys=True)
+        os.replace(tmp, path)
+    set_walk_wave(ctx, entry["walk_wave"])
+    set_stencil_tile(ctx, entry["stencil_tile"])
+    return entry, from_cache
 
 
 def _sha256(array: np.ndarray) -> bytes:

@@ -10,10 +10,13 @@ while others run are processed alongside them, each in its own library slot
   (``fx_frame_bytes(h, w)``, the same estimate the reference's CUDA backend
   checks against free memory, cuda_backend/engine.py:168-224) plus its input
   and output planes.  A slot whose buffers already hold the frame is reused
-  (no new memory); otherwise a slot without buffers takes it if the bytes
-  fit the budget (the free HBM reported by ``fx_mem_info`` at the start,
-  less a reserve).  Slot buffers are never freed while frames are in
-  flight: a ``cudaFree`` would wait for the whole device.
+  (no new memory); otherwise a slot without buffers takes it, or the idle
+  slot with the largest buffers grows, if the bytes fit the budget (the
+  free HBM reported by ``fx_mem_info`` at the start, less a reserve).  When
+  a request does not fit while nothing is in flight, the idle slots'
+  buffers are released (``fx_release_idle_slots``; freeing device memory
+  waits for the whole device, which costs nothing then) and the request is
+  admitted into fresh ones.
 * a request's upload is queued on a copy stream; the frame is submitted
   with ``fx_submit_device`` once the upload has landed; when the pass is
   done its RGB16 output is copied back into pinned host memory on a second
@@ -78,6 +81,7 @@ class ServeReport:
     peak_bytes: int = 0        # slot buffers + planes of the requests in flight
     budget_bytes: int = 0
     slots_used: int = 0        # library slots that got device buffers
+    releases: int = 0          # times the idle slots' buffers were released
     verified: int = 0          # outputs compared with their single-frame output
     mismatches: int = 0        # differing uint16 values over all verified outputs
 
@@ -96,7 +100,8 @@ class ServeReport:
                "max_in_flight": self.max_in_flight,
                "peak_device_bytes": self.peak_bytes,
                "budget_bytes": self.budget_bytes,
-               "slots_used": self.slots_used}
+               "slots_used": self.slots_used,
+               "buffer_releases": self.releases}
         if self.verified:
             out["verified"] = self.verified
             out["bit_exact"] = self.mismatches == 0 and self.verified == len(self.completions)
@@ -122,38 +127,162 @@ def frame_bytes(height: int, width: int) -> int:
 
 
 class SlotModel:
-    """The library's slot choice, mirrored on the host: the free slot with
-    the smallest buffers that hold the frame, else a slot without buffers.
-    Tracks which buffer sizes exist so admission knows whether a request
-    needs new device memory."""
+    """The library's slot choice (fx_api free_slot), mirrored on the host:
+    the idle slot with the smallest buffers that hold the frame, else a slot
+    without buffers, else the idle slot with the largest buffers, which
+    grows.  Tracks the buffer sizes so admission knows how much new device
+    memory a request needs."""
 
     def __init__(self, slots: int) -> None:
         self.free_sizes: list[int] = []   # buffers of idle slots
         self.empty = slots                 # slots without buffers
         self.allocated = 0                 # bytes of all slot buffers
 
-    def choose(self, need: int) -> tuple[str, int] | None:
+    def choose(self, need: int) -> tuple[str, int, int] | None:
+        """(kind, old buffer size, new buffer size), or None when every slot
+        is busy."""
+
         fits = [s for s in self.free_sizes if s >= need]
         if fits:
-            return "reuse", min(fits)
+            return "reuse", min(fits), min(fits)
         if self.empty:
-            return "new", need
+            return "new", 0, need
+        if self.free_sizes:
+            return "grow", max(self.free_sizes), need
         return None
 
-    def take(self, kind: str, size: int) -> None:
+    @staticmethod
+    def extra(choice: tuple[str, int, int]) -> int:
+        kind, old, new = choice
+        return 0 if kind == "reuse" else new - old
+
+    def take(self, choice: tuple[str, int, int]) -> int:
+        """Mark the chosen slot busy; returns its buffer size."""
+
+        kind, old, new = choice
         if kind == "reuse":
-            self.free_sizes.remove(size)
-        else:
+            self.free_sizes.remove(old)
+        elif kind == "new":
             self.empty -= 1
-            self.allocated += size
+            self.allocated += new
+        else:
+            self.free_sizes.remove(old)
+            self.allocated += new - old
+        return new
 
     def give_back(self, size: int) -> None:
         self.free_sizes.append(size)
 
+    def release_idle(self) -> None:
+        """The idle slots' buffers were freed."""
 
-def serve(ctx: _lib.Context, requests: Sequence[Request], *, max_slots: int = 12,
+        self.empty += len(self.free_sizes)
+        self.allocated -= sum(self.free_sizes)
+        self.free_sizes = []
+
+
+class TorchDevice:
+    """The device side of the request loop: torch streams and buffers for
+    the planes and the copies, the library for the passes."""
+
+    def __init__(self, ctx: _lib.Context, max_slots: int, max_out: int) -> None:
+        import torch
+
+        self.torch = torch
+        self.ctx = ctx
+        self.lib = _lib.load()
+        self.params = DEFAULT_PROFILE.hot_path_parameters().to_c()
+        batch.set_slots(ctx, max_slots)
+        self.host_out = [torch.empty(max_out, dtype=torch.int16).pin_memory()
+                         for _ in range(max_slots)]
+        self.up, self.down, self.checks = (torch.cuda.Stream(), torch.cuda.Stream(),
+                                           torch.cuda.Stream())
+        self.mismatch = torch.zeros((), dtype=torch.int64, device="cuda")
+        torch.cuda.synchronize()
+
+    def frame_bytes(self, h: int, w: int) -> int:
+        return frame_bytes(h, w)
+
+    def free_bytes(self) -> int:
+        free, total = ctypes.c_size_t(), ctypes.c_size_t()
+        with self.ctx.lock:
+            self.ctx.check(self.lib.fx_mem_info(self.ctx.handle, ctypes.byref(free),
+                                                ctypes.byref(total)))
+        return int(free.value)
+
+    def release_idle(self) -> None:
+        with self.ctx.lock:
+            self.ctx.check(self.lib.fx_release_idle_slots(self.ctx.handle, None))
+
+    def upload(self, st: dict, pixels) -> None:
+        torch = self.torch
+        h, w = st["h"], st["w"]
+        src = pixels
+        if isinstance(src, np.ndarray):
+            src = torch.from_numpy(np.ascontiguousarray(src, dtype=np.uint16).view(np.int16))
+        with torch.cuda.stream(self.up):
+            st["d_in"] = torch.empty((h, w, 4), dtype=torch.int16, device="cuda")
+            st["d_out"] = torch.empty((h, w, 3), dtype=torch.int16, device="cuda")
+            st["d_in"].copy_(src.view(h, w, 4), non_blocking=True)
+            st["event"] = torch.cuda.Event()
+            st["event"].record(self.up)
+
+    def landed(self, st: dict) -> bool:
+        return st["event"].query()
+
+    def submit(self, st: dict) -> int | None:
+        ticket = ctypes.c_int64()
+        with self.ctx.lock:
+            status = self.lib.fx_submit_device(
+                self.ctx.handle, ctypes.c_void_p(st["d_in"].data_ptr()), st["h"], st["w"],
+                ctypes.byref(self.params), None, NIKON_PE_INITIAL_STATE,
+                ctypes.c_void_p(st["d_out"].data_ptr()), None, None, ctypes.byref(ticket))
+        if status == batch.FX_PENDING:
+            return None
+        batch._check(self.ctx, status)
+        return ticket.value
+
+    def done(self, ticket: int) -> bool:
+        with self.ctx.lock:
+            return self.lib.fx_poll(self.ctx.handle, ticket) != batch.FX_PENDING
+
+    def finish(self, ticket: int) -> _lib.FxCounters:
+        counters = _lib.FxCounters()
+        batch._check(self.ctx, self.lib.fx_wait(self.ctx.handle, ticket, -1,
+                                                ctypes.byref(counters)))
+        return counters
+
+    def download(self, st: dict, expected) -> None:
+        """Queue the output's copy to pinned host memory and, when given,
+        its on-device comparison (the pass is complete: fx_wait returned)."""
+
+        torch = self.torch
+        n = st["h"] * st["w"] * 3
+        with torch.cuda.stream(self.down):
+            self.host_out[st["host"]][:n].copy_(st["d_out"].view(-1), non_blocking=True)
+            st["event"] = torch.cuda.Event()
+            st["event"].record(self.down)
+        if expected is not None:
+            with torch.cuda.stream(self.checks):
+                self.mismatch.add_((st["d_out"] != expected.view(st["h"], st["w"], 3)).sum())
+            st["d_out"].record_stream(self.checks)
+
+    def downloaded(self, st: dict) -> bool:
+        return st["event"].query()
+
+    def output(self, st: dict) -> np.ndarray:
+        n = st["h"] * st["w"] * 3
+        return self.host_out[st["host"]][:n].numpy().view(np.uint16).reshape(
+            st["h"], st["w"], 3).copy()
+
+    def mismatches(self) -> int:
+        self.checks.synchronize()
+        return int(self.mismatch.item())
+
+
+def serve(ctx: _lib.Context | None, requests: Sequence[Request], *, max_slots: int = 12,
           budget_bytes: int | None = None, reserve_bytes: int = 8 << 30,
-          keep_outputs: bool = False) -> ServeReport:
+          keep_outputs: bool = False, device=None) -> ServeReport:
     """Run the request loop in real time; requests must be sorted by arrival.
 
     ``max_slots`` bounds the requests in flight; device memory bounds them
@@ -162,43 +291,33 @@ def serve(ctx: _lib.Context, requests: Sequence[Request], *, max_slots: int = 12
     output planes of the requests in flight.  A request that carries its
     ``expected`` output is checked against it on the device, after its
     output's copy to host memory has been queued (off the latency path).
-    The context should hold no slot buffers yet (a fresh context, or one
-    whose slots this loop sized before): the host's model of the slots
-    starts empty.
+    The idle slots' buffers are released before the clock starts, so the
+    host's model of the slots and the library's slots start out empty.
+    ``device`` replaces the device side (a :class:`TorchDevice` on ``ctx``
+    by default; the tests drive the loop with a host-only stand-in).
     """
 
-    import torch
-
-    lib = _lib.load()
     report = ServeReport()
     if not requests:
         return report
-    batch.set_slots(ctx, max_slots)
+    max_out = max(int(r.pixels.shape[0]) * int(r.pixels.shape[1]) * 3 for r in requests)
+    dev = device if device is not None else TorchDevice(ctx, max_slots, max_out)
+    dev.release_idle()  # nothing is in flight yet: start from slots without buffers
     if budget_bytes is None:
-        free, total = ctypes.c_size_t(), ctypes.c_size_t()
-        with ctx.lock:
-            ctx.check(lib.fx_mem_info(ctx.handle, ctypes.byref(free), ctypes.byref(total)))
-        budget_bytes = int(free.value) - reserve_bytes
+        budget_bytes = dev.free_bytes() - reserve_bytes
     report.budget_bytes = int(budget_bytes)
-    largest = max(frame_bytes(*r.pixels.shape[:2]) + 14 * int(r.pixels.shape[0])
+    largest = max(dev.frame_bytes(*r.pixels.shape[:2]) + 14 * int(r.pixels.shape[0])
                   * int(r.pixels.shape[1]) for r in requests)
     if largest > budget_bytes:
         raise MemoryError(f"the largest request needs {largest} bytes of device memory; the "
                           f"budget is {budget_bytes}")
-    params = DEFAULT_PROFILE.hot_path_parameters().to_c()
     model = SlotModel(max_slots)
-    max_out = max(int(r.pixels.shape[0]) * int(r.pixels.shape[1]) * 3 for r in requests)
-    host_out = [torch.empty(max_out, dtype=torch.int16).pin_memory() for _ in range(max_slots)]
     free_host = deque(range(max_slots))
-    up_stream, down_stream = torch.cuda.Stream(), torch.cuda.Stream()
-    check_stream = torch.cuda.Stream()
-    mismatches = torch.zeros((), dtype=torch.int64, device="cuda")
     waiting: deque[int] = deque()
     staging: deque[dict] = deque()    # uploads in flight, in admission order
     inflight: dict[int, dict] = {}    # ticket -> request state
     downloads: deque[dict] = deque()  # outputs on their way to host memory
     in_use_bytes = 0                  # planes of the requests in flight
-    torch.cuda.synchronize()
     nxt = 0
     start = time.perf_counter()
 
@@ -210,82 +329,54 @@ def serve(ctx: _lib.Context, requests: Sequence[Request], *, max_slots: int = 12
         while nxt < len(requests) and requests[nxt].arrival_s <= t:
             waiting.append(nxt)
             nxt += 1
-        # admission, in arrival order: a slot (reused or new) and room
+        # admission, in arrival order: a slot (reused, new or grown) and room
         while waiting and free_host:
             i = waiting[0]
             h, w = (int(v) for v in requests[i].pixels.shape[:2])
             planes = 14 * h * w
-            choice = model.choose(frame_bytes(h, w))
-            if choice is None:
-                break
-            kind, size = choice
-            extra = size if kind == "new" else 0
-            if model.allocated + extra + in_use_bytes + planes > budget_bytes:
-                break
+            choice = model.choose(dev.frame_bytes(h, w))
+            fits = (choice is not None and model.allocated + model.extra(choice) + in_use_bytes
+                    + planes <= budget_bytes)
+            if not fits:
+                if staging or inflight or downloads or not model.free_sizes:
+                    break  # wait for a request in flight to finish
+                # nothing in flight: drop the idle buffers and start afresh
+                dev.release_idle()
+                model.release_idle()
+                report.releases += 1
+                continue
             waiting.popleft()
-            model.take(kind, size)
+            st = {"i": i, "h": h, "w": w, "admitted": now(), "size": model.take(choice),
+                  "planes": planes, "host": free_host.popleft()}
             in_use_bytes += planes
-            src = requests[i].pixels
-            if isinstance(src, np.ndarray):
-                src = torch.from_numpy(np.ascontiguousarray(src, dtype=np.uint16).view(np.int16))
-            with torch.cuda.stream(up_stream):
-                d_in = torch.empty((h, w, 4), dtype=torch.int16, device="cuda")
-                d_out = torch.empty((h, w, 3), dtype=torch.int16, device="cuda")
-                d_in.copy_(src.view(h, w, 4), non_blocking=True)
-                landed = torch.cuda.Event()
-                landed.record(up_stream)
-            staging.append({"i": i, "h": h, "w": w, "d_in": d_in, "d_out": d_out,
-                            "event": landed, "admitted": now(), "size": size,
-                            "planes": planes, "host": free_host.popleft()})
+            dev.upload(st, requests[i].pixels)
+            staging.append(st)
         report.max_in_flight = max(report.max_in_flight,
                                    len(staging) + len(inflight) + len(downloads))
         report.peak_bytes = max(report.peak_bytes, model.allocated + in_use_bytes)
         # submission: uploads that have landed go to a library slot
-        while staging and staging[0]["event"].query():
-            st = staging[0]
-            ticket = ctypes.c_int64()
-            with ctx.lock:
-                status = lib.fx_submit_device(
-                    ctx.handle, ctypes.c_void_p(st["d_in"].data_ptr()), st["h"], st["w"],
-                    ctypes.byref(params), None, NIKON_PE_INITIAL_STATE,
-                    ctypes.c_void_p(st["d_out"].data_ptr()), None, None, ctypes.byref(ticket))
-            if status == batch.FX_PENDING:
+        while staging and dev.landed(staging[0]):
+            ticket = dev.submit(staging[0])
+            if ticket is None:
                 break
-            batch._check(ctx, status)
-            staging.popleft()
-            inflight[ticket.value] = st
+            inflight[ticket] = staging.popleft()
         # finished passes: counters, then the output's copy to host memory
         for ticket in list(inflight):
-            with ctx.lock:
-                status = lib.fx_poll(ctx.handle, ticket)
-            if status == batch.FX_PENDING:
+            if not dev.done(ticket):
                 continue
             st = inflight.pop(ticket)
-            counters = _lib.FxCounters()
-            batch._check(ctx, lib.fx_wait(ctx.handle, ticket, -1, ctypes.byref(counters)))
-            st["counters"] = counters
-            n = st["h"] * st["w"] * 3
-            with torch.cuda.stream(down_stream):
-                host_out[st["host"]][:n].copy_(st["d_out"].view(-1), non_blocking=True)
-                st["event"] = torch.cuda.Event()
-                st["event"].record(down_stream)
+            st["counters"] = dev.finish(ticket)
             expected = requests[st["i"]].expected
+            dev.download(st, expected)
             if expected is not None:
-                # the pass is complete (fx_wait returned): no stream order needed
-                with torch.cuda.stream(check_stream):
-                    mismatches.add_((st["d_out"] != expected.view(st["h"], st["w"], 3)).sum())
-                st["d_out"].record_stream(check_stream)
                 report.verified += 1
             downloads.append(st)
         finished = False
-        while downloads and downloads[0]["event"].query():
+        while downloads and dev.downloaded(downloads[0]):
             st = downloads.popleft()
             done_t = now()
             i, h, w = st["i"], st["h"], st["w"]
-            output = None
-            if keep_outputs:
-                n = h * w * 3
-                output = host_out[st["host"]][:n].numpy().view(np.uint16).reshape(h, w, 3).copy()
+            output = dev.output(st) if keep_outputs else None
             free_host.append(st["host"])
             model.give_back(st["size"])
             in_use_bytes -= st["planes"]
@@ -297,7 +388,6 @@ def serve(ctx: _lib.Context, requests: Sequence[Request], *, max_slots: int = 12
             time.sleep(0.0001)
     report.wall_s = now()
     report.slots_used = max_slots - model.empty
-    check_stream.synchronize()
-    report.mismatches = int(mismatches.item())
+    report.mismatches = dev.mismatches()
     report.completions.sort(key=lambda c: c.index)
     return report

@@ -227,6 +227,13 @@ FX_API int fx_reserve_frames(fx_context *ctx, int32_t max_height, int32_t max_wi
  * fx_fetch; otherwise fx_wait copies them into the frame's own buffers.
  * FX_PENDING when every slot is busy. */
 FX_API int fx_submit(fx_context *ctx, const fx_frame *frame, int64_t *ticket);
+/* Free the device buffers of every slot without a request in flight (no
+ * reference counterpart).  A slot's buffers are otherwise kept and reused by
+ * later frames they hold; a frame larger than every idle slot's buffers
+ * grows the largest of them.  Both free device memory, which waits for the
+ * whole device, so a request loop calls this only when nothing is in flight.
+ * *released_bytes (may be NULL) receives the bytes freed. */
+FX_API int fx_release_idle_slots(fx_context *ctx, int64_t *released_bytes);
 /* fx_submit for a frame already in device memory: the pass is enqueued on
  * a free slot's stream and writes d_rgb_out / d_score_out / d_changed_out
  * (device pointers, NULL for the optional planes) directly.  The caller
@@ -269,6 +276,11 @@ FX_API int fx_fetch(fx_context *ctx, int64_t ticket, int64_t timeout_ns, uint16_
  * fx_set_list_capacity: entries of the RNG-dependent channel list each pass
  * reserves (0, the default: half the frame's chain sites).  A frame with
  * more such channels reruns with room for all of them. */
+/* Height of the analysis stencil's tiles, no reference counterpart: 8 rows
+ * (four resident blocks per SM, the default; 0 selects it) or 16 rows (two
+ * blocks per SM, less halo work per pixel).  Both compute the same values;
+ * the batching autotuner picks one per device and frame shape. */
+FX_API int fx_set_stencil_tile(fx_context *ctx, int32_t rows);
 FX_API int fx_set_walk_window(fx_context *ctx, double sigmas);
 FX_API int fx_set_list_capacity(fx_context *ctx, int64_t channels);
 

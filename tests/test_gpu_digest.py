@@ -43,3 +43,27 @@ def test_digest_is_refused_when_disabled():
         assert lib.fx_output_digest(ctx.handle, buf) != 0
     finally:
         assert lib.fx_set_output_digest(ctx.handle, 1) == 0
+
+
+def test_parity_receipt_of_a_device_result(tmp_path):
+    """A receipt for a B200 result against the oracle's output passes, with
+    the device's runtime recorded."""
+
+    import time
+
+    import cases
+    from _helpers import make_job
+    from fauxice_b200 import receipts
+    from fauxice_b200.engine import process_b200
+    from oracle import oracle as ox
+
+    main, prepass = cases.generated(71, 200, 333, "heavy")
+    t0 = time.perf_counter()
+    result = process_b200(make_job(main, prepass))
+    elapsed = time.perf_counter() - t0
+    doc = receipts.parity_receipt(result, ox.process(main, prepass).output_rgb16, main=main,
+                                  prepass=prepass, claim="200x333 heavy frame against the oracle",
+                                  elapsed_seconds=elapsed)
+    assert doc["status"] == "PASS" and doc["mismatch_samples"] == 0
+    assert doc["runtime"]["compute_capability"] == "10.0"
+    assert receipts.write_receipt(str(tmp_path / "receipt.json"), doc) == receipts.receipt_sha256(doc)
