@@ -193,6 +193,8 @@ def parse():
                     help="comma-separated Poisson request rates per second")
     ap.add_argument("--stencil-tile", type=int, default=0,
                     help="stencil tile rows of the plain path (8 or 16; 0: library default)")
+    ap.add_argument("--serve-only", action="store_true",
+                    help="run only the serving workload and print its report")
     ap.add_argument("--plan-only", action="store_true",
                     help="print each rank's work plan after the collectives; no GPU work")
     return ap.parse_args()
@@ -861,6 +863,17 @@ def main():
         run_plan(world, rank)
     elif args.impl == "reference":
         run_reference(args, world, rank)
+    elif args.serve_only:
+        if rank == 0:
+            from fauxice_b200 import engine
+
+            specs = serving_pool_specs()
+            pool = (generate(_serving_frame, specs), specs)
+            import torch
+
+            torch.cuda.set_device(local)
+            report = run_serving(engine.context(local), pool, args)
+            print(json.dumps({"metric": METRIC, "serving": report}), flush=True)
     else:
         frames = heavy = pool = None
         if world == 1 and not args.no_batch:
