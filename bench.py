@@ -179,7 +179,9 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", choices=("b200", "reference"), default="b200")
+    ap.add_argument("--impl", choices=("b200", "reference", "numba"), default="b200",
+                    help="reference: the CPU restatement of the path on all host cores; numba: "
+                         "the reference's own cpu-fast backend, when installed in baseline/_ref")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-routing", action="store_true",
                     help="skip the at-floor routing census measurement")
@@ -410,6 +412,68 @@ def run_reference(args, world, rank):
                 "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def run_numba(args, world, rank):
+    """The reference's own numba backend (fast_cpu/engine.py:537,
+    process_cpu_fast) on the seed-2 native frame, on all host cores and on
+    one thread, after a warm-up that compiles it.  It runs only where the
+    reference is installed in baseline/_ref (pip --target); otherwise the
+    line says it is unavailable."""
+
+    if rank != 0:
+        return
+    ref = os.path.join(ROOT, "baseline", "_ref")
+    if not os.path.isdir(os.path.join(ref, "portable_digital_ice")):
+        print(json.dumps({"impl": "numba", "unavailable": "the reference is not installed in "
+                                                          "baseline/_ref"}), flush=True)
+        return
+    os.environ.setdefault("NUMBA_CACHE_DIR", "/tmp/fauxice_numba_cache")
+    sys.path.insert(0, ref)
+    import numba
+    from portable_digital_ice import (AcquisitionEpoch, DualRGBIAcquisition, ProcessingJob,
+                                      ProcessingMode, RGBI16Frame, ScannerModel)
+    from portable_digital_ice.fast_cpu import process_cpu_fast
+
+    from fauxice_b200 import synthetic
+
+    def job(main, prepass):
+        return ProcessingJob(
+            acquisition=DualRGBIAcquisition(
+                prepass=RGBI16Frame(prepass, AcquisitionEpoch.PREPASS, 285, "p"),
+                main=RGBI16Frame(main, AcquisitionEpoch.MAIN, 4000, "m"), same_frame_id="n"),
+            scanner_model=ScannerModel.NIKON_SUPER_COOLSCAN_5000_ED, mode=ProcessingMode.NORMAL,
+            selector=8, resolution_metric=4000, bit_depth=16, focus_exposure_locked=True)
+
+    process_cpu_fast(job(*synthetic.small_crop(1)))  # compile
+    main, prepass = synthetic.native_frame(SEED)
+    golden = json.load(open(os.path.join(ROOT, "tests", "golden", "reference_results.json")))
+    expect = golden["jobs"]["native_full"]["output_sha256"]
+    mp = main.shape[0] * main.shape[1] / 1e6
+    cores = numba.config.NUMBA_NUM_THREADS
+    out = {}
+    for threads, steps in ((cores, max(1, min(args.steps, 3))), (1, 1)):
+        numba.set_num_threads(threads)
+        times, ok = [], True
+        for _ in range(steps):
+            t0 = time.perf_counter()
+            res = process_cpu_fast(job(main, prepass))
+            times.append(time.perf_counter() - t0)
+            ok &= res.replay.output_sha256 == expect
+        med = sorted(times)[len(times) // 2]
+        out[threads] = {"seconds": [round(t, 3) for t in times], "median_s": round(med, 3),
+                        "mp_per_s": round(mp / med, 4), "bit_exact": bool(ok)}
+    best = out[cores]
+    print(json.dumps({
+        "impl": "numba", "metric": METRIC, "value": best["mp_per_s"], "unit": "MP/s",
+        "n_gpus": args.gpus, "steps": len(best["seconds"]), "warmup": 1,
+        "ms_per_step": round(1000 * best["median_s"], 1), "higher_is_better": True,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "native 5782x3946 RGBI frame (seed 2), the reference's numba "
+                               "cpu-fast backend (process_cpu_fast)"},
+        "cpu_baseline": {"value": best["mp_per_s"], "unit": "MP/s", "cores": cores,
+                         "kind": "reference", "sample": "the whole native frame, warm"},
+        "one_thread": out[1], "all_cores": best}), flush=True)
 
 
 def run_b200(args, world, rank, local, frames=None, heavy=None, pool=None):
@@ -785,7 +849,7 @@ def run_e2e_batched(frames, batched):
 
     digests = batched.pop("_digests")
     jobs = [make_job(f, synthetic.make_prepass(f)) for f in frames]
-    batch.process_batch(jobs[:2], slots=batched["slots"])  # warm the host staging
+    batch.process_batch(jobs, slots=batched["slots"])  # warm: pinned staging of every slot
     t0 = time.perf_counter()
     results = batch.process_batch(jobs, slots=batched["slots"])
     elapsed = time.perf_counter() - t0
@@ -823,9 +887,11 @@ def run_serving(ctx, pool, args):
         pinned.append(torch.from_numpy(np.ascontiguousarray(f).view(np.int16)).pin_memory())
         d_in = pinned[-1].to("cuda")
         out = torch.empty((h, w, 3), dtype=torch.int16, device="cuda")
+        torch.cuda.synchronize()
+        # synchronous (counters given): d_in may be reused once this returns
         ctx.check(lib.fx_process_device(ctx.handle, d_in.data_ptr(), h, w, ctypes.byref(params),
                                         None, NIKON_PE_INITIAL_STATE, out.data_ptr(), None, None,
-                                        None, None))
+                                        None, ctypes.byref(_lib.FxCounters())))
         expected.append(out)
     torch.cuda.synchronize()
     groups = [[k for k, s in enumerate(specs) if (s[1], s[2]) == (5782, 3946)],
@@ -863,6 +929,8 @@ def main():
         run_plan(world, rank)
     elif args.impl == "reference":
         run_reference(args, world, rank)
+    elif args.impl == "numba":
+        run_numba(args, world, rank)
     elif args.serve_only:
         if rank == 0:
             from fauxice_b200 import engine

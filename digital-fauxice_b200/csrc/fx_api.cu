@@ -871,6 +871,29 @@ FX_API int fx_reserve_frames(fx_context *ctx, int32_t max_height, int32_t max_wi
     return FX_OK;
 }
 
+FX_API int fx_reserve_slots(fx_context *ctx, int32_t count, int32_t max_height,
+                            int32_t max_width) {
+    if (!ctx || count < 1 || count > 64 || max_height < 1 || max_width < 1)
+        return FX_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    cudaSetDevice(ctx->device);
+    if ((int64_t)max_height * max_width > (int64_t)1 << 30)
+        return fail(ctx, FX_ERR_INVALID_ARGUMENT, "frame too large");
+    int rc = ensure_slots(ctx, count);
+    if (rc) return rc;
+    const Geometry g = make_geometry(max_height, max_width);
+    for (int k = 0; k < count; ++k) {
+        Slot &s = ctx->slots[k];
+        if (s.busy) return fail(ctx, FX_ERR_INVALID_ARGUMENT, "a slot is busy: reserve first");
+        const int64_t cap = s.arena.base && s.arena.amb_capacity > amb_capacity(ctx, g)
+                                ? s.arena.amb_capacity
+                                : amb_capacity(ctx, g);
+        rc = ensure_arena(ctx, s, g, cap);
+        if (rc) return rc;
+    }
+    return FX_OK;
+}
+
 FX_API int fx_release_idle_slots(fx_context *ctx, int64_t *released_bytes) {
     if (!ctx) return FX_ERR_INVALID_ARGUMENT;
     std::lock_guard<std::mutex> lock(ctx->mu);

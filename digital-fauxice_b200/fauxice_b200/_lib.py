@@ -153,6 +153,7 @@ SIGNATURES = {
     "fx_wait": ([_P, ctypes.c_int64, ctypes.c_int64, ctypes.POINTER(FxCounters)], ctypes.c_int),
     "fx_cancel": ([_P, ctypes.c_int64], ctypes.c_int),
     "fx_release_idle_slots": ([_P, ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
+    "fx_reserve_slots": ([_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32], ctypes.c_int),
     "fx_fetch": ([_P, ctypes.c_int64, ctypes.c_int64, _P, ctypes.POINTER(FxCounters), _P, _P, _P],
                  ctypes.c_int),
     "fx_set_walk_window": ([_P, ctypes.c_double], ctypes.c_int),

@@ -234,6 +234,12 @@ FX_API int fx_submit(fx_context *ctx, const fx_frame *frame, int64_t *ticket);
  * whole device, so a request loop calls this only when nothing is in flight.
  * *released_bytes (may be NULL) receives the bytes freed. */
 FX_API int fx_release_idle_slots(fx_context *ctx, int64_t *released_bytes);
+/* fx_reserve_frames for the first `count` slots only (creating them as
+ * needed), no reference counterpart: a request loop sizes a few slots for
+ * its largest frame before its clock starts and lets memory decide how many
+ * more it adds. */
+FX_API int fx_reserve_slots(fx_context *ctx, int32_t count, int32_t max_height,
+                            int32_t max_width);
 /* fx_submit for a frame already in device memory: the pass is enqueued on
  * a free slot's stream and writes d_rgb_out / d_score_out / d_changed_out
  * (device pointers, NULL for the optional planes) directly.  The caller

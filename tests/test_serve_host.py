@@ -70,6 +70,11 @@ class FakeDevice:
             if not busy:
                 self.arena[k] = 0
 
+    def reserve(self, count, h, w, buffers):
+        for k in range(count):
+            self.arena[k] = max(self.arena[k], self.frame_bytes(h, w))
+        self.peak = max(self.peak, sum(self.arena))
+
     def upload(self, st, pixels):
         st["left"] = self.polls
 
@@ -154,7 +159,7 @@ def test_a_large_request_after_small_ones_is_admitted():
     sizes = [(10, 10), (12, 12), (14, 14), (200, 200), (11, 11)]
     largest = dev.frame_bytes(200, 200) + 14 * 200 * 200
     report = serve.serve(None, _fake_requests(sizes), max_slots=3, budget_bytes=largest + 5000,
-                         device=dev)
+                         warm_slots=0, device=dev)
     assert [c.index for c in report.completions] == list(range(5))
     assert report.releases >= 1 and dev.grows == 0
     assert dev.peak <= largest + 5000
@@ -164,6 +169,17 @@ def test_a_large_request_grows_an_idle_slot_when_the_budget_allows():
     dev = FakeDevice(2)
     sizes = [(10, 10), (12, 12), (100, 100)]
     report = serve.serve(None, _fake_requests(sizes, 0.01), max_slots=2,
-                         budget_bytes=1 << 30, device=dev)
+                         budget_bytes=1 << 30, warm_slots=0, device=dev)
     assert [c.index for c in report.completions] == [0, 1, 2]
     assert report.releases == 0 and dev.grows == 1
+
+
+def test_warm_slots_are_sized_for_the_largest_request():
+    dev = FakeDevice(4)
+    sizes = [(10, 10), (100, 100), (20, 20), (100, 100), (50, 50)]
+    report = serve.serve(None, _fake_requests(sizes, 0.001), max_slots=4,
+                         budget_bytes=1 << 30, warm_slots=2, device=dev)
+    assert [c.index for c in report.completions] == list(range(5))
+    big = dev.frame_bytes(100, 100)
+    assert sorted(dev.arena)[-2:] == [big, big]
+    assert dev.grows == 0
