@@ -123,11 +123,6 @@ __global__ void __launch_bounds__(256)
 // Shared scalar pieces
 // ---------------------------------------------------------------------------
 
-struct Record {
-    float a[4];
-    uint32_t fb;  // bit l: lane l takes the consumer row's fallback value
-};
-
 // Vertical chain of one column (reconstruction.py:187-237), p = 9 samples.
 struct ColumnSums {
     float s3, s5, s7, s9, b16;
@@ -453,15 +448,30 @@ struct Tile {
     static constexpr int BLOCKS_PER_SM = TH == 8 ? 4 : 2;
 };
 
+// A feature record of the stencil (streaming.py:236-308): the four feature
+// values and the W of its score patch (the consumer's weights when it is the
+// centre record).  A lane that takes the consumer row's fallback value holds
+// kFallbackBits, a NaN: the feature values are quotients and aux values of
+// finite planes, never NaN, so the marker cannot collide with a value.
+struct StencilRecord {
+    float a[4];
+    float w[3];
+};
+constexpr uint32_t kFallbackBits = 0x7FC0FB00u;
+
 template <int TH>
 struct StencilSmem {
     using T = Tile<TH>;
     float hs[T::PR][T::SW];
-    float hwa[T::PR][T::SW];
+    union {
+        float hwa[T::PR][T::SW];                // waux tile: dead after the column sums
+        StencilRecord rec[T::CR][T::RECC];      // written by the records phase
+    };
     float hwr[3][T::RR][T::SW];                 // staged column j: logical col j - RO
     float cs[2][5][T::CR][T::CC];               // [score|waux][S3,S5,S7,S9,B16]
     float rcs[3][4][TH][T::RC];                 // [channel][S3,S5,S7,S9]
-    Record rec[T::CR][T::RECC];
+    uint16_t reclist[T::CR * T::RECC];          // record positions an attempted pixel reads
+    int nrec;
     union {
         // aux at clamped (y0-4+r, x0-5+j): decision masks and point aux,
         // dead once the records are built
@@ -504,6 +514,15 @@ __global__ void __launch_bounds__(Tile<TH>::THREADS, Tile<TH>::BLOCKS_PER_SM)
     const int tid = threadIdx.x;
     const int y0 = blockIdx.y * TH, x0 = blockIdx.x * T::TW;
     const int h = g.h, w = g.w;
+    const int dty = tid / T::TW, dtx = tid % T::TW;
+    // the writer stage's gates of this thread's pixel row (stage y+7),
+    // loaded while the tile is staged
+    int gate_secondary = 0, row_gate = 1;
+    if (y0 + dty < h) {
+        gate_secondary = stages[y0 + dty + 6].gate_secondary;
+        row_gate = stages[y0 + dty + 6].row_gate;
+    }
+    if (tid == 0) S.nrec = 0;
 
     // ---- stage the tile ---------------------------------------------------
     // 16-byte copies, 11 per staged row: rows 0..PR-1 score, PR..2PR-1 waux
@@ -534,30 +553,38 @@ __global__ void __launch_bounds__(Tile<TH>::THREADS, Tile<TH>::BLOCKS_PER_SM)
     const float thr = p.decision_threshold;
     __syncthreads();
 
-    // ---- decision masks and vertical column sums ---------------------------
-    if (tid < RR) {
-        unsigned long long m = 0;
-        for (int c = 0; c < RC; ++c) m |= (unsigned long long)(S.auxt[tid][c + RO] < thr) << c;
-        S.rowlow[tid] = m;
-    } else if (tid >= 32 && tid < 32 + RC) {
-        const int c = tid - 32;
-        uint32_t m = 0;
-        for (int r = 0; r < RR; ++r) m |= (uint32_t)(S.auxt[r][c + RO] < thr) << r;
-        S.collow[c] = m;
+    // ---- decision masks -----------------------------------------------------
+    // bit c of rowlow[r] / bit r of collow[c]: aux (row r, col c) of the
+    // decision tile is below the threshold; rows by warp ballots (columns
+    // 0..31, then 32..RC-1), columns transposed from the rows
+    {
+        const int lane = tid & 31;
+        static_assert(T::RC > 32 && T::RC <= 64, "two ballots cover a mask row");
+        for (int r = tid >> 5; r < RR; r += NT / 32) {
+            const bool lo = S.auxt[r][lane + RO] < thr;
+            const bool hi = lane < RC - 32 && S.auxt[r][lane + 32 + RO] < thr;
+            const uint32_t b0 = __ballot_sync(0xFFFFFFFFu, lo);
+            const uint32_t b1 = __ballot_sync(0xFFFFFFFFu, hi);
+            if (lane == 0) S.rowlow[r] = ((unsigned long long)b1 << 32) | b0;
+        }
+        __syncthreads();
+        if (tid < RC) {
+            uint32_t m = 0;
+            for (int r = 0; r < RR; ++r) m |= (uint32_t)((S.rowlow[r] >> tid) & 1ull) << r;
+            S.collow[tid] = m;
+        }
+        __syncthreads();
     }
-    __syncthreads();
 
     // ---- per output pixel: the decision -------------------------------------
     // It needs only the aux masks, the point score and the stage gates, so it
     // comes first: a tile without an attempted pixel stops here, and the
     // others build only the records their attempted pixels read.
-    const int dty = tid / T::TW, dtx = tid % T::TW;
     bool eligible = false;
     {
         const int y = y0 + dty, x = x0 + dtx;
         if (y < h && x < w) {
-            const fx_stage ws = stages[y + 6];  // writer stage y+7
-            const bool floor_enabled = p.driver_gate_primary || ws.gate_secondary;
+            const bool floor_enabled = p.driver_gate_primary || gate_secondary;
             // decision bars (streaming.py:157-198), edge-replicated via the
             // tile: rows ty..ty+8 of a column, columns tx..tx+8 of a row
             const int rad = p.radius;
@@ -568,10 +595,10 @@ __global__ void __launch_bounds__(Tile<TH>::THREADS, Tile<TH>::BLOCKS_PER_SM)
             const int lim = p.count_limit;
             eligible = !(vl > lim || ha > lim || vr > lim || hb > lim);
             const float point_score = S.hs[dty + 5][dtx + 5];
-            if (ws.row_gate != 0) eligible = false;
+            if (row_gate != 0) eligible = false;
             else if (floor_enabled && !(point_score < 1.0f)) eligible = false;
             // driver_forces_fallback (reconstruction.py:890-904)
-            if (eligible && (ws.row_gate != 0 || (floor_enabled && point_score >= 1.0f)))
+            if (eligible && (row_gate != 0 || (floor_enabled && point_score >= 1.0f)))
                 eligible = false;
             if (!eligible) meta_out[6 * (int64_t)w + (int64_t)y * w + x] = 0;
         }
@@ -580,6 +607,21 @@ __global__ void __launch_bounds__(Tile<TH>::THREADS, Tile<TH>::BLOCKS_PER_SM)
         if (dtx == 0) S.rowbal[dty] = bal;
     }
     if (!__syncthreads_or(eligible)) return;  // no attempted pixel in the tile
+
+    // The record positions an attempted pixel reads, listed densely (any
+    // order: each record is computed alone): record row r is the centre row
+    // of pixel row r-1 and the cross neighbour of pixel rows r and r-2.
+    for (int i = tid; i < CR * RECC; i += NT) {
+        const int r = i / RECC, c = i % RECC;
+        unsigned long long need = 0;
+        if (r >= 1 && r <= TH) {
+            const unsigned long long b = S.rowbal[r - 1];
+            need |= b | (b << 1) | (b << 2);
+        }
+        if (r < TH) need |= (unsigned long long)S.rowbal[r] << 1;
+        if (r >= 2) need |= (unsigned long long)S.rowbal[r - 2] << 1;
+        if ((need >> c) & 1ull) S.reclist[atomicAdd(&S.nrec, 1)] = (uint16_t)i;
+    }
 
     // One work item is a vertical run of column sums in one column: the
     // samples are loaded and widened once and shared by the run's chains.
@@ -625,25 +667,17 @@ __global__ void __launch_bounds__(Tile<TH>::THREADS, Tile<TH>::BLOCKS_PER_SM)
     __syncthreads();
 
     // ---- feature records (streaming.py:236-308) ---------------------------
-    for (int i = tid; i < CR * RECC; i += NT) {
+    // (the record array overlays the waux tile, dead after the column sums)
+    const int nrec = S.nrec;
+    for (int k = tid; k < nrec; k += NT) {
+        const int i = S.reclist[k];
         const int r = i / RECC, c = i % RECC;
-        {   // read by an attempted pixel: record row r is the centre row of
-            // pixel row r-1 and the cross neighbour of pixel rows r and r-2
-            unsigned long long need = 0;
-            if (r >= 1 && r <= TH) {
-                const unsigned long long b = S.rowbal[r - 1];
-                need |= b | (b << 1) | (b << 2);
-            }
-            if (r < TH) need |= (unsigned long long)S.rowbal[r] << 1;
-            if (r >= 2) need |= (unsigned long long)S.rowbal[r - 2] << 1;
-            if (!((need >> c) & 1ull)) continue;
-        }
         const int xx = x0 - 1 + c;
-        Record rec;
+        StencilRecord rec;
         if (xx < 0 || xx >= w) {
             // horizontal guard records stay zero (streaming.py:281-282)
             rec.a[0] = rec.a[1] = rec.a[2] = rec.a[3] = 0.0f;
-            rec.fb = 0;
+            rec.w[0] = rec.w[1] = rec.w[2] = 0.0f;
         } else {
             double wq[3], nq[3];
 #pragma unroll
@@ -664,22 +698,13 @@ __global__ void __launch_bounds__(Tile<TH>::THREADS, Tile<TH>::BLOCKS_PER_SM)
                 dst[2] = q16;
             }
             const float point_score = S.hs[r + 4][c + 4];
-            rec.fb = 0;
 #pragma unroll
             for (int l = 0; l < 3; ++l) {
-                if (wq[l] > 0.0) {
-                    rec.a[l] = (float)(nq[l] / wq[l]);
-                } else {
-                    rec.a[l] = 0.0f;
-                    rec.fb |= 1u << l;
-                }
+                rec.a[l] = wq[l] > 0.0 ? (float)(nq[l] / wq[l]) : __uint_as_float(kFallbackBits);
+                rec.w[l] = (float)wq[l];
             }
-            if (point_score > 0.0f) {
-                rec.a[3] = S.auxt[r + 3][c + 3 + RO];  // xx is inside the row here
-            } else {
-                rec.a[3] = 0.0f;
-                rec.fb |= 8u;
-            }
+            rec.a[3] = point_score > 0.0f ? S.auxt[r + 3][c + 3 + RO]  // xx is inside the row
+                                          : __uint_as_float(kFallbackBits);
         }
         S.rec[r][c] = rec;
     }
@@ -724,28 +749,20 @@ __global__ void __launch_bounds__(Tile<TH>::THREADS, Tile<TH>::BLOCKS_PER_SM)
     const int rr[5] = {ty + 1, ty + 1, ty + 1, ty, ty + 2};
     const int rc[5] = {tx + 1, tx, tx + 2, tx + 1, tx + 1};
     for (int k = 0; k < records; ++k) {
-        const Record &rec = S.rec[rr[k]][rc[k]];
+        const StencilRecord &rec = S.rec[rr[k]][rc[k]];
 #pragma unroll
-        for (int l = 0; l < 4; ++l) feats[k][l] = (rec.fb >> l) & 1u ? fallback : rec.a[l];
+        for (int l = 0; l < 4; ++l)
+            feats[k][l] = __float_as_uint(rec.a[l]) == kFallbackBits ? fallback : rec.a[l];
     }
+    // W of the centre record (record row ty + 1, column tx + 1): the score
+    // patch averages its record phase computed, and the point score
     float weights[4];
-#pragma unroll
-    {   // W of the centre record: the score patch averages, recomputed from
-        // the column sums (record row ty + 1, column tx + 1)
-        const float(*s3)[CC] = S.cs[0][0];
-        const float(*s5)[CC] = S.cs[0][1];
-        const float(*s7)[CC] = S.cs[0][2];
-        const float(*s9)[CC] = S.cs[0][3];
-        const float(*bb)[CC] = S.cs[0][4];
-        const int r = ty + 1, c = tx + 1;
-        double q69, q21;
-        q69_q21([&](int k) { return s3[r][c + k]; }, [&](int k) { return s5[r][c + k]; },
-                [&](int k) { return s7[r][c + k]; }, [&](int k) { return s9[r][c + k]; }, q69,
-                q21);
-        weights[0] = (float)q69;
-        weights[1] = (float)q21;
-        weights[2] = (float)q16_wa([&](int k) { return bb[r][c + k]; });
-        weights[3] = S.hs[ty + 5][tx + 5];  // point score
+    {
+        const StencilRecord &centre = S.rec[ty + 1][tx + 1];
+        weights[0] = centre.w[0];
+        weights[1] = centre.w[1];
+        weights[2] = centre.w[2];
+        weights[3] = S.hs[ty + 5][tx + 5];
     }
 
     // RGB candidates (reconstruction.py:425-462), one weight at a time: its
