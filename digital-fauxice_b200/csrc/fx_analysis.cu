@@ -8,6 +8,8 @@
 //   k_stencil     streaming.py:454-521: decision gate, five feature records,
 //                 RGB candidates, combiner, then the writer classification
 //   k_startup     startup.py:186-353 hidden centres -6..-1 (RNG-free part)
+#include <cstddef>
+
 #include "fx_internal.cuh"
 
 namespace fx {
@@ -459,20 +461,22 @@ struct StencilRecord {
 };
 constexpr uint32_t kFallbackBits = 0x7FC0FB00u;
 
+// The tiles staged with 16-byte cp.async (hs, hwa, hwr, auxt) start on
+// 16-byte boundaries (checked below); the other members follow them.
 template <int TH>
 struct StencilSmem {
     using T = Tile<TH>;
-    float hs[T::PR][T::SW];
-    union {
+    __align__(16) float hs[T::PR][T::SW];
+    union __align__(16) {
         float hwa[T::PR][T::SW];                // waux tile: dead after the column sums
         StencilRecord rec[T::CR][T::RECC];      // written by the records phase
     };
-    float hwr[3][T::RR][T::SW];                 // staged column j: logical col j - RO
+    __align__(16) float hwr[3][T::RR][T::SW];   // staged column j: logical col j - RO
     float cs[2][5][T::CR][T::CC];               // [score|waux][S3,S5,S7,S9,B16]
     float rcs[3][4][TH][T::RC];                 // [channel][S3,S5,S7,S9]
     uint16_t reclist[T::CR * T::RECC];          // record positions an attempted pixel reads
     int nrec;
-    union {
+    union __align__(16) {
         // aux at clamped (y0-4+r, x0-5+j): decision masks and point aux,
         // dead once the records are built
         float auxt[T::RR][T::SW];
@@ -487,6 +491,14 @@ struct StencilSmem {
     uint32_t rowbal[TH];               // bit x: pixel (row, x) of the tile is attempted
 };
 // four 8-row blocks per SM (228 KB less 1 KB reserved per block); two 16-row
+template <int TH>
+constexpr bool staged_tiles_aligned() {
+    return offsetof(StencilSmem<TH>, hs) % 16 == 0 && offsetof(StencilSmem<TH>, hwa) % 16 == 0 &&
+           offsetof(StencilSmem<TH>, hwr) % 16 == 0 && offsetof(StencilSmem<TH>, auxt) % 16 == 0 &&
+           (Tile<TH>::SW * sizeof(float)) % 16 == 0;
+}
+static_assert(staged_tiles_aligned<8>() && staged_tiles_aligned<16>(),
+              "cp.async 16-byte destinations must start on 16-byte boundaries");
 static_assert(sizeof(StencilSmem<8>) <= 57344, "the 8-row tile keeps four blocks per SM");
 static_assert(sizeof(StencilSmem<16>) <= 115712, "the 16-row tile keeps two blocks per SM");
 static_assert(Tile<8>::RR <= 32 && Tile<16>::RR <= 32, "column masks are 32 bits");

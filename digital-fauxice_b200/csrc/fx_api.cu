@@ -46,6 +46,7 @@ struct Arena {
     uint32_t *seg_base = nullptr, *seg_amb = nullptr;
     AmbEntry *entries = nullptr;
     uint32_t *pos = nullptr, *extra = nullptr;
+    uint8_t *chunk_two = nullptr;
     void *producer = nullptr;
     float *rows = nullptr;
     uint16_t *out = nullptr;
@@ -80,6 +81,7 @@ static size_t arena_layout(const Geometry &g, int64_t amb_cap, Arena *a) {
     const size_t o_ent = take(amb_cap * sizeof(AmbEntry) + 64);
     const size_t o_pos = take(amb_cap * 4);
     const size_t o_ext = take(amb_cap * 4);
+    const size_t o_two = take(walk_chunks(amb_cap));
     const size_t o_prod = take(producer_bytes(g.h, g.w));
     const size_t o_rows = take(4 * (size_t)g.h * 4);
     const size_t o_out = take(px * 6);
@@ -102,6 +104,7 @@ static size_t arena_layout(const Geometry &g, int64_t amb_cap, Arena *a) {
         a->entries = (AmbEntry *)(b + o_ent);
         a->pos = (uint32_t *)(b + o_pos);
         a->extra = (uint32_t *)(b + o_ext);
+        a->chunk_two = (uint8_t *)(b + o_two);
         a->producer = (void *)(b + o_prod);
         a->rows = (float *)(b + o_rows);
         a->out = (uint16_t *)(b + o_out);
@@ -294,7 +297,8 @@ static int enqueue_pass(fx_context *ctx, Slot &s, const Geometry &g, const fx_pa
     const int wave = (ctx->walk_wave > 0 && ctx->walk_wave < g_per_wave) ? ctx->walk_wave
                                                                          : g_per_wave;
     WriterBuffers wb{a.seg_base, a.seg_amb, a.entries, a.pos, a.extra, a.counters,
-                     a.amb_capacity, a.walk, wave, ctx->parallel_walk, ctx->walk_sigmas, cancel};
+                     a.amb_capacity, a.walk, wave, ctx->parallel_walk, ctx->walk_sigmas, cancel,
+                     a.chunk_two};
     FX_CUDA(ctx, launch_writer(g, a.meta, a.cand, d_in, ctx->lut, ctx->high, ctx->low, ctx->ident, a.stages,
                                p, rng, wb, d_out, d_changed, a.err, st, marks));
     return FX_OK;

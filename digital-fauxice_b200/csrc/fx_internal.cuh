@@ -175,6 +175,8 @@ struct WriterBuffers {
     bool parallel_walk;
     double window_sigmas;          // walk window half-width in standard deviations
     const uint32_t *cancel;        // host-mapped cancel word read by the stage gates, or null
+    uint8_t *chunk_two;            // walk_chunks(capacity): 1 when a chunk holds a
+                                   // two-interval entry
 };
 
 // Optional CUDA events between kernel groups (measurement only).
@@ -207,11 +209,18 @@ cudaError_t walk_init();
 size_t walk_scratch_bytes(int64_t capacity, int per_wave);
 int walk_per_wave(int sms);
 constexpr double kDefaultWindowSigmas = 4.5;
+// Channels per staged chunk of the window walk; chunks start at multiples
+// of it in list order (segments are whole chunks).
+constexpr int kWalkChunk = 256;
+__host__ __device__ inline size_t walk_chunks(int64_t capacity) {
+    return (size_t)((capacity + kWalkChunk - 1) / kWalkChunk) + 1;
+}
 cudaError_t launch_walk(const AmbEntry *entries, const uint32_t *pos, const uint32_t *n_ptr,
                         int64_t capacity, uint32_t s0, void *scratch, int per_wave,
-                        bool parallel, double window_sigmas, uint32_t *extra_after,
-                        uint32_t *fallbacks_out, unsigned long long *stats_out,
-                        const uint32_t *err, cudaStream_t stream);
+                        bool parallel, double window_sigmas, const uint8_t *chunk_two,
+                        uint32_t *extra_after, uint32_t *fallbacks_out,
+                        unsigned long long *stats_out, const uint32_t *err,
+                        cudaStream_t stream);
 // Stage gate: when *cancel (host-mapped) is set, stop the pass: err[1] = 1
 // and err[0] = FX_ERR_CANCELLED unless an error came first.  No launch when
 // `cancel` is null.

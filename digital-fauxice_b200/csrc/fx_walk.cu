@@ -30,7 +30,7 @@ constexpr int kWinBlocksPerSM = 3;                  // three segments resident p
 constexpr int kWinSlots = 16;                       // candidates per thread
 constexpr int kWinMax = kWinThreads * kWinSlots;    // 4096 candidates
 constexpr uint32_t kSegLen = 4096;                  // channels per walk segment
-constexpr int kWinChunk = 256;                      // channels staged per chunk
+constexpr int kWinChunk = kWalkChunk;               // channels staged per chunk
 constexpr int kWinRing = 3;                         // staged chunks in flight
 constexpr uint32_t kCompactEvery = 512;             // block compaction period (steady state)
 constexpr uint32_t kSettledCompactEvery = 512;      // the same once at most 256 are left
@@ -81,6 +81,13 @@ __device__ __forceinline__ uint32_t lcg_distance_t(uint32_t from_t, uint32_t to_
 
 __device__ __forceinline__ bool copies(const uint4 &lw, uint32_t T) {
     return ((T - lw.x) <= lw.y) | ((T - lw.z) <= lw.w);
+}
+
+// The copy test of an entry whose copy set is one (cyclic) interval: the
+// second interval is the empty marker, so its test is always false.
+template <bool TWO>
+__device__ __forceinline__ bool copies_of(const uint4 &lw, uint32_t T) {
+    return TWO ? copies(lw, T) : ((T - lw.x) <= lw.y);
 }
 
 __device__ __forceinline__ uint4 intervals(const AmbEntry &e) {
@@ -227,7 +234,7 @@ static_assert(kWinSlots <= 32, "live mask is 32 bits");
 // candidates (merged into a neighbour) keep stepping: their values are
 // never read again, and skipping them would put a divergent branch on every
 // step.
-template <int SLOTS, int LEN>
+template <int SLOTS, int LEN, bool TWO>
 __device__ __forceinline__ void walk_group(const uint4 *r4, uint32_t r, bool tail_next,
                                            uint32_t (&rT)[kWinSlots], uint32_t live_mask,
                                            uint32_t &steps) {
@@ -243,12 +250,13 @@ __device__ __forceinline__ void walk_group(const uint4 *r4, uint32_t r, bool tai
     for (int k = 0; k < LEN; ++k) {
 #pragma unroll
         for (int s = 0; s < SLOTS; ++s)
-            rT[s] = copies(lw[k], rT[s]) ? ac[k].x * rT[s] + ac[k].y : ac[k].z * rT[s] + ac[k].w;
+            rT[s] = copies_of<TWO>(lw[k], rT[s]) ? ac[k].x * rT[s] + ac[k].y
+                                                 : ac[k].z * rT[s] + ac[k].w;
     }
 }
 
 // Single channels (segment and compaction boundaries).
-template <int SLOTS>
+template <int SLOTS, bool TWO>
 __device__ __forceinline__ void walk_one(const uint4 *r4, uint32_t r, bool has_next,
                                          uint32_t (&rT)[kWinSlots], uint32_t live_mask,
                                          uint32_t &steps) {
@@ -257,7 +265,7 @@ __device__ __forceinline__ void walk_one(const uint4 *r4, uint32_t r, bool has_n
     steps += (uint32_t)__popc(live_mask & ((1u << SLOTS) - 1u));
 #pragma unroll
     for (int s = 0; s < SLOTS; ++s)
-        rT[s] = copies(lw, rT[s]) ? ac.x * rT[s] + ac.y : ac.z * rT[s] + ac.w;
+        rT[s] = copies_of<TWO>(lw, rT[s]) ? ac.x * rT[s] + ac.y : ac.z * rT[s] + ac.w;
 }
 
 // Warp-local merge: lanes of one slot hold consecutive candidates; equal
@@ -280,8 +288,9 @@ __device__ __forceinline__ void warp_merge(const uint32_t (&rT)[kWinSlots], uint
     }
 }
 
-// Walk channels [r, stop) of the staged ring for one warp.
-template <int SLOTS>
+// Walk channels [r, stop) of the staged ring for one warp.  TWO: some entry
+// of the staged chunk has two copy intervals.
+template <int SLOTS, bool TWO>
 __device__ __forceinline__ void walk_span(const uint4 *r4, uint32_t r, uint32_t stop,
                                           bool end_next, uint32_t merge_len,
                                           uint32_t (&rT)[kWinSlots], uint32_t &live_mask,
@@ -292,12 +301,12 @@ __device__ __forceinline__ void walk_span(const uint4 *r4, uint32_t r, uint32_t 
     while (r < stop) {
         if (r + kLen <= stop) {
             const bool tail_next = (r + kLen < stop) || end_next;
-            walk_group<SLOTS, kLen>(r4, r, tail_next, rT, live_mask, steps);
+            walk_group<SLOTS, kLen, TWO>(r4, r, tail_next, rT, live_mask, steps);
             r += kLen;
             since += kLen;
         } else {
             const bool has_next = (r + 1 < stop) || end_next;
-            walk_one<SLOTS>(r4, r, has_next, rT, live_mask, steps);
+            walk_one<SLOTS, TWO>(r4, r, has_next, rT, live_mask, steps);
             r += 1;
             since += 1;
         }
@@ -328,7 +337,8 @@ __global__ void __launch_bounds__(kWinThreads, kWinBlocksPerSM)
              const WalkState *__restrict__ st, uint32_t wave, uint32_t per_wave, uint32_t t0,
              SegWindow *__restrict__ windows, uint32_t *__restrict__ table,
              SegList *__restrict__ lists, WalkState *stats, uint32_t serial_below,
-             double sigmas, const uint32_t *__restrict__ err) {
+             double sigmas, const uint8_t *__restrict__ chunk_two,
+             const uint32_t *__restrict__ err) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     WindowSmem &S = *reinterpret_cast<WindowSmem *>(smem_raw);
     if (pass_stopped(err)) return;
@@ -533,6 +543,7 @@ __global__ void __launch_bounds__(kWinThreads, kWinBlocksPerSM)
         const uint4 *r4 = reinterpret_cast<const uint4 *>(S.ring[b]);
         uint32_t r = 0;
         const uint32_t len = c1 - c0;
+        const bool two = chunk_two[c0 / kWinChunk] != 0;  // block-uniform
         while (r < len) {
             const uint32_t done0 = (c0 - i0) + r;
             const uint32_t stop =
@@ -547,14 +558,16 @@ __global__ void __launch_bounds__(kWinThreads, kWinBlocksPerSM)
                 switch (slots) {
 #define FX_WALK_CASE(K)                                                                         \
     case K:                                                                                     \
-        walk_span<K>(r4, r, stop, end_next, merge_len, rT, live_mask, steps);                   \
+        if (two) walk_span<K, true>(r4, r, stop, end_next, merge_len, rT, live_mask, steps);    \
+        else walk_span<K, false>(r4, r, stop, end_next, merge_len, rT, live_mask, steps);       \
         break;
                     FX_WALK_CASE(1) FX_WALK_CASE(2) FX_WALK_CASE(3) FX_WALK_CASE(4)
                     FX_WALK_CASE(5) FX_WALK_CASE(6) FX_WALK_CASE(7) FX_WALK_CASE(8)
                     FX_WALK_CASE(9) FX_WALK_CASE(10) FX_WALK_CASE(11) FX_WALK_CASE(12)
                     FX_WALK_CASE(13) FX_WALK_CASE(14) FX_WALK_CASE(15)
                 default:
-                    walk_span<16>(r4, r, stop, end_next, merge_len, rT, live_mask, steps);
+                    if (two) walk_span<16, true>(r4, r, stop, end_next, merge_len, rT, live_mask, steps);
+                    else walk_span<16, false>(r4, r, stop, end_next, merge_len, rT, live_mask, steps);
                     break;
 #undef FX_WALK_CASE
                 }
@@ -941,9 +954,10 @@ cudaError_t walk_init() {
 // warp instead of the speculative windows.
 cudaError_t launch_walk(const AmbEntry *entries, const uint32_t *pos, const uint32_t *n_ptr,
                         int64_t capacity, uint32_t s0, void *scratch, int per_wave,
-                        bool parallel, double window_sigmas, uint32_t *extra_after,
-                        uint32_t *fallbacks_out, unsigned long long *stats_out,
-                        const uint32_t *err, cudaStream_t stream) {
+                        bool parallel, double window_sigmas, const uint8_t *chunk_two,
+                        uint32_t *extra_after, uint32_t *fallbacks_out,
+                        unsigned long long *stats_out, const uint32_t *err,
+                        cudaStream_t stream) {
     const int64_t segs_max = walk_max_segments(capacity);
     char *p = reinterpret_cast<char *>(scratch);
     auto take = [&](size_t bytes) {
@@ -969,7 +983,7 @@ cudaError_t launch_walk(const AmbEntry *entries, const uint32_t *pos, const uint
             const uint32_t blocks = min((uint32_t)per_wave, segs - w * per_wave);
             k_window<<<blocks, kWinThreads, sizeof(WindowSmem), stream>>>(
                 entries, pos, n_ptr, capacity, mu, var, st, w, per_wave, t0, windows, table,
-                lists, st, serial_below, window_sigmas, err);
+                lists, st, serial_below, window_sigmas, chunk_two, err);
             k_resolve<<<1, kResolveThreads, resolve_smem_bytes(), stream>>>(
                 entries, pos, n_ptr, capacity, st, w, per_wave, t0, windows, table, lists, e_in,
                 serial_below, err);

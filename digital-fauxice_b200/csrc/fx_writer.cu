@@ -313,6 +313,13 @@ __device__ void copy_intervals(const ChannelView &cv, AmbEntry &e, uint32_t *err
     }
     // empty interval: l = 0x80 can never match a T value (low byte zero)
     e.l1 = 0x80u; e.w1 = 0u; e.l2 = 0x80u; e.w2 = 0u;
+    if (intervals == 2 && lo[0] == 0u && hi[1] == kLcgMask) {
+        // [0, hi0] and [lo1, 2^24 - 1] meet across the wrap: one cyclic
+        // interval from lo1 (the test (T - l) <= w wraps modulo 2^32)
+        e.l1 = lo[1] << 8;
+        e.w1 = (hi[0] - lo[1]) << 8;
+        return;
+    }
     if (intervals >= 1) { e.l1 = lo[0] << 8; e.w1 = (hi[0] - lo[0]) << 8; }
     if (intervals == 2) { e.l2 = lo[1] << 8; e.w2 = (hi[1] - lo[1]) << 8; }
 }
@@ -361,7 +368,8 @@ __global__ void k_coef(AmbEntry *__restrict__ entries, const uint32_t *__restric
                        const uint32_t *__restrict__ n_amb_ptr, int64_t capacity,
                        const uint32_t *__restrict__ site_of, const uint8_t *__restrict__ meta,
                        const double *__restrict__ cand, int w, const uint16_t *__restrict__ rgbi,
-                       const float *__restrict__ lut, fx_params p, uint32_t *err) {
+                       const float *__restrict__ lut, fx_params p, uint32_t *err,
+                       uint8_t *__restrict__ chunk_two) {
     if (pass_stopped(err)) return;
     const uint32_t n = (uint32_t)min((int64_t)*n_amb_ptr, capacity);
     const DitherConst dc = dither_const(p);
@@ -390,6 +398,9 @@ __global__ void k_coef(AmbEntry *__restrict__ entries, const uint32_t *__restric
         cv.od = (double)__ldg(lut + lane);
         AmbEntry e;
         copy_intervals(cv, e, err);
+        // a chunk of walk channels with a two-interval entry steps with both
+        // interval tests (every other chunk with one)
+        if (e.l2 != 0x80u) chunk_two[i / kWalkChunk] = 1;
         const uint64_t gap = (i == 0) ? (uint64_t)pos[0] + 1u : (uint64_t)(pos[i] - pos[i - 1]);
         const Affine f = lcg_power_t(gap);
         const Affine f1 = affine_compose(Affine{125u, 256u}, f);  // one more draw
@@ -724,14 +735,15 @@ cudaError_t launch_writer(const Geometry &g, const uint8_t *meta, const double *
     k_amb<<<(unsigned)segs, kSegThreads, 0, stream>>>(meta, g.sites, b.seg_base, b.seg_amb,
                                                       b.extra_after, b.pos, b.capacity, err);
     const uint32_t *n_amb = b.seg_amb + segs;
+    cudaMemsetAsync(b.chunk_two, 0, walk_chunks(b.capacity), stream);
     k_coef<<<1184, 256, 0, stream>>>(b.entries, b.pos, n_amb, b.capacity, b.extra_after, meta,
-                                     cand, g.w, rgbi, lut, p, err);
+                                     cand, g.w, rgbi, lut, p, err, b.chunk_two);
     marks.mark(5, stream);
     e = launch_gate(b.cancel, err, stream);
     if (e != cudaSuccess) return e;
     e = launch_walk(b.entries, b.pos, n_amb, b.capacity, s0, b.walk_scratch, b.per_wave,
-                    b.parallel_walk, b.window_sigmas, b.extra_after, &ctr->walk_fallbacks,
-                    ctr->walk_stats, err, stream);
+                    b.parallel_walk, b.window_sigmas, b.chunk_two, b.extra_after,
+                    &ctr->walk_fallbacks, ctr->walk_stats, err, stream);
     if (e != cudaSuccess) return e;
     marks.mark(6, stream);
     e = launch_gate(b.cancel, err, stream);
