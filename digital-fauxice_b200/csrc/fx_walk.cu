@@ -11,16 +11,18 @@
 //     happen between neighbours in E order;
 //   * candidates merge quickly (the gap is a lazy random walk absorbed at 0).
 //
-// k_window walks one segment for a window of candidate E_in values around
-// the predicted value (expected extras from the exact state-space measure of
-// every copy set), merging candidates as they meet and compacting the
-// survivors, and writes a dense E_in -> E_out table.  k_resolve chains the
-// exact E through a wave of segments with one table read per segment; when
-// E falls outside a window it walks that segment exactly, so correctness
-// never depends on the prediction.  k_rewalk then walks every segment in
-// parallel from its exact E_in and writes the running extra count per
-// channel.  With one segment covering the whole chain, k_rewalk alone is the
-// plain serial walk.
+// A wave of segments is one launch of k_wave.  Its window blocks each walk
+// one segment for a window of candidate E_in values around the predicted
+// value (expected extras from the exact state-space measure of every copy
+// set), merging candidates as they meet and compacting the survivors, and
+// write a dense E_in -> E_out table and a compact survivor list.  Block 0
+// chains the exact E through the wave with one list read per segment, each
+// segment as soon as its window block has finished (per-segment completion
+// flags); when E falls outside a window it walks that segment exactly, so
+// correctness never depends on the prediction.  k_rewalk then walks every
+// segment in parallel from its exact E_in and writes the running extra
+// count per channel.  With one segment covering the whole chain, k_rewalk
+// alone is the plain serial walk.
 #include "fx_internal.cuh"
 
 namespace fx {
@@ -330,22 +332,30 @@ __device__ __forceinline__ int window_slots(uint32_t live) {
     return s > (uint32_t)kWinSlots ? kWinSlots : (int)s;
 }
 
-__global__ void __launch_bounds__(kWinThreads, kWinBlocksPerSM)
-    k_window(const AmbEntry *__restrict__ entries, const uint32_t *__restrict__ pos,
-             const uint32_t *__restrict__ n_ptr, int64_t capacity,
-             const double *__restrict__ seg_mu, const double *__restrict__ seg_var,
-             const WalkState *__restrict__ st, uint32_t wave, uint32_t per_wave, uint32_t t0,
-             SegWindow *__restrict__ windows, uint32_t *__restrict__ table,
-             SegList *__restrict__ lists, WalkState *stats, uint32_t serial_below,
-             double sigmas, const uint8_t *__restrict__ chunk_two,
-             const uint32_t *__restrict__ err) {
+// Release / acquire of the per-segment completion flags (gpu scope).
+__device__ __forceinline__ void flag_release(uint32_t *p, uint32_t v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;\n" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ uint32_t flag_acquire(const uint32_t *p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];\n" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// One segment's window walk: block blk of the wave (segment seg0 + blk).
+// When its table, list and window are written it releases flags[blk] = tag,
+// which the wave's resolve block waits for.
+__device__ __forceinline__ void window_block(
+    const AmbEntry *__restrict__ entries, const uint32_t *__restrict__ pos, uint32_t n,
+    const double *__restrict__ seg_mu, const double *__restrict__ seg_var,
+    const WalkState *st, uint32_t wave, uint32_t per_wave, uint32_t t0,
+    SegWindow *__restrict__ windows, uint32_t *__restrict__ table, SegList *__restrict__ lists,
+    WalkState *stats, double sigmas, const uint8_t *__restrict__ chunk_two, uint32_t blk,
+    uint32_t *flags, uint32_t tag) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     WindowSmem &S = *reinterpret_cast<WindowSmem *>(smem_raw);
-    if (pass_stopped(err)) return;
-    const uint32_t n = (uint32_t)min((int64_t)*n_ptr, capacity);
-    if (n < serial_below) return;  // the chain is walked serially instead
     const uint32_t seg0 = wave * per_wave;
-    const uint32_t j = seg0 + blockIdx.x;
+    const uint32_t j = seg0 + blk;
     const uint32_t i0 = j * kSegLen;
     if (i0 >= n) return;
     const uint32_t i1 = min(n, i0 + kSegLen);
@@ -608,14 +618,14 @@ __global__ void __launch_bounds__(kWinThreads, kWinBlocksPerSM)
     }
 
     // Outputs.  Survivors sit compacted in S.* in E_in order.
-    uint32_t *out = table + (size_t)blockIdx.x * kWinMax;
+    uint32_t *out = table + (size_t)blk * kWinMax;
     for (uint32_t k = tid; k < live; k += kWinThreads) {
         const uint32_t from = S.ein[k] - wlo;
         const uint32_t to = (k + 1 < live) ? S.ein[k + 1] - wlo : count;
         const uint32_t value = S.e[k];
         for (uint32_t m = from; m < to; ++m) out[m] = value;
     }
-    SegList *list = lists + blockIdx.x;
+    SegList *list = lists + blk;
     if (live <= (uint32_t)kListMax) {
         for (uint32_t k = tid; k < live; k += kWinThreads) {
             list->ein[k] = (uint16_t)(S.ein[k] - wlo);
@@ -623,7 +633,7 @@ __global__ void __launch_bounds__(kWinThreads, kWinBlocksPerSM)
         }
     }
     if (tid == 0) {
-        windows[blockIdx.x] = SegWindow{wlo, wlo + count - 1};
+        windows[blk] = SegWindow{wlo, wlo + count - 1};
         list->count = (live <= (uint32_t)kListMax) ? live : 0xFFFFu;
         atomicAdd(&stats->window_sum, (unsigned long long)count);
         atomicAdd(&stats->survivor_sum, (unsigned long long)live);
@@ -631,6 +641,11 @@ __global__ void __launch_bounds__(kWinThreads, kWinBlocksPerSM)
     }
     for (int o = 16; o > 0; o >>= 1) steps += __shfl_down_sync(0xFFFFFFFFu, steps, o);
     if ((tid & 31) == 0 && steps) atomicAdd(&stats->candidate_steps, (unsigned long long)steps);
+    __syncthreads();  // every output of the segment is written
+    if (tid == 0) {
+        __threadfence();
+        flag_release(flags + blk, tag);
+    }
 }
 
 // Exact serial walk of one segment from a known entry count (the fallback).
@@ -661,50 +676,82 @@ __device__ __noinline__ uint32_t resolve_off_list(const AmbEntry *entries, const
                                                   uint32_t n, uint32_t t0, const uint32_t *table,
                                                   SegWindow win, uint32_t E, uint32_t j,
                                                   uint32_t b, uint32_t &fallbacks) {
-    if (E >= win.lo && E <= win.hi) return table[(size_t)b * kWinMax + (E - win.lo)];
+    if (E >= win.lo && E <= win.hi) return __ldcg(table + (size_t)b * kWinMax + (E - win.lo));
     const uint32_t i0 = j * kSegLen, i1 = min(n, i0 + kSegLen);
     fallbacks += 1;
     return walk_segment_exact(entries, pos, i0, i1, E, t0);
 }
 
-constexpr int kResolveChunk = 96;  // lists per staged chunk
-constexpr int kResolveThreads = 512;
+// The resolve block of a wave stages the segments' lists in chunks of
+// kResolveChunk (two chunks in flight within the window kernel's shared
+// memory): warps 1..7 wait for a chunk's window blocks and copy it while
+// warp 0 chains the previous chunk.
+constexpr int kResolveChunk = 32;
+constexpr int kStageWarps = kWinThreads / 32 - 1;
+// A wait for a window block gives up after kFlagSpins polls about 128 ns
+// apart (about half a second), sets an error and stops the wave.
+constexpr uint32_t kFlagSpins = 1u << 22;
 
 struct ResolveSmem {
     SegList list[2][kResolveChunk];
     SegWindow win[2][kResolveChunk];
     uint32_t e_in[2][kResolveChunk];  // exact entry counts found by warp 0
+    int abort;                        // a wait for a window block gave up
 };
+static_assert(sizeof(ResolveSmem) <= sizeof(WindowSmem),
+              "the resolve block runs in a window block's shared memory");
 
-__global__ void __launch_bounds__(kResolveThreads)
-    k_resolve(const AmbEntry *__restrict__ entries, const uint32_t *__restrict__ pos,
-              const uint32_t *__restrict__ n_ptr, int64_t capacity, WalkState *st,
-              uint32_t wave, uint32_t per_wave, uint32_t t0,
-              const SegWindow *__restrict__ windows, const uint32_t *__restrict__ table,
-              const SegList *__restrict__ lists, uint32_t *__restrict__ e_in_exact,
-              uint32_t serial_below, const uint32_t *__restrict__ err) {
+// Resolve one wave: chain the exact E through its segments.  Hops read the
+// window results only through L2 (cp.async.cg, ld.global.cg): the same
+// scratch slots are rewritten every wave, and a line this SM cached in an
+// earlier wave must not be read.
+__device__ void resolve_block(const AmbEntry *__restrict__ entries,
+                              const uint32_t *__restrict__ pos, uint32_t n, WalkState *st,
+                              uint32_t wave, uint32_t per_wave, uint32_t t0,
+                              const SegWindow *__restrict__ windows,
+                              const uint32_t *__restrict__ table,
+                              const SegList *__restrict__ lists, uint32_t *__restrict__ e_in_exact,
+                              const uint32_t *flags, uint32_t tag, uint32_t *err) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ResolveSmem &S = *reinterpret_cast<ResolveSmem *>(smem_raw);
-    if (pass_stopped(err)) return;
-    const uint32_t n = (uint32_t)min((int64_t)*n_ptr, capacity);
-    if (n < serial_below) return;
     const uint32_t segs = (n + kSegLen - 1) / kSegLen;
     const uint32_t here = min(per_wave, segs > wave * per_wave ? segs - wave * per_wave : 0u);
     const uint32_t chunks = (here + kResolveChunk - 1) / kResolveChunk;
     const int tid = threadIdx.x, lane = tid & 31;
+    if (tid == 0) S.abort = 0;
+    __syncthreads();
+    // threads 32..255: wait (warp 1, one lane per segment) until the chunk's
+    // window blocks are done, then copy the chunk
     auto stage = [&](uint32_t c) {
         const uint32_t first = c * kResolveChunk;
         const uint32_t cnt = min((uint32_t)kResolveChunk, here - first);
-        const uint4 *src = reinterpret_cast<const uint4 *>(lists + first);
-        uint4 *dst = reinterpret_cast<uint4 *>(S.list[c & 1]);
-        const uint32_t vecs = cnt * (uint32_t)(sizeof(SegList) / 16);
-        for (uint32_t v = tid - 32; v < vecs; v += kResolveThreads - 32) {
-            const uint32_t sa = (uint32_t)__cvta_generic_to_shared(dst + v);
-            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(src + v));
+        if (tid < 64 && (uint32_t)lane < cnt) {
+            uint32_t spins = 0;
+            while (flag_acquire(flags + first + lane) != tag) {
+                if (++spins > kFlagSpins) {
+                    S.abort = 1;
+                    raise_error(err, FX_ERR_INTERNAL);
+                    break;
+                }
+                __nanosleep(128);
+            }
+        }
+        asm volatile("bar.sync 1, %0;\n" ::"n"(kStageWarps * 32) : "memory");
+        __threadfence();
+        if (!S.abort) {
+            const uint4 *src = reinterpret_cast<const uint4 *>(lists + first);
+            uint4 *dst = reinterpret_cast<uint4 *>(S.list[c & 1]);
+            const uint32_t vecs = cnt * (uint32_t)(sizeof(SegList) / 16);
+            for (uint32_t v = tid - 32; v < vecs; v += kWinThreads - 32) {
+                const uint32_t sa = (uint32_t)__cvta_generic_to_shared(dst + v);
+                asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(src + v));
+            }
+            for (uint32_t bb = tid - 32; bb < cnt; bb += kWinThreads - 32) {
+                const uint2 wv = __ldcg(reinterpret_cast<const uint2 *>(windows + first + bb));
+                S.win[c & 1][bb] = SegWindow{wv.x, wv.y};
+            }
         }
         asm volatile("cp.async.commit_group;\n" ::);
-        for (uint32_t b = tid - 32; b < cnt; b += kResolveThreads - 32)
-            S.win[c & 1][b] = windows[first + b];
     };
     if (tid >= 32 && chunks > 0) stage(0);
     uint32_t E = st->e_wave;
@@ -712,6 +759,7 @@ __global__ void __launch_bounds__(kResolveThreads)
     for (uint32_t c = 0; c < chunks; ++c) {
         if (tid >= 32) asm volatile("cp.async.wait_group 0;\n" ::);
         __syncthreads();  // chunk c visible; warp 0 is done with chunk c-1
+        if (S.abort) break;
         if (tid >= 32) {
             if (c + 1 < chunks) stage(c + 1);
             continue;
@@ -767,11 +815,39 @@ __global__ void __launch_bounds__(kResolveThreads)
         for (uint32_t bb = lane; bb < cnt_c; bb += 32)
             e_in_exact[wave * per_wave + first + bb] = S.e_in[c & 1][bb];
     }
-    if (tid == 0) {
+    if (tid == 0 && !S.abort) {
         st->e_wave = E;
         st->waves += 1;
         st->fallbacks += fallbacks;
     }
+}
+
+// One wave of the speculative walk in one launch: block 0 resolves the wave
+// (chaining the exact entry count through its segments as their window
+// blocks finish, segment by segment), blocks 1.. walk one segment's window
+// each.  Only block 0 waits, and only for window blocks, which wait for
+// nothing: they always finish, whichever blocks are resident.
+__global__ void __launch_bounds__(kWinThreads, kWinBlocksPerSM)
+    k_wave(const AmbEntry *__restrict__ entries, const uint32_t *__restrict__ pos,
+           const uint32_t *__restrict__ n_ptr, int64_t capacity,
+           const double *__restrict__ seg_mu, const double *__restrict__ seg_var, WalkState *st,
+           uint32_t wave, uint32_t per_wave, uint32_t t0, SegWindow *__restrict__ windows,
+           uint32_t *__restrict__ table, SegList *__restrict__ lists,
+           uint32_t *__restrict__ e_in_exact, uint32_t serial_below, double sigmas,
+           const uint8_t *__restrict__ chunk_two, uint32_t *flags, uint32_t *err) {
+    if (pass_stopped(err)) return;
+    const uint32_t n = (uint32_t)min((int64_t)*n_ptr, capacity);
+    if (n < serial_below) return;  // the chain is walked serially instead
+    const uint32_t tag = wave + 1;  // flags are cleared once per pass
+    if (blockIdx.x == 0) {
+        resolve_block(entries, pos, n, st, wave, per_wave, t0, windows, table, lists, e_in_exact,
+                      flags, tag, err);
+        return;
+    }
+    const uint32_t b = blockIdx.x - 1;
+    if ((wave * per_wave + b) * (uint64_t)kSegLen >= n) return;  // past the chain: no flag
+    window_block(entries, pos, n, seg_mu, seg_var, st, wave, per_wave, t0, windows, table, lists,
+                 st, sigmas, chunk_two, b, flags, tag);
 }
 
 // ---------------------------------------------------------------------------
@@ -929,19 +1005,16 @@ size_t walk_scratch_bytes(int64_t capacity, int per_wave) {
     add((size_t)per_wave * kWinMax * sizeof(uint32_t));
     add((size_t)per_wave * sizeof(SegList));
     add(sizeof(WalkState));
+    add((size_t)per_wave * sizeof(uint32_t));  // completion flags of a wave's windows
     return b;
 }
 
-static size_t resolve_smem_bytes() { return sizeof(ResolveSmem); }
 
 int walk_per_wave(int sms) { return kWinBlocksPerSM * sms; }
 
 cudaError_t walk_init() {
-    cudaError_t e = cudaFuncSetAttribute(k_window, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(k_wave, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)sizeof(WindowSmem));
-    if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_resolve, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)resolve_smem_bytes());
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(k_rewalk, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)sizeof(RewalkSmem));
@@ -972,21 +1045,22 @@ cudaError_t launch_walk(const AmbEntry *entries, const uint32_t *pos, const uint
     uint32_t *table = (uint32_t *)take((size_t)per_wave * kWinMax * sizeof(uint32_t));
     SegList *lists = (SegList *)take((size_t)per_wave * sizeof(SegList));
     WalkState *st = (WalkState *)take(sizeof(WalkState));
+    uint32_t *flags = (uint32_t *)take((size_t)per_wave * sizeof(uint32_t));
     const uint32_t t0 = (s0 & kLcgMask) << 8;
     const uint32_t serial_below = parallel ? kSerialBelow : 0xFFFFFFFFu;
     cudaMemsetAsync(st, 0, sizeof(WalkState), stream);
+    cudaMemsetAsync(flags, 0, (size_t)per_wave * sizeof(uint32_t), stream);
     const uint32_t segs = (uint32_t)segs_max;
     if (parallel) {
         const uint32_t waves = (segs + per_wave - 1) / per_wave;
         k_seg_prob<<<segs, 256, 0, stream>>>(entries, n_ptr, capacity, mu, var, err);
         for (uint32_t w = 0; w < waves; ++w) {
-            const uint32_t blocks = min((uint32_t)per_wave, segs - w * per_wave);
-            k_window<<<blocks, kWinThreads, sizeof(WindowSmem), stream>>>(
+            // block 0 resolves the wave, blocks 1.. walk its windows
+            const uint32_t blocks = min((uint32_t)per_wave, segs - w * per_wave) + 1u;
+            k_wave<<<blocks, kWinThreads, sizeof(WindowSmem), stream>>>(
                 entries, pos, n_ptr, capacity, mu, var, st, w, per_wave, t0, windows, table,
-                lists, st, serial_below, window_sigmas, chunk_two, err);
-            k_resolve<<<1, kResolveThreads, resolve_smem_bytes(), stream>>>(
-                entries, pos, n_ptr, capacity, st, w, per_wave, t0, windows, table, lists, e_in,
-                serial_below, err);
+                lists, e_in, serial_below, window_sigmas, chunk_two, flags,
+                const_cast<uint32_t *>(err));
         }
     }
     constexpr uint32_t kRewalkPerBlock = kRewalkWarps * kRewalkLanes;
