@@ -60,19 +60,21 @@ SERVE_RATES = (2.0, 8.0, 32.0, 400.0)  # the last one above the GPU's capacity
 NCU_COUNTERS = os.path.join(ROOT, "profiles", "ncu_counters.json")
 
 
-WALK_BLOCKS_PER_SM = 3   # window-walk segments per SM in one wave (kWinBlocksPerSM)
+WALK_BLOCKS_PER_SM = 3   # window-walk blocks per SM in one wave (kWinBlocksPerSM)
 
 
-def launches_per_frame(h: int, w: int, per_wave: int) -> int:
+def launches_per_frame(h: int, w: int, sms: int) -> int:
     """Kernel launches of one plain pass (the library's launch sequence):
-    producer 3, planes 1, stencil 1, startup 1, chain 4, walk 1 + 2 per wave
-    + 1, apply 3.  Waves are sized from the RNG-dependent list capacity."""
+    producer 3, planes 1, stencil 1, startup 1, chain 4, walk 1 + 1 per wave
+    + 1, apply 3.  Waves are sized from the RNG-dependent list capacity, with
+    three window blocks per SM less one slot for the wave's resolve block."""
 
     sites = 6 * w + h * w
     capacity = max(65536, sites // 2)
     segments = (capacity + 4095) // 4096 + 1
+    per_wave = WALK_BLOCKS_PER_SM * sms - 1
     waves = (segments + per_wave - 1) // per_wave
-    return 15 + 2 * waves
+    return 15 + waves
 
 
 def ncu_counter(kernel: str, name: str):
@@ -626,8 +628,8 @@ def run_b200(args, world, rank, local, frames=None, heavy=None, pool=None):
             "cpu_baseline": cpu,
             "e2e": e2e,
             "clocks": clocks,
-            "gpu_launches": launches_per_frame(h, w, WALK_BLOCKS_PER_SM * torch.cuda.get_device_properties(
-                local).multi_processor_count) * args.steps,
+            "gpu_launches": launches_per_frame(
+                h, w, torch.cuda.get_device_properties(local).multi_processor_count) * args.steps,
             "rng_dependent_channels": int(counters.rng_dependent),
             "walk_fallback_segments": int(counters.walk_fallbacks),
             "walk_candidate_steps": int(counters.walk_candidate_steps),

@@ -1010,7 +1010,11 @@ size_t walk_scratch_bytes(int64_t capacity, int per_wave) {
 }
 
 
-int walk_per_wave(int sms) { return kWinBlocksPerSM * sms; }
+// Segments per wave: three window blocks per SM, less one slot for the
+// wave's resolve block, so every block of a wave is resident at once (a
+// window block left waiting for a slot would start late, and it would be
+// the wave's last, widest window).
+int walk_per_wave(int sms) { return kWinBlocksPerSM * sms - 1; }
 
 cudaError_t walk_init() {
     cudaError_t e = cudaFuncSetAttribute(k_wave, cudaFuncAttributeMaxDynamicSharedMemorySize,
