@@ -39,21 +39,27 @@ __device__ __forceinline__ float aux_value(const uint2 raw, const fx_stage &st, 
 }
 
 // One padded row segment of the history planes (streaming.py:111-147,
-// 201-233), with the auxiliary plane computed on the way: each thread
-// computes the aux of its own column (the edge threads also their outer
-// neighbour's, for the horizontal minimum).  History planes: rows above the
+// 201-233), with the auxiliary plane computed on the way.  A block of 256
+// threads covers kPlaneCols = 254 columns: thread t computes the aux of
+// column base + t - 1, so the first and last thread compute only the
+// segment's outer neighbours for the horizontal minimum and every thread
+// computes one aux value.  History planes: rows above the
 // image take the pseudo row, rows below repeat the last row, columns outside
 // are zero.  The auxiliary plane is written padded too, but edge-replicated
 // (the decision bars clamp their indices, streaming.py:166-198): padded
 // (y, x) holds the aux of (clamp(y), clamp(x)).
+constexpr int kPlaneCols = 254;  // output columns per 256-thread k_planes block
+
 __global__ void __launch_bounds__(256)
     k_planes(const uint16_t *__restrict__ rgbi, Geometry g, const float *__restrict__ lut,
              const fx_stage *__restrict__ stages, fx_params p, float *__restrict__ auxp,
              float *__restrict__ hs, float *__restrict__ hwa, float *__restrict__ hwr,
              int64_t plane, uint32_t *err) {
-    __shared__ float s_aux[256 + 2];  // aux of columns x-1 .. x+256 of the segment
+    __shared__ float s_aux[256];  // aux of columns base-1 .. base+254 of the segment
     if (pass_stopped(err)) return;
-    const int px = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = threadIdx.x;
+    const bool owner = t >= 1 && t <= kPlaneCols;  // threads 0 and 255: neighbours only
+    const int px = blockIdx.x * kPlaneCols + t - 1;
     const int py = blockIdx.y;
     const int y = py - kPad, x = px - kPad;
     const bool live = y >= -1;  // rows above the pseudo row are zero
@@ -61,31 +67,23 @@ __global__ void __launch_bounds__(256)
     const int64_t row0 = (int64_t)r * g.w;
     const fx_stage ast = stages[r];  // stage y+1 (stage_parameters.py:207-212)
     const bool inside = x >= 0 && x < g.w;
-    const bool own = live && px < g.pitch && inside;
+    const bool own = live && px >= 0 && px < g.pitch && inside;
     uint2 raw = make_uint2(0u, 0u);
     float a = 0.0f;
-    if (px < g.pitch) {
+    if (px >= 0 && px < g.pitch) {
         // the aux of (clamp(y), clamp(x)), for the edge-replicated plane
         const int xc = x < 0 ? 0 : (x < g.w ? x : g.w - 1);
         const uint2 rc = reinterpret_cast<const uint2 *>(rgbi)[row0 + xc];
         const float ac = aux_value(rc, ast, p.visible_channel, lut, err);
-        auxp[(int64_t)py * g.pitch + px] = ac;
+        if (owner) auxp[(int64_t)py * g.pitch + px] = ac;
         if (own) {
             raw = rc;
             a = ac;
         }
     }
-    s_aux[threadIdx.x + 1] = a;
-    if (threadIdx.x == 0 || threadIdx.x == blockDim.x - 1) {
-        const int xe = threadIdx.x == 0 ? x - 1 : x + 1;
-        float ae = 0.0f;
-        if (live && xe >= 0 && xe < g.w)
-            ae = aux_value(reinterpret_cast<const uint2 *>(rgbi)[row0 + xe], ast,
-                           p.visible_channel, lut, err);
-        s_aux[threadIdx.x == 0 ? 0 : blockDim.x + 1] = ae;
-    }
+    s_aux[t] = a;  // 0 outside the row, as the horizontal minimum's guard needs
     __syncthreads();
-    if (px >= g.pitch) return;
+    if (!owner || px < 0 || px >= g.pitch) return;
     const float floor = p.score_floor;
     float s = 0.0f, wa = 0.0f, wr[3] = {0.0f, 0.0f, 0.0f};
     if (own) {
@@ -99,7 +97,7 @@ __global__ void __launch_bounds__(256)
         } else {
             float sample = a;
             if (p.horizontal_minimum && g.w > 2 && x > 0 && x < g.w - 1) {
-                const float l = s_aux[threadIdx.x], rr = s_aux[threadIdx.x + 2];
+                const float l = s_aux[t - 1], rr = s_aux[t + 1];
                 const float m = (l < a) ? l : a;
                 sample = (m < rr) ? m : rr;
             }
@@ -620,19 +618,33 @@ __global__ void __launch_bounds__(Tile<TH>::THREADS, Tile<TH>::BLOCKS_PER_SM)
     }
     if (!__syncthreads_or(eligible)) return;  // no attempted pixel in the tile
 
-    // The record positions an attempted pixel reads, listed densely (any
-    // order: each record is computed alone): record row r is the centre row
-    // of pixel row r-1 and the cross neighbour of pixel rows r and r-2.
-    for (int i = tid; i < CR * RECC; i += NT) {
-        const int r = i / RECC, c = i % RECC;
-        unsigned long long need = 0;
-        if (r >= 1 && r <= TH) {
-            const unsigned long long b = S.rowbal[r - 1];
-            need |= b | (b << 1) | (b << 2);
+    // The record positions an attempted pixel reads, listed densely: record
+    // row r is the centre row of pixel row r-1 and the cross neighbour of
+    // pixel rows r and r-2.  Each warp appends its positions in order (one
+    // ballot, one shared atomic), so neighbouring lanes of the record phase
+    // read neighbouring columns of the column sums.
+    {
+        const int lane = tid & 31;
+        for (int base = tid - lane; base < CR * RECC; base += NT) {
+            const int i = base + lane;
+            bool needed = false;
+            if (i < CR * RECC) {
+                const int r = i / RECC, c = i % RECC;
+                unsigned long long need = 0;
+                if (r >= 1 && r <= TH) {
+                    const unsigned long long b = S.rowbal[r - 1];
+                    need |= b | (b << 1) | (b << 2);
+                }
+                if (r < TH) need |= (unsigned long long)S.rowbal[r] << 1;
+                if (r >= 2) need |= (unsigned long long)S.rowbal[r - 2] << 1;
+                needed = (need >> c) & 1ull;
+            }
+            const uint32_t bal = __ballot_sync(0xFFFFFFFFu, needed);
+            int at = 0;
+            if (lane == 0 && bal) at = atomicAdd(&S.nrec, __popc(bal));
+            at = __shfl_sync(0xFFFFFFFFu, at, 0);
+            if (needed) S.reclist[at + __popc(bal & ((1u << lane) - 1u))] = (uint16_t)i;
         }
-        if (r < TH) need |= (unsigned long long)S.rowbal[r] << 1;
-        if (r >= 2) need |= (unsigned long long)S.rowbal[r - 2] << 1;
-        if ((need >> c) & 1ull) S.reclist[atomicAdd(&S.nrec, 1)] = (uint16_t)i;
     }
 
     // One work item is a vertical run of column sums in one column: the
@@ -982,7 +994,7 @@ cudaError_t launch_analysis(const uint16_t *rgbi, const Geometry &g, const float
                             int tile_rows) {
     const CombineConst cc = combine_const(p);
     {
-        dim3 block(256), grid((g.pitch + 255) / 256, g.prow);
+        dim3 block(256), grid((g.pitch + kPlaneCols - 1) / kPlaneCols, g.prow);
         k_planes<<<grid, block, 0, stream>>>(rgbi, g, lut, stages, p, aux, hs, hwa, hwr, plane,
                                              err);
     }

@@ -118,6 +118,7 @@ static size_t arena_layout(const Geometry &g, int64_t amb_cap, Arena *a) {
 }
 
 struct Slot {
+    int64_t cap_hint = 0;  // the longest RNG-dependent list this slot has needed
     cudaStream_t stream = nullptr;
     cudaStream_t last_stream = nullptr;  // stream of the last device-buffer pass
     cudaEvent_t done = nullptr;
@@ -159,6 +160,8 @@ struct fx_context {
     int walk_wave = 0;  // window segments per wave; 0: g_per_wave (three per SM)
     double walk_sigmas = fx::kDefaultWindowSigmas;  // walk window half-width
     int stencil_rows = 8;  // stencil tile height: 8 (four blocks per SM) or 16 (two)
+    int top_priority = 0;     // the device's greatest launch priority
+    bool use_priority = true;  // chain and walk launched at top_priority
     int64_t list_capacity = 0;  // RNG-dependent list entries per frame; 0: sites / 2
     std::vector<std::vector<cudaEvent_t>> pending;  // recorded, not yet read
     std::vector<std::vector<cudaEvent_t>> spare;
@@ -184,6 +187,25 @@ namespace fx {
 // fx_set_list_capacity when one is set, else sites / 2 (at least 65536).
 static int64_t amb_capacity(const fx_context *ctx, const Geometry &g) {
     return ctx->list_capacity > 0 ? ctx->list_capacity : default_amb_capacity(g);
+}
+
+// The list capacity of a pass on slot s: the frame's own (amb_capacity),
+// raised to the longest list the slot has needed before, so that a slot
+// that once overflowed (heavy damage) does not overflow again on the next
+// such frame.  Never above three channels per site, the most a frame can
+// list: a small frame on a slot that held a heavy one keeps a short walk
+// launch shape.  The fx_set_list_capacity override is taken as given.
+static int64_t pass_capacity(const fx_context *ctx, const Slot &s, const Geometry &g) {
+    const int64_t cap = amb_capacity(ctx, g);
+    if (ctx->list_capacity > 0) return cap;
+    const int64_t most = 3 * g.sites;
+    const int64_t hint = s.cap_hint < most ? s.cap_hint : most;
+    return hint > cap ? hint : cap;
+}
+
+// After an overflow: the slot's next passes list at least `cap` channels.
+static void note_capacity(Slot &s, int64_t cap) {
+    if (cap > s.cap_hint) s.cap_hint = cap;
 }
 
 static char g_error[512];
@@ -285,7 +307,8 @@ static int enqueue_pass(fx_context *ctx, Slot &s, const Geometry &g, const fx_pa
                                      cudaMemcpyHostToDevice, st));
     } else {
         FX_CUDA(ctx, launch_producer(d_in, g.h, g.w, ctx->lut, a.producer, a.stages,
-                                     producer_rows ? a.rows : nullptr, a.err, st));
+                                     producer_rows ? a.rows : nullptr, a.err, st,
+                                     ctx->use_priority ? ctx->top_priority : 0));
     }
     marks.mark(1, st);
     const uint32_t *cancel = cancellable ? s.cancel_dev : nullptr;
@@ -298,7 +321,7 @@ static int enqueue_pass(fx_context *ctx, Slot &s, const Geometry &g, const fx_pa
                                                                          : g_per_wave;
     WriterBuffers wb{a.seg_base, a.seg_amb, a.entries, a.pos, a.extra, a.counters,
                      a.amb_capacity, a.walk, wave, ctx->parallel_walk, ctx->walk_sigmas, cancel,
-                     a.chunk_two};
+                     a.chunk_two, ctx->use_priority ? ctx->top_priority : 0};
     FX_CUDA(ctx, launch_writer(g, a.meta, a.cand, d_in, ctx->lut, ctx->high, ctx->low, ctx->ident, a.stages,
                                p, rng, wb, d_out, d_changed, a.err, st, marks));
     return FX_OK;
@@ -392,9 +415,7 @@ static int ensure_slots(fx_context *ctx, int n) {
 static int run_device(fx_context *ctx, Slot &s, const Geometry &g, const fx_params &p,
                       const fx_stage *stages, uint32_t rng, const uint16_t *d_in, uint16_t *d_out,
                       uint8_t *d_changed, fx_counters *counters, bool producer_rows) {
-    int64_t cap = s.arena.base ? s.arena.amb_capacity : default_amb_capacity(g);
-    if (cap < default_amb_capacity(g)) cap = default_amb_capacity(g);
-    if (ctx->list_capacity > 0) cap = ctx->list_capacity;
+    int64_t cap = pass_capacity(ctx, s, g);
     for (int attempt = 0; attempt < 2; ++attempt) {
         // keep caller-side device pointers stable: the arena may move only
         // when the input/outputs live in it
@@ -416,8 +437,12 @@ static int run_device(fx_context *ctx, Slot &s, const Geometry &g, const fx_para
         bool overflow;
         rc = finish_counters(ctx, s, hc, err, counters, &overflow);
         if (rc) return rc;
-        if (!overflow) return FX_OK;
+        if (!overflow) {
+            if (counters) counters->capacity_reruns = attempt;
+            return FX_OK;
+        }
         cap = (int64_t)counters_n_amb(hc) + 1024;
+        note_capacity(s, cap);
         if (!d_in) return fail(ctx, FX_ERR_INTERNAL, "amb capacity retry needs the input");
     }
     return fail(ctx, FX_ERR_INTERNAL, "amb capacity retry failed");
@@ -471,6 +496,9 @@ FX_API int fx_context_create(int device, fx_context **out) {
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess &&
         sms > 0)
         g_per_wave = walk_per_wave(sms);
+    int least = 0, greatest = 0;
+    if (cudaDeviceGetStreamPriorityRange(&least, &greatest) == cudaSuccess)
+        ctx->top_priority = greatest;
     if (analysis_init() != cudaSuccess || ensure_slots(ctx, 1) != FX_OK ||
         cudaMalloc(&ctx->lut, 65536 * 4) != cudaSuccess ||
         cudaMalloc(&ctx->high, 256 * 4) != cudaSuccess ||
@@ -728,7 +756,7 @@ FX_API int fx_process(fx_context *ctx, const fx_frame *f, fx_counters *counters)
     Slot &s = slot0(ctx);
     const Geometry g = make_geometry(f->height, f->width);
     const size_t px = (size_t)g.h * g.w;
-    int64_t cap = amb_capacity(ctx, g);
+    int64_t cap = pass_capacity(ctx, s, g);
     for (int attempt = 0; attempt < 2; ++attempt) {
         rc = ensure_arena(ctx, s, g, cap);
         if (rc) return rc;
@@ -750,8 +778,10 @@ FX_API int fx_process(fx_context *ctx, const fx_frame *f, fx_counters *counters)
         if (rc) return rc;
         if (overflow) {
             cap = (int64_t)counters_n_amb(hc) + 1024;
+            note_capacity(s, cap);
             continue;
         }
+        if (counters) counters->capacity_reruns = attempt;
         ctx->digest_valid = false;
         rc = staged_download(ctx, s, f->rgb_out, s.arena.out, px * 6,
                              ctx->hash_output ? ctx->digest : nullptr);
@@ -789,7 +819,7 @@ FX_API int fx_process_device(fx_context *ctx, const uint16_t *d_rgbi, int32_t h,
     if (counters) {
         rc = run_device(ctx, s, g, *params, stages, rng, d_rgbi, d_out, d_changed, counters, false);
     } else {
-        rc = ensure_arena(ctx, s, g, amb_capacity(ctx, g));
+        rc = ensure_arena(ctx, s, g, pass_capacity(ctx, s, g));
         if (!rc) rc = enqueue_pass(ctx, s, g, *params, stages, rng, d_rgbi, d_out, d_changed, false);
     }
     s.last_stream = s.stream;
@@ -848,6 +878,13 @@ FX_API int fx_output_digest(fx_context *ctx, uint8_t *digest) {
     return FX_OK;
 }
 
+FX_API int fx_set_launch_priority(fx_context *ctx, int enable) {
+    if (!ctx) return FX_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    ctx->use_priority = enable != 0;
+    return FX_OK;
+}
+
 FX_API int fx_set_walk_wave(fx_context *ctx, int32_t segments) {
     if (!ctx || segments < 0) return FX_ERR_INVALID_ARGUMENT;
     std::lock_guard<std::mutex> lock(ctx->mu);
@@ -866,9 +903,7 @@ FX_API int fx_reserve_frames(fx_context *ctx, int32_t max_height, int32_t max_wi
     const Geometry g = make_geometry(max_height, max_width);
     for (Slot &s : ctx->slots) {
         if (s.busy) return fail(ctx, FX_ERR_INVALID_ARGUMENT, "a slot is busy: reserve first");
-        const int64_t cap = s.arena.base && s.arena.amb_capacity > amb_capacity(ctx, g)
-                                ? s.arena.amb_capacity
-                                : amb_capacity(ctx, g);
+        const int64_t cap = pass_capacity(ctx, s, g);
         const int rc = ensure_arena(ctx, s, g, cap);
         if (rc) return rc;
     }
@@ -889,9 +924,7 @@ FX_API int fx_reserve_slots(fx_context *ctx, int32_t count, int32_t max_height,
     for (int k = 0; k < count; ++k) {
         Slot &s = ctx->slots[k];
         if (s.busy) return fail(ctx, FX_ERR_INVALID_ARGUMENT, "a slot is busy: reserve first");
-        const int64_t cap = s.arena.base && s.arena.amb_capacity > amb_capacity(ctx, g)
-                                ? s.arena.amb_capacity
-                                : amb_capacity(ctx, g);
+        const int64_t cap = pass_capacity(ctx, s, g);
         rc = ensure_arena(ctx, s, g, cap);
         if (rc) return rc;
     }
@@ -949,7 +982,6 @@ static int stage_host_results(fx_context *ctx, Slot &s) {
 // slot with the largest arena (which then grows: a cudaFree, which waits
 // for the whole device).
 static Slot *free_slot(fx_context *ctx, const Geometry &g) {
-    const size_t need = arena_layout(g, amb_capacity(ctx, g), nullptr);
     Slot *fit = nullptr, *empty = nullptr, *largest = nullptr;
     for (Slot &s : ctx->slots) {
         if (s.busy) continue;
@@ -957,6 +989,7 @@ static Slot *free_slot(fx_context *ctx, const Geometry &g) {
             if (!empty) empty = &s;
             continue;
         }
+        const size_t need = arena_layout(g, pass_capacity(ctx, s, g), nullptr);
         if (s.arena.bytes >= need && (!fit || s.arena.bytes < fit->arena.bytes)) fit = &s;
         if (!largest || s.arena.bytes > largest->arena.bytes) largest = &s;
     }
@@ -976,7 +1009,7 @@ FX_API int fx_submit(fx_context *ctx, const fx_frame *f, int64_t *ticket) {
     if (!slot) return fail(ctx, FX_PENDING, "no free slot");
     Slot &s = *slot;
     const size_t px = (size_t)g.h * g.w;
-    rc = ensure_arena(ctx, s, g, amb_capacity(ctx, g));
+    rc = ensure_arena(ctx, s, g, pass_capacity(ctx, s, g));
     if (rc) return rc;
     const size_t in_bytes = px * 8;
     const size_t out_bytes = px * 6 + px * 4 + px;
@@ -1051,7 +1084,7 @@ FX_API int fx_submit_device(fx_context *ctx, const uint16_t *d_rgbi, int32_t h, 
     Slot *slot = free_slot(ctx, g);
     if (!slot) return fail(ctx, FX_PENDING, "no free slot");
     Slot &s = *slot;
-    rc = ensure_arena(ctx, s, g, amb_capacity(ctx, g));
+    rc = ensure_arena(ctx, s, g, pass_capacity(ctx, s, g));
     if (rc) return rc;
     s.frame = fx_frame{};
     s.frame.height = h;
@@ -1120,6 +1153,7 @@ struct FetchTargets {
 static int rerun_with_capacity(fx_context *ctx, Slot &s, fx_counters *counters) {
     char *hc = reinterpret_cast<char *>(s.h_ctr);
     const int64_t cap = (int64_t)counters_n_amb(hc) + 1024;
+    note_capacity(s, cap);
     int rc = ensure_arena(ctx, s, s.g, cap);
     if (rc) return rc;
     if (s.device) {
@@ -1143,6 +1177,7 @@ static int rerun_with_capacity(fx_context *ctx, Slot &s, fx_counters *counters) 
     bool overflow;
     rc = finish_counters(ctx, s, hc, err, counters, &overflow);
     if (!rc && overflow) rc = fail(ctx, FX_ERR_INTERNAL, "capacity rerun overflowed");
+    if (!rc && counters) counters->capacity_reruns = 1;
     return rc;
 }
 

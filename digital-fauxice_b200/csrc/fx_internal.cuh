@@ -8,6 +8,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <utility>
+
 #include "../../include/fauxice_b200.h"
 
 namespace fx {
@@ -177,7 +179,28 @@ struct WriterBuffers {
     const uint32_t *cancel;        // host-mapped cancel word read by the stage gates, or null
     uint8_t *chunk_two;            // walk_chunks(capacity): 1 when a chunk holds a
                                    // two-interval entry
+    int priority;                  // launch priority of the chain and the walk (0: default)
 };
+
+// A kernel launch with an execution priority (cudaLaunchAttributePriority;
+// numerically lower is higher, 0 is the default).  When several streams
+// have work pending, the block scheduler dispatches the blocks of the
+// higher-priority launch first; results do not depend on it.
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_prio(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                               cudaStream_t stream, int priority, Args &&...args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributePriority;
+    attr[0].val.priority = priority;
+    cfg.attrs = attr;
+    cfg.numAttrs = priority ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
 
 // Optional CUDA events between kernel groups (measurement only).
 // mark(i) records boundary i: 0 before the producer, then after each stage.
@@ -220,7 +243,7 @@ cudaError_t launch_walk(const AmbEntry *entries, const uint32_t *pos, const uint
                         bool parallel, double window_sigmas, const uint8_t *chunk_two,
                         uint32_t *extra_after, uint32_t *fallbacks_out,
                         unsigned long long *stats_out, const uint32_t *err,
-                        cudaStream_t stream);
+                        cudaStream_t stream, int priority);
 // Stage gate: when *cancel (host-mapped) is set, stop the pass: err[1] = 1
 // and err[0] = FX_ERR_CANCELLED unless an error came first.  No launch when
 // `cancel` is null.
@@ -230,7 +253,7 @@ uint32_t counters_n_amb(const void *dev_copy);
 size_t producer_bytes(int h, int w);
 cudaError_t launch_producer(const uint16_t *rgbi, int h, int w, const float *lut, void *scratch,
                             fx_stage *stages, float *rows_out, uint32_t *err,
-                            cudaStream_t stream);
+                            cudaStream_t stream, int priority = 0);
 int host_reduce_prepass(const uint16_t *px, int h, int w, const float *lut, uint8_t payload[64],
                         int64_t *valid_pixels, int64_t *fully_valid_tiles);
 int host_stage_table(int h, const float *p1, const float *p2, const float *mv, const float *mi,

@@ -564,7 +564,7 @@ size_t producer_bytes(int h, int w) {
 
 cudaError_t launch_producer(const uint16_t *rgbi, int h, int w, const float *lut, void *scratch,
                             fx_stage *stages, float *rows_out, uint32_t *err,
-                            cudaStream_t stream) {
+                            cudaStream_t stream, int priority) {
     const int aw = (w / 8) * 8, cells = aw / 8, ne = h / 8;
     ProducerBuffers b;
     char *p = reinterpret_cast<char *>(scratch);
@@ -581,8 +581,14 @@ cudaError_t launch_producer(const uint16_t *rgbi, int h, int w, const float *lut
     b.p_epoch = (float *)take(2 * (size_t)ne * sizeof(float));
     k_producer_rows<<<(h + kRows - 1) / kRows, kRowWarps * 32, sizeof(RowSmem), stream>>>(rgbi, h, w, aw,
                                                                                cells, lut, b);
-    k_producer_scan<<<1, kScanThreads, sizeof(ScanSmem), stream>>>(h, ne, b);
-    k_stage_table<<<(h + 6 + 255) / 256, 256, 0, stream>>>(h, ne, 1.0f, b, stages, rows_out, err);
+    // the scan is one block: given priority, it starts as soon as the row
+    // sums are done even when other frames' kernels have blocks pending
+    cudaError_t e = launch_prio(k_producer_scan, dim3(1), dim3(kScanThreads), sizeof(ScanSmem),
+                                stream, priority, h, ne, b);
+    if (e != cudaSuccess) return e;
+    e = launch_prio(k_stage_table, dim3((h + 6 + 255) / 256), dim3(256), 0, stream, priority, h,
+                    ne, 1.0f, b, stages, rows_out, err);
+    if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }
 

@@ -1034,7 +1034,7 @@ cudaError_t launch_walk(const AmbEntry *entries, const uint32_t *pos, const uint
                         bool parallel, double window_sigmas, const uint8_t *chunk_two,
                         uint32_t *extra_after, uint32_t *fallbacks_out,
                         unsigned long long *stats_out, const uint32_t *err,
-                        cudaStream_t stream) {
+                        cudaStream_t stream, int priority) {
     const int64_t segs_max = walk_max_segments(capacity);
     char *p = reinterpret_cast<char *>(scratch);
     auto take = [&](size_t bytes) {
@@ -1057,20 +1057,25 @@ cudaError_t launch_walk(const AmbEntry *entries, const uint32_t *pos, const uint
     const uint32_t segs = (uint32_t)segs_max;
     if (parallel) {
         const uint32_t waves = (segs + per_wave - 1) / per_wave;
-        k_seg_prob<<<segs, 256, 0, stream>>>(entries, n_ptr, capacity, mu, var, err);
+        cudaError_t e = launch_prio(k_seg_prob, dim3(segs), dim3(256), 0, stream, priority,
+                                    entries, n_ptr, capacity, mu, var, err);
+        if (e != cudaSuccess) return e;
         for (uint32_t w = 0; w < waves; ++w) {
             // block 0 resolves the wave, blocks 1.. walk its windows
             const uint32_t blocks = min((uint32_t)per_wave, segs - w * per_wave) + 1u;
-            k_wave<<<blocks, kWinThreads, sizeof(WindowSmem), stream>>>(
-                entries, pos, n_ptr, capacity, mu, var, st, w, per_wave, t0, windows, table,
-                lists, e_in, serial_below, window_sigmas, chunk_two, flags,
-                const_cast<uint32_t *>(err));
+            e = launch_prio(k_wave, dim3(blocks), dim3(kWinThreads), sizeof(WindowSmem), stream,
+                            priority, entries, pos, n_ptr, capacity, mu, var, st, w, per_wave, t0,
+                            windows, table, lists, e_in, serial_below, window_sigmas, chunk_two,
+                            flags, const_cast<uint32_t *>(err));
+            if (e != cudaSuccess) return e;
         }
     }
     constexpr uint32_t kRewalkPerBlock = kRewalkWarps * kRewalkLanes;
-    k_rewalk<<<(segs + kRewalkPerBlock - 1) / kRewalkPerBlock, kRewalkWarps * 32, sizeof(RewalkSmem),
-               stream>>>(entries, pos, n_ptr, capacity, kSegLen, e_in, t0, extra_after,
-                         serial_below, err);
+    cudaError_t e = launch_prio(k_rewalk, dim3((segs + kRewalkPerBlock - 1) / kRewalkPerBlock),
+                                dim3(kRewalkWarps * 32), sizeof(RewalkSmem), stream, priority,
+                                entries, pos, n_ptr, capacity, (uint32_t)kSegLen, e_in, t0,
+                                extra_after, serial_below, err);
+    if (e != cudaSuccess) return e;
     // fallbacks_out[0] = segments walked exactly, fallbacks_out[1] = packed segments
     if (fallbacks_out)
         cudaMemcpyAsync(fallbacks_out, &st->fallbacks, 2 * sizeof(uint32_t),

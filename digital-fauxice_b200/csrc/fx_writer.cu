@@ -728,22 +728,32 @@ cudaError_t launch_writer(const Geometry &g, const uint8_t *meta, const double *
     cudaMemsetAsync(ctr, 0, sizeof(DevCounters), stream);
     cudaError_t e = launch_gate(b.cancel, err, stream);
     if (e != cudaSuccess) return e;
-    k_seg_sums<<<(unsigned)segs, kSegThreads, 0, stream>>>(meta, g.sites, b.seg_base, b.seg_amb,
-                                                           err);
-    k_seg_scan<<<1, 1024, 0, stream>>>(b.seg_base, b.seg_amb, segs, err);
+    // the chain and the walk are latency-bound: launched with b.priority, so
+    // that with several frames in flight their blocks are dispatched ahead
+    // of other frames' stencil and apply blocks, which fill the SMs they
+    // leave idle
+    const int pr = b.priority;
+    e = launch_prio(k_seg_sums, dim3((unsigned)segs), dim3(kSegThreads), 0, stream, pr, meta,
+                    g.sites, b.seg_base, b.seg_amb, err);
+    if (e != cudaSuccess) return e;
+    e = launch_prio(k_seg_scan, dim3(1), dim3(1024), 0, stream, pr, b.seg_base, b.seg_amb, segs,
+                    err);
+    if (e != cudaSuccess) return e;
     // the site list lives in extra_after until the walk writes the counts
-    k_amb<<<(unsigned)segs, kSegThreads, 0, stream>>>(meta, g.sites, b.seg_base, b.seg_amb,
-                                                      b.extra_after, b.pos, b.capacity, err);
+    e = launch_prio(k_amb, dim3((unsigned)segs), dim3(kSegThreads), 0, stream, pr, meta, g.sites,
+                    b.seg_base, b.seg_amb, b.extra_after, b.pos, b.capacity, err);
+    if (e != cudaSuccess) return e;
     const uint32_t *n_amb = b.seg_amb + segs;
     cudaMemsetAsync(b.chunk_two, 0, walk_chunks(b.capacity), stream);
-    k_coef<<<1184, 256, 0, stream>>>(b.entries, b.pos, n_amb, b.capacity, b.extra_after, meta,
-                                     cand, g.w, rgbi, lut, p, err, b.chunk_two);
+    e = launch_prio(k_coef, dim3(1184), dim3(256), 0, stream, pr, b.entries, b.pos, n_amb,
+                    b.capacity, b.extra_after, meta, cand, g.w, rgbi, lut, p, err, b.chunk_two);
+    if (e != cudaSuccess) return e;
     marks.mark(5, stream);
     e = launch_gate(b.cancel, err, stream);
     if (e != cudaSuccess) return e;
     e = launch_walk(b.entries, b.pos, n_amb, b.capacity, s0, b.walk_scratch, b.per_wave,
                     b.parallel_walk, b.window_sigmas, b.chunk_two, b.extra_after,
-                    &ctr->walk_fallbacks, ctr->walk_stats, err, stream);
+                    &ctr->walk_fallbacks, ctr->walk_stats, err, stream, pr);
     if (e != cudaSuccess) return e;
     marks.mark(6, stream);
     e = launch_gate(b.cancel, err, stream);
@@ -793,6 +803,7 @@ void counters_to_host(const void *dev_copy, fx_counters *out) {
     out->walk_candidates = (int64_t)c.walk_stats[1];
     out->walk_survivors = (int64_t)c.walk_stats[2];
     out->walk_packed_segments = (int64_t)c.walk_packed;
+    out->capacity_reruns = 0;  // set by the host when the pass runs again
 }
 
 uint32_t counters_n_amb(const void *dev_copy) {

@@ -103,6 +103,7 @@ class FxCounters(ctypes.Structure):
         ("walk_candidates", ctypes.c_int64),
         ("walk_survivors", ctypes.c_int64),
         ("walk_packed_segments", ctypes.c_int64),
+        ("capacity_reruns", ctypes.c_int64),
     ]
 
 
@@ -142,6 +143,7 @@ SIGNATURES = {
     "fx_set_slots": ([_P, ctypes.c_int32], ctypes.c_int),
     "fx_set_parallel_walk": ([_P, ctypes.c_int], ctypes.c_int),
     "fx_set_walk_wave": ([_P, ctypes.c_int32], ctypes.c_int),
+    "fx_set_launch_priority": ([_P, ctypes.c_int], ctypes.c_int),
     "fx_set_output_digest": ([_P, ctypes.c_int], ctypes.c_int),
     "fx_reserve_frames": ([_P, ctypes.c_int32, ctypes.c_int32], ctypes.c_int),
     "fx_output_digest": ([_P, _P], ctypes.c_int),

@@ -99,6 +99,15 @@ def set_stencil_tile(ctx: _lib.Context, rows: int) -> None:
         _check(ctx, _lib.load().fx_set_stencil_tile(ctx.handle, int(rows)))
 
 
+def set_launch_priority(ctx: _lib.Context, enable: bool) -> None:
+    """Launch the latency-bound kernels (producer scan, writer chain, walk)
+    at the device's greatest priority (the default), or every kernel at the
+    default priority."""
+
+    with ctx.lock:
+        _check(ctx, _lib.load().fx_set_launch_priority(ctx.handle, 1 if enable else 0))
+
+
 def run_device_batch(ctx: _lib.Context, frames: Sequence[DeviceFrame], *, slots: int = 4,
                      params: _lib.FxParams | None = None) -> list[_lib.FxCounters]:
     """Process device-resident frames with up to ``slots`` in flight.

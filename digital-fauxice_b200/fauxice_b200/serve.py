@@ -84,6 +84,11 @@ class ServeReport:
     releases: int = 0          # times the idle slots' buffers were released
     verified: int = 0          # outputs compared with their single-frame output
     mismatches: int = 0        # differing uint16 values over all verified outputs
+    slowest_call_s: dict = field(default_factory=dict)  # device call -> longest host time
+
+    def note_call(self, name: str, seconds: float) -> None:
+        if seconds > self.slowest_call_s.get(name, 0.0):
+            self.slowest_call_s[name] = seconds
 
     def percentile_ms(self, q: float, attr: str = "latency_s") -> float:
         lat = np.array([getattr(c, attr) for c in self.completions]) * 1e3
@@ -101,7 +106,11 @@ class ServeReport:
                "peak_device_bytes": self.peak_bytes,
                "budget_bytes": self.budget_bytes,
                "slots_used": self.slots_used,
-               "buffer_releases": self.releases}
+               "buffer_releases": self.releases,
+               "capacity_reruns": int(sum(getattr(c.counters, "capacity_reruns", 0)
+                                          for c in self.completions)),
+               "slowest_call_ms": {k: round(v * 1e3, 2)
+                                   for k, v in sorted(self.slowest_call_s.items())}}
         if self.verified:
             out["verified"] = self.verified
             out["bit_exact"] = self.mismatches == 0 and self.verified == len(self.completions)
@@ -350,6 +359,15 @@ def serve(ctx: _lib.Context | None, requests: Sequence[Request], *, max_slots: i
     def now() -> float:
         return time.perf_counter() - start
 
+    def call(name: str, fn, *args):
+        """A device call of the loop, with its host time noted: the loop is
+        single-threaded, so a call that blocks delays every request."""
+
+        t0 = time.perf_counter()
+        out = fn(*args)
+        report.note_call(name, time.perf_counter() - t0)
+        return out
+
     while nxt < len(requests) or waiting or staging or inflight or downloads:
         t = now()
         while nxt < len(requests) and requests[nxt].arrival_s <= t:
@@ -367,7 +385,7 @@ def serve(ctx: _lib.Context | None, requests: Sequence[Request], *, max_slots: i
                 if staging or inflight or downloads or not model.free_sizes:
                     break  # wait for a request in flight to finish
                 # nothing in flight: drop the idle buffers and start afresh
-                dev.release_idle()
+                call("release_idle", dev.release_idle)
                 model.release_idle()
                 report.releases += 1
                 continue
@@ -375,25 +393,25 @@ def serve(ctx: _lib.Context | None, requests: Sequence[Request], *, max_slots: i
             st = {"i": i, "h": h, "w": w, "admitted": now(), "size": model.take(choice),
                   "planes": planes, "host": free_host.popleft()}
             in_use_bytes += planes
-            dev.upload(st, requests[i].pixels)
+            call("upload", dev.upload, st, requests[i].pixels)
             staging.append(st)
         report.max_in_flight = max(report.max_in_flight,
                                    len(staging) + len(inflight) + len(downloads))
         report.peak_bytes = max(report.peak_bytes, model.allocated + in_use_bytes)
         # submission: uploads that have landed go to a library slot
         while staging and dev.landed(staging[0]):
-            ticket = dev.submit(staging[0])
+            ticket = call("submit", dev.submit, staging[0])
             if ticket is None:
                 break
             inflight[ticket] = staging.popleft()
         # finished passes: counters, then the output's copy to host memory
         for ticket in list(inflight):
-            if not dev.done(ticket):
+            if not call("poll", dev.done, ticket):
                 continue
             st = inflight.pop(ticket)
-            st["counters"] = dev.finish(ticket)
+            st["counters"] = call("finish", dev.finish, ticket)
             expected = requests[st["i"]].expected
-            dev.download(st, expected)
+            call("download", dev.download, st, expected)
             if expected is not None:
                 report.verified += 1
             downloads.append(st)

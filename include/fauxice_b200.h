@@ -100,6 +100,9 @@ typedef struct fx_counters {
     int64_t walk_candidate_steps, walk_candidates, walk_survivors; /* walk work */
     int64_t walk_packed_segments; /* segments whose settled phase ran two
                                      candidates per lane (walk diagnostics) */
+    int64_t capacity_reruns;      /* 1 when the pass ran a second time because
+                                     its RNG-dependent list overflowed (the
+                                     slot then keeps the larger list) */
 } fx_counters;
 
 /* One frame for fx_process / fx_submit.  Host pointers. */
@@ -207,6 +210,13 @@ FX_API int fx_set_parallel_walk(fx_context *ctx, int enable);
  * candidate windows (less total work, for throughput when several frames
  * are in flight) and more waves (longer latency for one frame). */
 FX_API int fx_set_walk_wave(fx_context *ctx, int32_t segments);
+/* 1 (default): the latency-bound kernels of a pass (the producer's scan, the
+ * writer's prefix, interval and jump kernels, the walk) are launched at the
+ * device's greatest execution priority, so that with several frames in
+ * flight their blocks are dispatched ahead of other frames' stencil and
+ * emit blocks; 0: every launch at the default priority.  No effect on
+ * results, nor on a single frame (no reference counterpart). */
+FX_API int fx_set_launch_priority(fx_context *ctx, int enable);
 /* SHA-256 of the RGB16 output of fx_process, little-endian bytes in
  * row-major order (the replay result's output_sha256, streaming.py:533-536).
  * When enabled, fx_process hashes each staged chunk of the output as soon as

@@ -63,12 +63,18 @@ def test_device_batch_matches_single_frame_runs(golden):
     torch.cuda.synchronize()
     jobs = [batch.DeviceFrame(d.data_ptr(), f.shape[0], f.shape[1], o.data_ptr())
             for f, d, o in zip(frames, d_in, outs)]
-    for slots in (3, 6):  # two rounds in a row: slots and arenas are reused
-        counters = batch.run_device_batch(ctx, jobs, slots=slots)
-        for k in range(len(frames)):
-            got = outs[k].cpu().numpy().view(np.uint16)
-            assert np.array_equal(got, alone_out[k]), (slots, k)
-            assert _counters(counters[k]) == alone_ctr[k], (slots, k)
+    # rounds in a row: slots and arenas are reused; the launch priority of
+    # the chain and the walk changes only the order blocks are dispatched in
+    try:
+        for slots, priority in ((3, True), (6, True), (4, False)):
+            batch.set_launch_priority(ctx, priority)
+            counters = batch.run_device_batch(ctx, jobs, slots=slots)
+            for k in range(len(frames)):
+                got = outs[k].cpu().numpy().view(np.uint16)
+                assert np.array_equal(got, alone_out[k]), (slots, priority, k)
+                assert _counters(counters[k]) == alone_ctr[k], (slots, priority, k)
+    finally:
+        batch.set_launch_priority(ctx, True)
     expected = golden["jobs"]["batch_3"]
     assert sha(alone_out[2]) == expected["output_sha256"]
 

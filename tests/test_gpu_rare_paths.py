@@ -102,6 +102,7 @@ def test_list_overflow_reruns_fx_process(golden):
     with _knobs(ctx, capacity=4096):
         outcome = _run(ctx, "batch_3")
     assert outcome.counters.rng_dependent > 4096  # the first pass overflowed
+    assert outcome.counters.capacity_reruns == 1
     assert _mismatches(golden, "batch_3", outcome) == []
 
 
@@ -139,6 +140,7 @@ def test_list_overflow_reruns_fx_submit_device(golden):
     expected = golden["jobs"]["batch_3"]
     for out, ctr in zip(outs, counters):
         assert ctr.rng_dependent > 4096
+        assert ctr.capacity_reruns == 1
         assert sha(out.cpu().numpy().view(np.uint16)) == expected["output_sha256"]
         assert ctr.final_state == expected["final_rng_state"]
         assert ctr.public_advances == expected["public_rng_advances"]
@@ -163,8 +165,52 @@ def test_list_overflow_reruns_fx_process_device(golden):
     assert rc == 0, ctx._error(ctx.handle)
     expected = golden["jobs"]["batch_3"]
     assert ctr.rng_dependent > 4096
+    assert ctr.capacity_reruns == 1
     assert sha(out.cpu().numpy().view(np.uint16)) == expected["output_sha256"]
     assert ctr.final_state == expected["final_rng_state"]
+
+
+def test_a_slot_that_overflowed_keeps_the_longer_list(golden):
+    """Heavy damage lists more RNG-dependent channels than the default list
+    holds (half the sites).  On a fresh context the first pass reruns with a
+    longer list and the slot keeps it, so the next heavy frame on that slot
+    runs once; through fx_process and through fx_submit_device, each on its
+    own fresh context.  Every result equals the reference's."""
+
+    import torch
+
+    from fauxice_b200.profile import factor_tables, response_lut
+
+    high, low = factor_tables()
+    params = DEFAULT_PROFILE.hot_path_parameters().to_c()
+    px = _frame("heavy_full_0")
+    h, w = px.shape[:2]
+    expected = golden["jobs"]["heavy_full_0"]
+    fresh = _lib.Context(0, lut=response_lut(), high=high, low=low)
+    try:
+        first = engine.run_frame(fresh, px, params, None, NIKON_PE_INITIAL_STATE, True)
+        second = engine.run_frame(fresh, px, params, None, NIKON_PE_INITIAL_STATE, True)
+    finally:
+        fresh.close()
+    assert first.counters.rng_dependent > (6 * w + h * w) // 2
+    assert [first.counters.capacity_reruns, second.counters.capacity_reruns] == [1, 0]
+    for outcome in (first, second):
+        assert _mismatches(golden, "heavy_full_0", outcome) == []
+
+    fresh = _lib.Context(0, lut=response_lut(), high=high, low=low)
+    try:
+        d_in = torch.from_numpy(px.view(np.int16).copy()).to("cuda")
+        outs = [torch.full((h, w, 3), -1, dtype=torch.int16, device="cuda") for _ in range(2)]
+        torch.cuda.synchronize()
+        reruns = []
+        for out in outs:  # one slot: the second request finds the longer list
+            frame = batch.DeviceFrame(d_in.data_ptr(), h, w, out.data_ptr())
+            reruns += [c.capacity_reruns for c in batch.run_device_batch(fresh, [frame], slots=1)]
+    finally:
+        fresh.close()
+    assert reruns == [1, 0]
+    for out in outs:
+        assert sha(out.cpu().numpy().view(np.uint16)) == expected["output_sha256"]
 
 
 def test_one_warp_serial_walk(golden):

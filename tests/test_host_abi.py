@@ -49,7 +49,7 @@ def test_struct_layouts_match_the_oracle():
     assert ctypes.sizeof(_lib.FxParams) == ctypes.sizeof(ox.OxParams)
     assert _lib.STAGE_DTYPE.itemsize == ox.STAGE_DTYPE.itemsize
     # fx_counters carries walk diagnostics beyond the reference's counters
-    assert ctypes.sizeof(_lib.FxCounters) == ctypes.sizeof(ox.OxCounters) + 6 * 8
+    assert ctypes.sizeof(_lib.FxCounters) == ctypes.sizeof(ox.OxCounters) + 7 * 8
 
 
 def test_request_entry_points_reject_bad_arguments():
