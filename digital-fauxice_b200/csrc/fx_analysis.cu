@@ -618,33 +618,21 @@ __global__ void __launch_bounds__(Tile<TH>::THREADS, Tile<TH>::BLOCKS_PER_SM)
     }
     if (!__syncthreads_or(eligible)) return;  // no attempted pixel in the tile
 
-    // The record positions an attempted pixel reads, listed densely: record
-    // row r is the centre row of pixel row r-1 and the cross neighbour of
-    // pixel rows r and r-2.  Each warp appends its positions in order (one
-    // ballot, one shared atomic), so neighbouring lanes of the record phase
-    // read neighbouring columns of the column sums.
-    {
-        const int lane = tid & 31;
-        for (int base = tid - lane; base < CR * RECC; base += NT) {
-            const int i = base + lane;
-            bool needed = false;
-            if (i < CR * RECC) {
-                const int r = i / RECC, c = i % RECC;
-                unsigned long long need = 0;
-                if (r >= 1 && r <= TH) {
-                    const unsigned long long b = S.rowbal[r - 1];
-                    need |= b | (b << 1) | (b << 2);
-                }
-                if (r < TH) need |= (unsigned long long)S.rowbal[r] << 1;
-                if (r >= 2) need |= (unsigned long long)S.rowbal[r - 2] << 1;
-                needed = (need >> c) & 1ull;
-            }
-            const uint32_t bal = __ballot_sync(0xFFFFFFFFu, needed);
-            int at = 0;
-            if (lane == 0 && bal) at = atomicAdd(&S.nrec, __popc(bal));
-            at = __shfl_sync(0xFFFFFFFFu, at, 0);
-            if (needed) S.reclist[at + __popc(bal & ((1u << lane) - 1u))] = (uint16_t)i;
+    // The record positions an attempted pixel reads, listed densely (any
+    // order: each record is computed alone): record row r is the centre row
+    // of pixel row r-1 and the cross neighbour of pixel rows r and r-2.
+    // (A warp-ordered list, by ballot and one atomic per warp, measured 2%
+    // more instructions and no fewer shared-memory bank conflicts.)
+    for (int i = tid; i < CR * RECC; i += NT) {
+        const int r = i / RECC, c = i % RECC;
+        unsigned long long need = 0;
+        if (r >= 1 && r <= TH) {
+            const unsigned long long b = S.rowbal[r - 1];
+            need |= b | (b << 1) | (b << 2);
         }
+        if (r < TH) need |= (unsigned long long)S.rowbal[r] << 1;
+        if (r >= 2) need |= (unsigned long long)S.rowbal[r - 2] << 1;
+        if ((need >> c) & 1ull) S.reclist[atomicAdd(&S.nrec, 1)] = (uint16_t)i;
     }
 
     // One work item is a vertical run of column sums in one column: the

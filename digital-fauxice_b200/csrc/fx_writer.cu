@@ -113,47 +113,80 @@ __device__ __forceinline__ void load_meta(const uint8_t *meta, int64_t first, in
     }
 }
 
-__global__ void k_seg_sums(const uint8_t *__restrict__ meta, int64_t sites,
-                           uint32_t *__restrict__ seg_base, uint32_t *__restrict__ seg_amb,
-                           const uint32_t *__restrict__ err) {
-    __shared__ uint32_t scratch[kSegThreads / 32];
+// (fixed draws << 16) | RNG-dependent channels of the four sites of one
+// meta word.  Per channel code k (bits 2c, 2c+1): fixed draws k, except 1
+// for k = 3, and one RNG-dependent channel when k = 3; so over the lows
+// (k & 1), highs (k >> 1) and both: fixed = lows + 2 highs - 2 both.
+__device__ __forceinline__ uint32_t packed_word(uint32_t w) {
+    const uint32_t lo = w & 0x15151515u, hi = (w >> 1) & 0x15151515u;
+    const uint32_t amb = (uint32_t)__popc(lo & hi);
+    const uint32_t base = (uint32_t)__popc(lo) + 2u * (uint32_t)__popc(hi) - 2u * amb;
+    return (base << 16) | amb;
+}
+
+__device__ __forceinline__ uint32_t packed_site(uint8_t m) {
+    return ((uint32_t)meta_base(m) << 16) | (uint32_t)meta_amb(m);
+}
+
+constexpr int kSegWarps = 8;  // segments per block of the chain kernels (one per warp)
+
+// Fixed draws and RNG-dependent channels of every segment: one warp per
+// segment, 32 sites per lane in two 16-byte loads (the meta array starts on
+// a 256-byte boundary and segments on multiples of 1024 sites).
+__global__ void __launch_bounds__(kSegWarps * 32)
+    k_seg_sums(const uint8_t *__restrict__ meta, int64_t sites, int64_t segs,
+               uint32_t *__restrict__ seg_base, uint32_t *__restrict__ seg_amb,
+               const uint32_t *__restrict__ err) {
     if (pass_stopped(err)) return;
-    const int64_t first = (int64_t)blockIdx.x * kSegment + threadIdx.x * kPer;
-    uint8_t m[kPer];
-    load_meta(meta, first, sites, m);
+    const int lane = threadIdx.x & 31;
+    const int64_t seg = (int64_t)blockIdx.x * kSegWarps + (threadIdx.x >> 5);
+    if (seg >= segs) return;
+    const int64_t first = seg * kSegment + lane * 32;
     uint32_t packed = 0;
+    if (first + 32 <= sites) {
+        const uint4 *q = reinterpret_cast<const uint4 *>(meta + first);
+        const uint4 u = q[0], v = q[1];
+        packed = packed_word(u.x) + packed_word(u.y) + packed_word(u.z) + packed_word(u.w) +
+                 packed_word(v.x) + packed_word(v.y) + packed_word(v.z) + packed_word(v.w);
+    } else {
+        for (int i = 0; i < 32; ++i)
+            if (first + i < sites) packed += packed_site(meta[first + i]);
+    }
 #pragma unroll
-    for (int i = 0; i < kPer; ++i) packed += ((uint32_t)meta_base(m[i]) << 16) | meta_amb(m[i]);
-    const uint32_t total = block_sum<kSegThreads, uint32_t>(packed, scratch);
-    if (threadIdx.x == 0) {
-        seg_base[blockIdx.x] = total >> 16;
-        seg_amb[blockIdx.x] = total & 0xFFFFu;
+    for (int o = 16; o > 0; o >>= 1) packed += __shfl_xor_sync(0xFFFFFFFFu, packed, o);
+    if (lane == 0) {
+        seg_base[seg] = packed >> 16;
+        seg_amb[seg] = packed & 0xFFFFu;
     }
 }
 
-// Exclusive scan of the per-segment sums; entry [n] holds the totals.
+// Exclusive scan of the per-segment sums; entry [n] holds the totals.  One
+// block: each thread sums a contiguous run of segments, one block scan
+// gives the runs' offsets, and each thread writes its run's prefixes.
 __global__ void k_seg_scan(uint32_t *__restrict__ seg_base, uint32_t *__restrict__ seg_amb,
                            int64_t n, const uint32_t *__restrict__ err) {
     __shared__ uint32_t ws[32];
     if (pass_stopped(err)) return;
-    uint32_t carry_b = 0, carry_a = 0;
-    for (int64_t base = 0; base < n; base += 1024) {
-        const int64_t i = base + threadIdx.x;
-        const uint32_t vb = (i < n) ? seg_base[i] : 0u;
-        const uint32_t va = (i < n) ? seg_amb[i] : 0u;
-        uint32_t tb, ta;
-        const uint32_t eb = block_exclusive_scan<1024>(vb, tb, ws);
-        const uint32_t ea = block_exclusive_scan<1024>(va, ta, ws);
-        if (i < n) {
-            seg_base[i] = carry_b + eb;
-            seg_amb[i] = carry_a + ea;
-        }
-        carry_b += tb;
-        carry_a += ta;
+    const int64_t per = (n + 1023) / 1024;
+    const int64_t lo = min(n, per * (int64_t)threadIdx.x), hi = min(n, lo + per);
+    uint32_t sb = 0, sa = 0;
+    for (int64_t i = lo; i < hi; ++i) {
+        sb += seg_base[i];
+        sa += seg_amb[i];
+    }
+    uint32_t tb, ta;
+    uint32_t eb = block_exclusive_scan<1024>(sb, tb, ws);
+    uint32_t ea = block_exclusive_scan<1024>(sa, ta, ws);
+    for (int64_t i = lo; i < hi; ++i) {
+        const uint32_t vb = seg_base[i], va = seg_amb[i];
+        seg_base[i] = eb;
+        seg_amb[i] = ea;
+        eb += vb;
+        ea += va;
     }
     if (threadIdx.x == 0) {
-        seg_base[n] = carry_b;
-        seg_amb[n] = carry_a;
+        seg_base[n] = tb;
+        seg_amb[n] = ta;
     }
 }
 
@@ -326,28 +359,44 @@ __device__ void copy_intervals(const ChannelView &cv, AmbEntry &e, uint32_t *err
 
 // Lists every RNG-dependent channel in chain order: entry a gets its site
 // (site_of[a], a compact array so the writes coalesce) and its draw
-// position; k_coef fills in the intervals and jumps.
-__global__ void __launch_bounds__(kSegThreads)
-    k_amb(const uint8_t *__restrict__ meta, int64_t sites, const uint32_t *__restrict__ seg_base,
-          const uint32_t *__restrict__ seg_amb, uint32_t *__restrict__ site_of,
-          uint32_t *__restrict__ pos_out, int64_t capacity, const uint32_t *__restrict__ err) {
-    __shared__ uint32_t ws[kSegThreads / 32];
+// position; k_coef fills in the intervals and jumps.  One warp per segment,
+// in 32 rounds of 32 consecutive sites (all the segment's meta loads issued
+// first); a round's offsets come from one warp scan, so a round's entries
+// are written by consecutive lanes to consecutive list positions.
+__global__ void __launch_bounds__(kSegWarps * 32)
+    k_amb(const uint8_t *__restrict__ meta, int64_t sites, int64_t segs,
+          const uint32_t *__restrict__ seg_base, const uint32_t *__restrict__ seg_amb,
+          uint32_t *__restrict__ site_of, uint32_t *__restrict__ pos_out, int64_t capacity,
+          const uint32_t *__restrict__ err) {
     if (pass_stopped(err)) return;
-    const int64_t first = (int64_t)blockIdx.x * kSegment + threadIdx.x * kPer;
-    uint8_t m[kPer];
-    load_meta(meta, first, sites, m);
-    uint32_t P, A;
-    site_offsets(m, seg_base, seg_amb, ws, P, A);
+    const int lane = threadIdx.x & 31;
+    const int64_t seg = (int64_t)blockIdx.x * kSegWarps + (threadIdx.x >> 5);
+    if (seg >= segs) return;
+    const int64_t first = seg * kSegment + lane;
+    uint8_t m[32];
 #pragma unroll
-    for (int i = 0; i < kPer; ++i) {
-        if (meta_amb(m[i])) {
-            uint32_t pos = P, a = A;
+    for (int r = 0; r < 32; ++r) m[r] = (first + 32 * r < sites) ? meta[first + 32 * r] : 0;
+    uint32_t P = seg_base[seg], A = seg_amb[seg];
+#pragma unroll
+    for (int r = 0; r < 32; ++r) {
+        const uint8_t mi = m[r];
+        const uint32_t x = packed_site(mi);
+        uint32_t inc = x;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, inc, o);
+            if (lane >= o) inc += y;
+        }
+        const uint32_t total = __shfl_sync(0xFFFFFFFFu, inc, 31);
+        const uint32_t ex = inc - x;
+        if (x & 0xFFFFu) {
+            uint32_t pos = P + (ex >> 16), a = A + (ex & 0xFFFFu);
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-                const int code = meta_code(m[i], c);
+                const int code = meta_code(mi, c);
                 if (code == 3) {
                     if ((int64_t)a < capacity) {
-                        site_of[a] = (uint32_t)(first + i);
+                        site_of[a] = (uint32_t)(first + 32 * r);
                         pos_out[a] = pos;
                     }
                     ++a;
@@ -357,13 +406,58 @@ __global__ void __launch_bounds__(kSegThreads)
                 }
             }
         }
-        P += meta_base(m[i]);
-        A += meta_amb(m[i]);
+        P += total >> 16;
+        A += total & 0xFFFFu;
     }
 }
 
-// One thread per listed channel: its copy intervals (from the exact binary64
-// predicates) and the affine jumps from the previous listed channel.
+// k_coef's inputs of one entry, gathered in two dependent steps: the list
+// (coalesced) gives the site, the site gives its meta, pixel and candidates.
+struct CoefList {
+    uint32_t site, gap_lo, gap_hi;  // gap_lo/hi: pos[i-1] (0 for the first) and pos[i]
+    int k;                          // this entry is the k-th of its site
+};
+struct CoefSite {
+    uint8_t meta;
+    uint2 raw;
+    double cand[3];
+};
+
+__device__ __forceinline__ CoefList coef_list(const uint32_t *__restrict__ site_of,
+                                              const uint32_t *__restrict__ pos, uint32_t i,
+                                              uint32_t n) {
+    CoefList l{0u, 0u, 0u, 0};
+    if (i >= n) return l;
+    l.site = site_of[i];
+    // a site's RNG-dependent channels are listed in channel order
+    l.k = (i >= 1 && site_of[i - 1] == l.site) ? ((i >= 2 && site_of[i - 2] == l.site) ? 2 : 1)
+                                                : 0;
+    l.gap_hi = pos[i];
+    l.gap_lo = i ? pos[i - 1] : 0u;
+    return l;
+}
+
+__device__ __forceinline__ CoefSite coef_site(const CoefList &l, bool live, int64_t su, int w,
+                                              const uint8_t *__restrict__ meta,
+                                              const double *__restrict__ cand,
+                                              const uint16_t *__restrict__ rgbi) {
+    CoefSite c{};
+    if (!live) return c;
+    const int64_t site = l.site;
+    const int64_t pixel = site < su ? site % w : site - su;
+    c.meta = meta[site];
+    c.raw = reinterpret_cast<const uint2 *>(rgbi)[pixel];
+    c.cand[0] = cand[3 * site];
+    c.cand[1] = cand[3 * site + 1];
+    c.cand[2] = cand[3 * site + 2];
+    return c;
+}
+
+// Copy intervals and jumps of every RNG-dependent channel.  A thread's
+// entries i, i + stride, ... run through a three-stage software pipeline:
+// while entry i's interval search computes, the site of entry i + 2 stride
+// and the meta, pixel and candidates of entry i + stride are in flight, so
+// the dependent gathers overlap the arithmetic instead of stalling it.
 __global__ void k_coef(AmbEntry *__restrict__ entries, const uint32_t *__restrict__ pos,
                        const uint32_t *__restrict__ n_amb_ptr, int64_t capacity,
                        const uint32_t *__restrict__ site_of, const uint8_t *__restrict__ meta,
@@ -374,23 +468,23 @@ __global__ void k_coef(AmbEntry *__restrict__ entries, const uint32_t *__restric
     const uint32_t n = (uint32_t)min((int64_t)*n_amb_ptr, capacity);
     const DitherConst dc = dither_const(p);
     const int64_t su = 6 * (int64_t)w;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint32_t site32 = site_of[i];
-        const int64_t site = site32;
-        // a site's RNG-dependent channels are listed in channel order: this
-        // entry is the k-th of its site
-        const int k = (i >= 1 && site_of[i - 1] == site32)
-                          ? ((i >= 2 && site_of[i - 2] == site32) ? 2 : 1)
-                          : 0;
-        const uint8_t mi = meta[site];
+    const uint32_t stride = gridDim.x * blockDim.x;
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    CoefList l0 = coef_list(site_of, pos, i, n);
+    CoefSite s0 = coef_site(l0, i < n, su, w, meta, cand, rgbi);
+    CoefList l1 = coef_list(site_of, pos, i + stride, n);
+    for (; i < n; i += stride) {
+        const uint32_t i1 = i + stride, i2 = i1 + stride;
+        const CoefSite s1 = coef_site(l1, i1 < n && i1 > i, su, w, meta, cand, rgbi);
+        const CoefList l2 = coef_list(site_of, pos, i2 > i1 ? i2 : n, n);
+        const uint8_t mi = s0.meta;
         int c = 0;
         for (int seen = 0; c < 3; ++c)
-            if (meta_code(mi, c) == 3 && seen++ == k) break;
-        const int64_t pixel = site < su ? site % w : site - su;
-        const uint2 raw = reinterpret_cast<const uint2 *>(rgbi)[pixel];
+            if (meta_code(mi, c) == 3 && seen++ == l0.k) break;
+        const uint2 raw = s0.raw;
         const uint32_t lane = c == 0 ? (raw.x & 0xFFFFu) : (c == 1 ? (raw.x >> 16) : (raw.y & 0xFFFFu));
         ChannelView cv;
-        cv.cand = cand[3 * site + c];
+        cv.cand = c == 0 ? s0.cand[0] : (c == 1 ? s0.cand[1] : s0.cand[2]);
         cv.cd = (double)(float)cv.cand;
         cv.dc = dc;
         cv.env = ((dc.high - cv.cd) * (cv.cd - dc.low)) * dc.coefficient;
@@ -401,7 +495,8 @@ __global__ void k_coef(AmbEntry *__restrict__ entries, const uint32_t *__restric
         // a chunk of walk channels with a two-interval entry steps with both
         // interval tests (every other chunk with one)
         if (e.l2 != 0x80u) chunk_two[i / kWalkChunk] = 1;
-        const uint64_t gap = (i == 0) ? (uint64_t)pos[0] + 1u : (uint64_t)(pos[i] - pos[i - 1]);
+        const uint64_t gap = (i == 0) ? (uint64_t)l0.gap_hi + 1u
+                                      : (uint64_t)(uint32_t)(l0.gap_hi - l0.gap_lo);
         const Affine f = lcg_power_t(gap);
         const Affine f1 = affine_compose(Affine{125u, 256u}, f);  // one more draw
         e.a0 = f.a;
@@ -409,6 +504,9 @@ __global__ void k_coef(AmbEntry *__restrict__ entries, const uint32_t *__restric
         e.a1 = (i == 0) ? f.a : f1.a;  // no previous channel before the first
         e.c1 = (i == 0) ? f.c : f1.c;
         entries[i] = e;
+        l0 = l1;
+        s0 = s1;
+        l1 = l2;
     }
 }
 
@@ -733,15 +831,16 @@ cudaError_t launch_writer(const Geometry &g, const uint8_t *meta, const double *
     // of other frames' stencil and apply blocks, which fill the SMs they
     // leave idle
     const int pr = b.priority;
-    e = launch_prio(k_seg_sums, dim3((unsigned)segs), dim3(kSegThreads), 0, stream, pr, meta,
-                    g.sites, b.seg_base, b.seg_amb, err);
+    const unsigned seg_blocks = (unsigned)((segs + kSegWarps - 1) / kSegWarps);
+    e = launch_prio(k_seg_sums, dim3(seg_blocks), dim3(kSegWarps * 32), 0, stream, pr, meta,
+                    g.sites, segs, b.seg_base, b.seg_amb, err);
     if (e != cudaSuccess) return e;
     e = launch_prio(k_seg_scan, dim3(1), dim3(1024), 0, stream, pr, b.seg_base, b.seg_amb, segs,
                     err);
     if (e != cudaSuccess) return e;
     // the site list lives in extra_after until the walk writes the counts
-    e = launch_prio(k_amb, dim3((unsigned)segs), dim3(kSegThreads), 0, stream, pr, meta, g.sites,
-                    b.seg_base, b.seg_amb, b.extra_after, b.pos, b.capacity, err);
+    e = launch_prio(k_amb, dim3(seg_blocks), dim3(kSegWarps * 32), 0, stream, pr, meta, g.sites,
+                    segs, b.seg_base, b.seg_amb, b.extra_after, b.pos, b.capacity, err);
     if (e != cudaSuccess) return e;
     const uint32_t *n_amb = b.seg_amb + segs;
     cudaMemsetAsync(b.chunk_two, 0, walk_chunks(b.capacity), stream);

@@ -33,6 +33,7 @@ caching allocator); the processing itself is the library's.
 from __future__ import annotations
 
 import ctypes
+import gc
 import time
 from collections import deque
 from dataclasses import dataclass, field
@@ -354,83 +355,93 @@ def serve(ctx: _lib.Context | None, requests: Sequence[Request], *, max_slots: i
     downloads: deque[dict] = deque()  # outputs on their way to host memory
     in_use_bytes = 0                  # planes of the requests in flight
     nxt = 0
-    start = time.perf_counter()
+    # no cyclic garbage collection while requests are timed: a full
+    # collection over a large process heap pauses the loop for tens of
+    # milliseconds, and every request in flight waits for it
+    collect = gc.isenabled()
+    gc.collect()
+    gc.disable()
+    try:
+        start = time.perf_counter()
 
-    def now() -> float:
-        return time.perf_counter() - start
+        def now() -> float:
+            return time.perf_counter() - start
 
-    def call(name: str, fn, *args):
-        """A device call of the loop, with its host time noted: the loop is
-        single-threaded, so a call that blocks delays every request."""
+        def call(name: str, fn, *args):
+            """A device call of the loop, with its host time noted: the loop is
+            single-threaded, so a call that blocks delays every request."""
 
-        t0 = time.perf_counter()
-        out = fn(*args)
-        report.note_call(name, time.perf_counter() - t0)
-        return out
+            t0 = time.perf_counter()
+            out = fn(*args)
+            report.note_call(name, time.perf_counter() - t0)
+            return out
 
-    while nxt < len(requests) or waiting or staging or inflight or downloads:
-        t = now()
-        while nxt < len(requests) and requests[nxt].arrival_s <= t:
-            waiting.append(nxt)
-            nxt += 1
-        # admission, in arrival order: a slot (reused, new or grown) and room
-        while waiting and free_host:
-            i = waiting[0]
-            h, w = (int(v) for v in requests[i].pixels.shape[:2])
-            planes = 14 * h * w
-            choice = model.choose(dev.frame_bytes(h, w))
-            fits = (choice is not None and model.allocated + model.extra(choice) + in_use_bytes
-                    + planes <= budget_bytes)
-            if not fits:
-                if staging or inflight or downloads or not model.free_sizes:
-                    break  # wait for a request in flight to finish
-                # nothing in flight: drop the idle buffers and start afresh
-                call("release_idle", dev.release_idle)
-                model.release_idle()
-                report.releases += 1
-                continue
-            waiting.popleft()
-            st = {"i": i, "h": h, "w": w, "admitted": now(), "size": model.take(choice),
-                  "planes": planes, "host": free_host.popleft()}
-            in_use_bytes += planes
-            call("upload", dev.upload, st, requests[i].pixels)
-            staging.append(st)
-        report.max_in_flight = max(report.max_in_flight,
-                                   len(staging) + len(inflight) + len(downloads))
-        report.peak_bytes = max(report.peak_bytes, model.allocated + in_use_bytes)
-        # submission: uploads that have landed go to a library slot
-        while staging and dev.landed(staging[0]):
-            ticket = call("submit", dev.submit, staging[0])
-            if ticket is None:
-                break
-            inflight[ticket] = staging.popleft()
-        # finished passes: counters, then the output's copy to host memory
-        for ticket in list(inflight):
-            if not call("poll", dev.done, ticket):
-                continue
-            st = inflight.pop(ticket)
-            st["counters"] = call("finish", dev.finish, ticket)
-            expected = requests[st["i"]].expected
-            call("download", dev.download, st, expected)
-            if expected is not None:
-                report.verified += 1
-            downloads.append(st)
-        finished = False
-        while downloads and dev.downloaded(downloads[0]):
-            st = downloads.popleft()
-            done_t = now()
-            i, h, w = st["i"], st["h"], st["w"]
-            output = dev.output(st) if keep_outputs else None
-            free_host.append(st["host"])
-            model.give_back(st["size"])
-            in_use_bytes -= st["planes"]
-            report.completions.append(Completion(i, requests[i].arrival_s, st["admitted"],
-                                                 done_t, st["counters"], output))
-            report.megapixels += h * w / 1e6
-            finished = True
-        if not finished:
-            time.sleep(0.0001)
-    report.wall_s = now()
+        while nxt < len(requests) or waiting or staging or inflight or downloads:
+            t = now()
+            while nxt < len(requests) and requests[nxt].arrival_s <= t:
+                waiting.append(nxt)
+                nxt += 1
+            # admission, in arrival order: a slot (reused, new or grown) and room
+            while waiting and free_host:
+                i = waiting[0]
+                h, w = (int(v) for v in requests[i].pixels.shape[:2])
+                planes = 14 * h * w
+                choice = model.choose(dev.frame_bytes(h, w))
+                fits = (choice is not None and model.allocated + model.extra(choice) + in_use_bytes
+                        + planes <= budget_bytes)
+                if not fits:
+                    if staging or inflight or downloads or not model.free_sizes:
+                        break  # wait for a request in flight to finish
+                    # nothing in flight: drop the idle buffers and start afresh
+                    call("release_idle", dev.release_idle)
+                    model.release_idle()
+                    report.releases += 1
+                    continue
+                waiting.popleft()
+                st = {"i": i, "h": h, "w": w, "admitted": now(), "size": model.take(choice),
+                      "planes": planes, "host": free_host.popleft()}
+                in_use_bytes += planes
+                call("upload", dev.upload, st, requests[i].pixels)
+                staging.append(st)
+            report.max_in_flight = max(report.max_in_flight,
+                                       len(staging) + len(inflight) + len(downloads))
+            report.peak_bytes = max(report.peak_bytes, model.allocated + in_use_bytes)
+            # submission: uploads that have landed go to a library slot
+            while staging and dev.landed(staging[0]):
+                ticket = call("submit", dev.submit, staging[0])
+                if ticket is None:
+                    break
+                inflight[ticket] = staging.popleft()
+            # finished passes: counters, then the output's copy to host memory
+            for ticket in list(inflight):
+                if not call("poll", dev.done, ticket):
+                    continue
+                st = inflight.pop(ticket)
+                st["counters"] = call("finish", dev.finish, ticket)
+                expected = requests[st["i"]].expected
+                call("download", dev.download, st, expected)
+                if expected is not None:
+                    report.verified += 1
+                downloads.append(st)
+            finished = False
+            while downloads and dev.downloaded(downloads[0]):
+                st = downloads.popleft()
+                done_t = now()
+                i, h, w = st["i"], st["h"], st["w"]
+                output = dev.output(st) if keep_outputs else None
+                free_host.append(st["host"])
+                model.give_back(st["size"])
+                in_use_bytes -= st["planes"]
+                report.completions.append(Completion(i, requests[i].arrival_s, st["admitted"],
+                                                     done_t, st["counters"], output))
+                report.megapixels += h * w / 1e6
+                finished = True
+            if not finished:
+                time.sleep(0.0001)
+        report.wall_s = now()
+    finally:
+        if collect:
+            gc.enable()
     report.slots_used = max_slots - model.empty
     report.mismatches = dev.mismatches()
     report.completions.sort(key=lambda c: c.index)
