@@ -3,6 +3,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <cmath>
 #include <mutex>
 #include <thread>
 #include <algorithm>
@@ -118,7 +119,6 @@ static size_t arena_layout(const Geometry &g, int64_t amb_cap, Arena *a) {
 }
 
 struct Slot {
-    int64_t cap_hint = 0;  // the longest RNG-dependent list this slot has needed
     cudaStream_t stream = nullptr;
     cudaStream_t last_stream = nullptr;  // stream of the last device-buffer pass
     cudaEvent_t done = nullptr;
@@ -160,6 +160,7 @@ struct fx_context {
     int walk_wave = 0;  // window segments per wave; 0: g_per_wave (three per SM)
     double walk_sigmas = fx::kDefaultWindowSigmas;  // walk window half-width
     int stencil_rows = 8;  // stencil tile height: 8 (four blocks per SM) or 16 (two)
+    double list_per_site = 0.0;  // longest RNG-dependent list per site a pass has needed
     int top_priority = 0;     // the device's greatest launch priority
     bool use_priority = true;  // chain and walk launched at top_priority
     int64_t list_capacity = 0;  // RNG-dependent list entries per frame; 0: sites / 2
@@ -189,23 +190,26 @@ static int64_t amb_capacity(const fx_context *ctx, const Geometry &g) {
     return ctx->list_capacity > 0 ? ctx->list_capacity : default_amb_capacity(g);
 }
 
-// The list capacity of a pass on slot s: the frame's own (amb_capacity),
-// raised to the longest list the slot has needed before, so that a slot
-// that once overflowed (heavy damage) does not overflow again on the next
-// such frame.  Never above three channels per site, the most a frame can
-// list: a small frame on a slot that held a heavy one keeps a short walk
-// launch shape.  The fx_set_list_capacity override is taken as given.
-static int64_t pass_capacity(const fx_context *ctx, const Slot &s, const Geometry &g) {
+// The list capacity of a pass: the frame's own (amb_capacity), raised to
+// the longest list per site any pass of this context has needed, so that
+// once a frame has overflowed (heavy damage) the next such frame, on any
+// slot and at any size, does not.  Never above three channels per site, the
+// most a frame can list.  The fx_set_list_capacity override is taken as
+// given.
+static int64_t pass_capacity(const fx_context *ctx, const Geometry &g) {
     const int64_t cap = amb_capacity(ctx, g);
-    if (ctx->list_capacity > 0) return cap;
+    if (ctx->list_capacity > 0 || ctx->list_per_site <= 0.0) return cap;
     const int64_t most = 3 * g.sites;
-    const int64_t hint = s.cap_hint < most ? s.cap_hint : most;
-    return hint > cap ? hint : cap;
+    int64_t learned = (int64_t)std::ceil(ctx->list_per_site * (double)g.sites) + 1;
+    if (learned > most) learned = most;
+    return learned > cap ? learned : cap;
 }
 
-// After an overflow: the slot's next passes list at least `cap` channels.
-static void note_capacity(Slot &s, int64_t cap) {
-    if (cap > s.cap_hint) s.cap_hint = cap;
+// After an overflow: later passes list at least `cap` channels per
+// `g.sites` sites.
+static void note_capacity(fx_context *ctx, const Geometry &g, int64_t cap) {
+    const double r = (double)cap / (double)g.sites;
+    if (r > ctx->list_per_site) ctx->list_per_site = r;
 }
 
 static char g_error[512];
@@ -415,7 +419,7 @@ static int ensure_slots(fx_context *ctx, int n) {
 static int run_device(fx_context *ctx, Slot &s, const Geometry &g, const fx_params &p,
                       const fx_stage *stages, uint32_t rng, const uint16_t *d_in, uint16_t *d_out,
                       uint8_t *d_changed, fx_counters *counters, bool producer_rows) {
-    int64_t cap = pass_capacity(ctx, s, g);
+    int64_t cap = pass_capacity(ctx, g);
     for (int attempt = 0; attempt < 2; ++attempt) {
         // keep caller-side device pointers stable: the arena may move only
         // when the input/outputs live in it
@@ -442,7 +446,7 @@ static int run_device(fx_context *ctx, Slot &s, const Geometry &g, const fx_para
             return FX_OK;
         }
         cap = (int64_t)counters_n_amb(hc) + 1024;
-        note_capacity(s, cap);
+        note_capacity(ctx, g, cap);
         if (!d_in) return fail(ctx, FX_ERR_INTERNAL, "amb capacity retry needs the input");
     }
     return fail(ctx, FX_ERR_INTERNAL, "amb capacity retry failed");
@@ -756,7 +760,7 @@ FX_API int fx_process(fx_context *ctx, const fx_frame *f, fx_counters *counters)
     Slot &s = slot0(ctx);
     const Geometry g = make_geometry(f->height, f->width);
     const size_t px = (size_t)g.h * g.w;
-    int64_t cap = pass_capacity(ctx, s, g);
+    int64_t cap = pass_capacity(ctx, g);
     for (int attempt = 0; attempt < 2; ++attempt) {
         rc = ensure_arena(ctx, s, g, cap);
         if (rc) return rc;
@@ -778,7 +782,7 @@ FX_API int fx_process(fx_context *ctx, const fx_frame *f, fx_counters *counters)
         if (rc) return rc;
         if (overflow) {
             cap = (int64_t)counters_n_amb(hc) + 1024;
-            note_capacity(s, cap);
+            note_capacity(ctx, g, cap);
             continue;
         }
         if (counters) counters->capacity_reruns = attempt;
@@ -819,7 +823,7 @@ FX_API int fx_process_device(fx_context *ctx, const uint16_t *d_rgbi, int32_t h,
     if (counters) {
         rc = run_device(ctx, s, g, *params, stages, rng, d_rgbi, d_out, d_changed, counters, false);
     } else {
-        rc = ensure_arena(ctx, s, g, pass_capacity(ctx, s, g));
+        rc = ensure_arena(ctx, s, g, pass_capacity(ctx, g));
         if (!rc) rc = enqueue_pass(ctx, s, g, *params, stages, rng, d_rgbi, d_out, d_changed, false);
     }
     s.last_stream = s.stream;
@@ -903,7 +907,7 @@ FX_API int fx_reserve_frames(fx_context *ctx, int32_t max_height, int32_t max_wi
     const Geometry g = make_geometry(max_height, max_width);
     for (Slot &s : ctx->slots) {
         if (s.busy) return fail(ctx, FX_ERR_INVALID_ARGUMENT, "a slot is busy: reserve first");
-        const int64_t cap = pass_capacity(ctx, s, g);
+        const int64_t cap = pass_capacity(ctx, g);
         const int rc = ensure_arena(ctx, s, g, cap);
         if (rc) return rc;
     }
@@ -924,7 +928,7 @@ FX_API int fx_reserve_slots(fx_context *ctx, int32_t count, int32_t max_height,
     for (int k = 0; k < count; ++k) {
         Slot &s = ctx->slots[k];
         if (s.busy) return fail(ctx, FX_ERR_INVALID_ARGUMENT, "a slot is busy: reserve first");
-        const int64_t cap = pass_capacity(ctx, s, g);
+        const int64_t cap = pass_capacity(ctx, g);
         rc = ensure_arena(ctx, s, g, cap);
         if (rc) return rc;
     }
@@ -989,7 +993,7 @@ static Slot *free_slot(fx_context *ctx, const Geometry &g) {
             if (!empty) empty = &s;
             continue;
         }
-        const size_t need = arena_layout(g, pass_capacity(ctx, s, g), nullptr);
+        const size_t need = arena_layout(g, pass_capacity(ctx, g), nullptr);
         if (s.arena.bytes >= need && (!fit || s.arena.bytes < fit->arena.bytes)) fit = &s;
         if (!largest || s.arena.bytes > largest->arena.bytes) largest = &s;
     }
@@ -1009,7 +1013,7 @@ FX_API int fx_submit(fx_context *ctx, const fx_frame *f, int64_t *ticket) {
     if (!slot) return fail(ctx, FX_PENDING, "no free slot");
     Slot &s = *slot;
     const size_t px = (size_t)g.h * g.w;
-    rc = ensure_arena(ctx, s, g, pass_capacity(ctx, s, g));
+    rc = ensure_arena(ctx, s, g, pass_capacity(ctx, g));
     if (rc) return rc;
     const size_t in_bytes = px * 8;
     const size_t out_bytes = px * 6 + px * 4 + px;
@@ -1084,7 +1088,7 @@ FX_API int fx_submit_device(fx_context *ctx, const uint16_t *d_rgbi, int32_t h, 
     Slot *slot = free_slot(ctx, g);
     if (!slot) return fail(ctx, FX_PENDING, "no free slot");
     Slot &s = *slot;
-    rc = ensure_arena(ctx, s, g, pass_capacity(ctx, s, g));
+    rc = ensure_arena(ctx, s, g, pass_capacity(ctx, g));
     if (rc) return rc;
     s.frame = fx_frame{};
     s.frame.height = h;
@@ -1153,7 +1157,7 @@ struct FetchTargets {
 static int rerun_with_capacity(fx_context *ctx, Slot &s, fx_counters *counters) {
     char *hc = reinterpret_cast<char *>(s.h_ctr);
     const int64_t cap = (int64_t)counters_n_amb(hc) + 1024;
-    note_capacity(s, cap);
+    note_capacity(ctx, s.g, cap);
     int rc = ensure_arena(ctx, s, s.g, cap);
     if (rc) return rc;
     if (s.device) {
@@ -1317,6 +1321,15 @@ FX_API int64_t fx_frame_bytes(int32_t h, int32_t w) {
     if (h < 1 || w < 1) return -1;
     const Geometry g = make_geometry(h, w);
     return (int64_t)arena_layout(g, default_amb_capacity(g), nullptr);
+}
+
+FX_API int fx_pass_bytes(fx_context *ctx, int32_t h, int32_t w, int64_t *bytes) {
+    if (!ctx || !bytes || h < 1 || w < 1) return FX_ERR_INVALID_ARGUMENT;
+    if ((int64_t)h * w > (int64_t)1 << 30) return FX_ERR_INVALID_ARGUMENT;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    const Geometry g = make_geometry(h, w);
+    *bytes = (int64_t)arena_layout(g, pass_capacity(ctx, g), nullptr);
+    return FX_OK;
 }
 
 }  // extern "C"

@@ -161,32 +161,72 @@ __global__ void __launch_bounds__(kSegWarps * 32)
 }
 
 // Exclusive scan of the per-segment sums; entry [n] holds the totals.  One
-// block: each thread sums a contiguous run of segments, one block scan
-// gives the runs' offsets, and each thread writes its run's prefixes.
-__global__ void k_seg_scan(uint32_t *__restrict__ seg_base, uint32_t *__restrict__ seg_amb,
-                           int64_t n, const uint32_t *__restrict__ err) {
-    __shared__ uint32_t ws[32];
+// block of 1024 threads, over tiles of 4096 segments: a tile is loaded
+// coalesced into shared memory, each thread scans four neighbouring
+// segments, and one block scan of (fixed << 32 | RNG-dependent) pairs gives
+// the threads' offsets (the RNG-dependent total stays below 2^32: at most
+// three per site).
+__global__ void __launch_bounds__(1024)
+    k_seg_scan(uint32_t *__restrict__ seg_base, uint32_t *__restrict__ seg_amb, int64_t n,
+               const uint32_t *__restrict__ err) {
+    constexpr int kPerThread = 4, kTile = 1024 * kPerThread;
+    __shared__ uint32_t tb[kTile], ta[kTile];
+    __shared__ unsigned long long ws[32];
     if (pass_stopped(err)) return;
-    const int64_t per = (n + 1023) / 1024;
-    const int64_t lo = min(n, per * (int64_t)threadIdx.x), hi = min(n, lo + per);
-    uint32_t sb = 0, sa = 0;
-    for (int64_t i = lo; i < hi; ++i) {
-        sb += seg_base[i];
-        sa += seg_amb[i];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    unsigned long long carry = 0;
+    for (int64_t t0 = 0; t0 < n; t0 += kTile) {
+        for (int j = tid; j < kTile; j += 1024) {
+            const int64_t i = t0 + j;
+            tb[j] = i < n ? seg_base[i] : 0u;
+            ta[j] = i < n ? seg_amb[i] : 0u;
+        }
+        __syncthreads();
+        unsigned long long mine = 0;
+#pragma unroll
+        for (int k = 0; k < kPerThread; ++k)
+            mine += ((unsigned long long)tb[kPerThread * tid + k] << 32) | ta[kPerThread * tid + k];
+        unsigned long long x = mine;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned long long y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) ws[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            unsigned long long v = ws[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned long long y = __shfl_up_sync(0xFFFFFFFFu, v, o);
+                if (lane >= o) v += y;
+            }
+            ws[lane] = v;
+        }
+        __syncthreads();
+        unsigned long long run = carry + (warp ? ws[warp - 1] : 0ull) + x - mine;
+#pragma unroll
+        for (int k = 0; k < kPerThread; ++k) {
+            const int j = kPerThread * tid + k;
+            const unsigned long long v = ((unsigned long long)tb[j] << 32) | ta[j];
+            tb[j] = (uint32_t)(run >> 32);
+            ta[j] = (uint32_t)run;
+            run += v;
+        }
+        carry += ws[31];
+        __syncthreads();
+        for (int j = tid; j < kTile; j += 1024) {
+            const int64_t i = t0 + j;
+            if (i < n) {
+                seg_base[i] = tb[j];
+                seg_amb[i] = ta[j];
+            }
+        }
+        __syncthreads();
     }
-    uint32_t tb, ta;
-    uint32_t eb = block_exclusive_scan<1024>(sb, tb, ws);
-    uint32_t ea = block_exclusive_scan<1024>(sa, ta, ws);
-    for (int64_t i = lo; i < hi; ++i) {
-        const uint32_t vb = seg_base[i], va = seg_amb[i];
-        seg_base[i] = eb;
-        seg_amb[i] = ea;
-        eb += vb;
-        ea += va;
-    }
-    if (threadIdx.x == 0) {
-        seg_base[n] = tb;
-        seg_amb[n] = ta;
+    if (tid == 0) {
+        seg_base[n] = (uint32_t)(carry >> 32);
+        seg_amb[n] = (uint32_t)carry;
     }
 }
 
@@ -239,6 +279,9 @@ struct ChannelView {
     float span;
     DitherConst dc;
     __device__ double raw(uint32_t s1) const { return dither_raw_delta(cd, env, span, s1); }
+    __device__ bool low_ok(uint32_t s1) const { return dc.low < cd + raw(s1); }
+    __device__ bool high_ok(uint32_t s1) const { return cd + raw(s1) < dc.high; }
+    __device__ bool floor_test(uint32_t s1) const { return cand + raw(s1) <= od; }
     __device__ bool copies(uint32_t s1) const {
         const double d = raw(s1);
         const double changed = cd + d;
@@ -247,117 +290,70 @@ struct ChannelView {
     }
 };
 
-// The search for the first state where a monotone predicate differs from
-// its value at 0 (2^24 when it never does).  It starts from an estimate of
-// that state, gallops from it to a bracket checked on the exact predicate
-// and bisects inside, so the estimate changes only the cost, never the
-// result.  The search is a small state machine: prepare() names the next
-// state to test (false when done), apply() takes the predicate's value
-// there.  copy_intervals runs its three searches in lockstep, so the three
-// predicate evaluations of a step are independent and overlap.
-struct SwitchSearch {
-    uint32_t lo, hi, step, q;
-    int phase;  // 0 probe the estimate, 1 gallop up, 2 gallop down, 3 bisect, 4 done
-    bool p0;
-
-    // p0 = pred(0), pm = pred(2^24 - 1); invariant: pred(lo) == p0, pred(hi) != p0
-    __device__ void start(bool at0, bool at_max, double guess) {
-        p0 = at0;
-        lo = 0u;
-        hi = kLcgMask;
-        step = 1u;
-        if (at_max == at0) {
-            hi = kLcgMask + 1u;
-            phase = 4;
-            return;
-        }
-        q = kLcgMask / 2u;
-        if (guess == guess) {  // not NaN
-            const double top = (double)(kLcgMask - 1u);
-            q = (uint32_t)(guess < 1.0 ? 1.0 : (guess > top ? top : guess));
-        }
-        phase = 0;
+// First state where a monotone predicate differs from its value at 0
+// (2^24 when it never does).  `guess` estimates that state; the search
+// gallops from it to a bracket checked on the exact predicate and bisects
+// inside, so the estimate changes only the cost, never the result.
+template <class F>
+__device__ __forceinline__ uint32_t switch_point(F pred, double guess) {
+    const bool p0 = pred(0u);
+    if (pred(kLcgMask) == p0) return kLcgMask + 1u;
+    // invariant: pred(lo) == p0, pred(hi) != p0, lo < hi
+    uint32_t lo = 0u, hi = kLcgMask;
+    uint32_t x = kLcgMask / 2u;
+    if (guess == guess) {  // not NaN
+        const double top = (double)(kLcgMask - 1u);
+        x = (uint32_t)(guess < 1.0 ? 1.0 : (guess > top ? top : guess));
     }
-    __device__ bool prepare() {
-        for (;;) {
-            switch (phase) {
-            case 0:
-                return true;
-            case 1:
-            case 2:
-                if (hi - lo <= 1u || hi - lo <= step) {
-                    phase = 3;
-                    continue;
-                }
-                q = phase == 1 ? lo + step : hi - step;
-                return true;
-            case 3:
-                if (hi - lo <= 1u) {
-                    phase = 4;
-                    return false;
-                }
-                q = lo + ((hi - lo) >> 1);
-                return true;
-            default:
-                return false;
+    uint32_t step = 1u;
+    if (pred(x) == p0) {
+        lo = x;
+        while (hi - lo > 1u) {
+            if (hi - lo <= step) break;
+            const uint32_t y = lo + step;
+            if (pred(y) == p0) {
+                lo = y;
+                step <<= 1;
+            } else {
+                hi = y;
+                break;
+            }
+        }
+    } else {
+        hi = x;
+        while (hi - lo > 1u) {
+            if (hi - lo <= step) break;
+            const uint32_t y = hi - step;
+            if (pred(y) != p0) {
+                hi = y;
+                step <<= 1;
+            } else {
+                lo = y;
+                break;
             }
         }
     }
-    __device__ void apply(bool v) {
-        switch (phase) {
-        case 0:
-            if (v == p0) { lo = q; phase = 1; } else { hi = q; phase = 2; }
-            break;
-        case 1:
-            if (v == p0) { lo = q; step <<= 1; } else { hi = q; phase = 3; }
-            break;
-        case 2:
-            if (v != p0) { hi = q; step <<= 1; } else { lo = q; phase = 3; }
-            break;
-        default:
-            if (v == p0) lo = q; else hi = q;
-            break;
-        }
+    while (hi - lo > 1u) {
+        const uint32_t mid = lo + ((hi - lo) >> 1);
+        if (pred(mid) == p0) lo = mid;
+        else hi = mid;
     }
-};
+    return hi;
+}
 
 // The state s1 at which base + raw(s1) would reach `target` if the delta
-// were computed exactly (it is affine in s1): a starting point for the
-// search.
+// were computed exactly (it is affine in s1): a starting point for
+// switch_point.
 __device__ __forceinline__ double crossing(const ChannelView &cv, double base, double target) {
     const double scale = cv.env * (double)cv.span;
     return ((target - base) / scale + 0.5) / kNormalization - 1.0;
 }
 
-// The three predicates that bound the copy intervals, on one raw delta d:
-// 0 the lower accept bound, 1 the upper accept bound, 2 the floor test.
-__device__ __forceinline__ bool interval_pred(const ChannelView &cv, int k, double d) {
-    return k == 0 ? cv.dc.low < cv.cd + d : (k == 1 ? cv.cd + d < cv.dc.high : cv.cand + d <= cv.od);
-}
-
 __device__ void copy_intervals(const ChannelView &cv, AmbEntry &e, uint32_t *err) {
-    SwitchSearch sr[3];
-    {
-        const double d0 = cv.raw(0u), dm = cv.raw(kLcgMask);
-        const double guess[3] = {crossing(cv, cv.cd, cv.dc.low), crossing(cv, cv.cd, cv.dc.high),
-                                 crossing(cv, cv.cand, cv.od)};
-#pragma unroll
-        for (int k = 0; k < 3; ++k)
-            sr[k].start(interval_pred(cv, k, d0), interval_pred(cv, k, dm), guess[k]);
-    }
-    for (;;) {
-        bool act[3];
-#pragma unroll
-        for (int k = 0; k < 3; ++k) act[k] = sr[k].prepare();
-        if (!act[0] && !act[1] && !act[2]) break;
-        double d[3];
-#pragma unroll
-        for (int k = 0; k < 3; ++k) d[k] = cv.raw(act[k] ? sr[k].q : 0u);
-#pragma unroll
-        for (int k = 0; k < 3; ++k)
-            if (act[k]) sr[k].apply(interval_pred(cv, k, d[k]));
-    }
-    uint32_t b[3] = {sr[0].hi, sr[1].hi, sr[2].hi};
+    uint32_t b[3] = {
+        switch_point([&](uint32_t s) { return cv.low_ok(s); }, crossing(cv, cv.cd, cv.dc.low)),
+        switch_point([&](uint32_t s) { return cv.high_ok(s); }, crossing(cv, cv.cd, cv.dc.high)),
+        switch_point([&](uint32_t s) { return cv.floor_test(s); }, crossing(cv, cv.cand, cv.od))};
     // sort the three breakpoints
     if (b[0] > b[1]) { const uint32_t t = b[0]; b[0] = b[1]; b[1] = t; }
     if (b[1] > b[2]) { const uint32_t t = b[1]; b[1] = b[2]; b[2] = t; }

@@ -164,6 +164,8 @@ SIGNATURES = {
     "fx_mem_info": ([_P, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)],
                     ctypes.c_int),
     "fx_frame_bytes": ([ctypes.c_int32, ctypes.c_int32], ctypes.c_int64),
+    "fx_pass_bytes": ([_P, ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_int64)],
+                      ctypes.c_int),
     "fx_profile_enable": ([_P, ctypes.c_int], ctypes.c_int),
     "fx_profile_read": ([_P, _P, ctypes.POINTER(ctypes.c_int64), ctypes.c_int], ctypes.c_int),
     # at-floor routing census primitives

@@ -7,9 +7,10 @@ while others run are processed alongside them, each in its own library slot
 (its own stream and device buffers):
 
 * admission is by device memory: a request needs its pass buffers
-  (``fx_frame_bytes(h, w)``, the same estimate the reference's CUDA backend
-  checks against free memory, cuda_backend/engine.py:168-224) plus its input
-  and output planes.  A slot whose buffers already hold the frame is reused
+  (``fx_pass_bytes(h, w)``: ``fx_frame_bytes``, the same estimate the
+  reference's CUDA backend checks against free memory,
+  cuda_backend/engine.py:168-224, with the RNG-dependent list grown by any
+  overflow the context has seen) plus its input and output planes.  A slot whose buffers already hold the frame is reused
   (no new memory); otherwise a slot without buffers takes it, or the idle
   slot with the largest buffers grows, if the bytes fit the budget (the
   free HBM reported by ``fx_mem_info`` at the start, less a reserve).  When
@@ -86,10 +87,13 @@ class ServeReport:
     verified: int = 0          # outputs compared with their single-frame output
     mismatches: int = 0        # differing uint16 values over all verified outputs
     slowest_call_s: dict = field(default_factory=dict)  # device call -> longest host time
+    stalls: list = field(default_factory=list)  # (at_s, call, ms, in flight) of calls > 20 ms
 
-    def note_call(self, name: str, seconds: float) -> None:
+    def note_call(self, name: str, seconds: float, at_s: float = 0.0, in_flight: int = 0) -> None:
         if seconds > self.slowest_call_s.get(name, 0.0):
             self.slowest_call_s[name] = seconds
+        if seconds > 0.020:
+            self.stalls.append((round(at_s, 3), name, round(seconds * 1e3, 1), in_flight))
 
     def percentile_ms(self, q: float, attr: str = "latency_s") -> float:
         lat = np.array([getattr(c, attr) for c in self.completions]) * 1e3
@@ -111,7 +115,9 @@ class ServeReport:
                "capacity_reruns": int(sum(getattr(c.counters, "capacity_reruns", 0)
                                           for c in self.completions)),
                "slowest_call_ms": {k: round(v * 1e3, 2)
-                                   for k, v in sorted(self.slowest_call_s.items())}}
+                                   for k, v in sorted(self.slowest_call_s.items())},
+               "calls_over_20ms": len(self.stalls),
+               "longest_stalls": sorted(self.stalls, key=lambda x: -x[2])[:5]}
         if self.verified:
             out["verified"] = self.verified
             out["bit_exact"] = self.mismatches == 0 and self.verified == len(self.completions)
@@ -211,7 +217,13 @@ class TorchDevice:
         torch.cuda.synchronize()
 
     def frame_bytes(self, h: int, w: int) -> int:
-        return frame_bytes(h, w)
+        """Pass buffers of an h x w frame on this context (fx_pass_bytes:
+        the list grown by any overflow the context has seen)."""
+
+        out = ctypes.c_int64()
+        with self.ctx.lock:
+            self.ctx.check(self.lib.fx_pass_bytes(self.ctx.handle, h, w, ctypes.byref(out)))
+        return int(out.value)
 
     def free_bytes(self) -> int:
         free, total = ctypes.c_size_t(), ctypes.c_size_t()
@@ -373,7 +385,8 @@ def serve(ctx: _lib.Context | None, requests: Sequence[Request], *, max_slots: i
 
             t0 = time.perf_counter()
             out = fn(*args)
-            report.note_call(name, time.perf_counter() - t0)
+            report.note_call(name, time.perf_counter() - t0, t0 - start,
+                             len(staging) + len(inflight) + len(downloads))
             return out
 
         while nxt < len(requests) or waiting or staging or inflight or downloads:

@@ -101,8 +101,9 @@ typedef struct fx_counters {
     int64_t walk_packed_segments; /* segments whose settled phase ran two
                                      candidates per lane (walk diagnostics) */
     int64_t capacity_reruns;      /* 1 when the pass ran a second time because
-                                     its RNG-dependent list overflowed (the
-                                     slot then keeps the larger list) */
+                                     its RNG-dependent list overflowed (later
+                                     passes of the context list that many
+                                     channels per site) */
 } fx_counters;
 
 /* One frame for fx_process / fx_submit.  Host pointers. */
@@ -315,8 +316,13 @@ FX_API int fx_profile_read(fx_context *ctx, double *ms, int64_t *passes, int res
 /* Free / total device memory, for admission control. */
 FX_API int fx_mem_info(fx_context *ctx, size_t *free_bytes, size_t *total_bytes);
 
-/* Device bytes one frame of the given size needs (admission estimate). */
+/* Device bytes one frame of the given size needs (admission estimate), with
+ * the default RNG-dependent list of half the sites. */
 FX_API int64_t fx_frame_bytes(int32_t height, int32_t width);
+/* The same on this context: after a frame's list overflowed (heavy damage),
+ * later passes list up to the longest list per site seen so far, and their
+ * buffers grow by that much (no reference counterpart). */
+FX_API int fx_pass_bytes(fx_context *ctx, int32_t height, int32_t width, int64_t *bytes);
 
 /* ------------------------------------------------------------------------
  * At-floor routing census (hybrid routing.py:447-682, route_at_floor_mask).

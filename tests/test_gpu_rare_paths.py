@@ -170,12 +170,13 @@ def test_list_overflow_reruns_fx_process_device(golden):
     assert ctr.final_state == expected["final_rng_state"]
 
 
-def test_a_slot_that_overflowed_keeps_the_longer_list(golden):
+def test_a_context_that_overflowed_keeps_the_longer_list(golden):
     """Heavy damage lists more RNG-dependent channels than the default list
     holds (half the sites).  On a fresh context the first pass reruns with a
-    longer list and the slot keeps it, so the next heavy frame on that slot
-    runs once; through fx_process and through fx_submit_device, each on its
-    own fresh context.  Every result equals the reference's."""
+    longer list and the context keeps that length per site, so the next heavy
+    frame runs once (and fx_pass_bytes grows by the longer list); through
+    fx_process and through fx_submit_device, each on its own fresh context.
+    Every result equals the reference's."""
 
     import torch
 
@@ -186,10 +187,16 @@ def test_a_slot_that_overflowed_keeps_the_longer_list(golden):
     px = _frame("heavy_full_0")
     h, w = px.shape[:2]
     expected = golden["jobs"]["heavy_full_0"]
+    lib = _lib.load()
     fresh = _lib.Context(0, lut=response_lut(), high=high, low=low)
     try:
+        before, after = ctypes.c_int64(), ctypes.c_int64()
+        assert lib.fx_pass_bytes(fresh.handle, h, w, ctypes.byref(before)) == 0
+        assert before.value == lib.fx_frame_bytes(h, w)
         first = engine.run_frame(fresh, px, params, None, NIKON_PE_INITIAL_STATE, True)
         second = engine.run_frame(fresh, px, params, None, NIKON_PE_INITIAL_STATE, True)
+        assert lib.fx_pass_bytes(fresh.handle, h, w, ctypes.byref(after)) == 0
+        assert after.value > before.value
     finally:
         fresh.close()
     assert first.counters.rng_dependent > (6 * w + h * w) // 2

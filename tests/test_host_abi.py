@@ -58,6 +58,7 @@ def test_request_entry_points_reject_bad_arguments():
 
     lib = _lib.load()
     assert lib.fx_cancel(None, 1) == 1
+    assert lib.fx_pass_bytes(None, 16, 16, ctypes.byref(ctypes.c_int64())) == 1
     assert lib.fx_fetch(None, 1, 0, None, None, None, None, None) == 1
     assert lib.fx_set_walk_window(None, 4.5) == 1
     assert lib.fx_set_list_capacity(None, 0) == 1
