@@ -40,6 +40,7 @@ struct DevCounters {
     unsigned long long walk_stats[3];  // candidate steps, window sum, survivor sum
     uint32_t su_base[6], su_amb[6];    // per startup row, for the last block's prefix
     uint32_t su_done;                  // startup rows summed
+    unsigned long long apply_next;     // k_apply's next segment
 };
 
 // ---------------------------------------------------------------------------
@@ -230,17 +231,17 @@ __global__ void __launch_bounds__(1024)
     }
 }
 
-// Per-site exclusive chain offsets inside a segment block.
+// Per-site exclusive chain offsets inside segment `seg`, one block.
 __device__ __forceinline__ void site_offsets(const uint8_t m[kPer], const uint32_t *seg_base,
-                                             const uint32_t *seg_amb, uint32_t *warp_sums,
-                                             uint32_t &P, uint32_t &A) {
+                                             const uint32_t *seg_amb, int64_t seg,
+                                             uint32_t *warp_sums, uint32_t &P, uint32_t &A) {
     uint32_t packed = 0;
 #pragma unroll
     for (int i = 0; i < kPer; ++i) packed += ((uint32_t)meta_base(m[i]) << 16) | meta_amb(m[i]);
     uint32_t total;
     const uint32_t ex = block_exclusive_scan<kSegThreads>(packed, total, warp_sums);
-    P = seg_base[blockIdx.x] + (ex >> 16);
-    A = seg_amb[blockIdx.x] + (ex & 0xFFFFu);
+    P = seg_base[seg] + (ex >> 16);
+    A = seg_amb[seg] + (ex & 0xFFFFu);
 }
 
 struct SiteInfo {
@@ -647,8 +648,15 @@ cudaError_t writer_identity_table(const float *lut, const uint32_t *hi, const ui
 // below 2^36 draws is six table lookups and compositions.
 constexpr int kJumpDigits = 6;
 __device__ Affine g_jump[kJumpDigits][64];
+constexpr int kApplyBlocksPerSM = 5;  // k_apply's resident blocks per SM
+static int g_apply_blocks = kApplyBlocksPerSM * 148;
 
 cudaError_t writer_init() {
+    int device = 0, sms = 0;
+    if (cudaGetDevice(&device) == cudaSuccess &&
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) == cudaSuccess &&
+        sms > 0)
+        g_apply_blocks = kApplyBlocksPerSM * sms;
     Affine tab[kJumpDigits][64];
     Affine step{125u, 256u};  // g^(64^j)
     for (int j = 0; j < kJumpDigits; ++j) {
@@ -670,12 +678,15 @@ __device__ __forceinline__ uint32_t jump_by_table(const Affine (*tab)[64], uint3
     return ((r.a * (s << 8) + r.c) >> 8) & kLcgMask;
 }
 
-// Public sites: exact draws and values, emit, counters.  Phase 1 emits every
-// site that was not attempted (its output is the identity emit) and lists
-// the attempted ones in shared memory; phase 2 processes that list densely,
-// each entry from its own start state g^(fixed + extra before it)(s0), and
-// checks the draws it makes against the classification and the walk.
-__global__ void __launch_bounds__(kSegThreads, 5)
+// Public sites: exact draws and values, emit, counters.  A block takes
+// 1024-site segments by ticket until none is left (one resident wave of
+// blocks; the LCG jump and emit tables are loaded once per block).  Phase 1
+// emits every site that was not attempted (its output is the identity emit)
+// and lists the attempted ones in shared memory; phase 2 processes that list
+// densely, each entry from its own start state g^(fixed + extra before
+// it)(s0), and checks the draws it makes against the classification and the
+// walk.
+__global__ void __launch_bounds__(kSegThreads, kApplyBlocksPerSM)
     k_apply(const uint8_t *__restrict__ meta, const double *__restrict__ cand, int64_t sites,
             int w, const uint16_t *__restrict__ rgbi, const float *__restrict__ lut,
             const uint32_t *__restrict__ g_high, const uint32_t *__restrict__ g_low,
@@ -689,6 +700,7 @@ __global__ void __launch_bounds__(kSegThreads, 5)
     __shared__ unsigned long long s_sums[kSegThreads / 32][4];
     __shared__ Affine s_jump[kJumpDigits][64];
     __shared__ uint32_t s_ref[kSegment], s_p[kSegment], s_a[kSegment];
+    __shared__ unsigned long long s_seg;
     if (pass_stopped(err)) return;  // cancelled: the output stays untouched
     for (int i = threadIdx.x; i < 256; i += kSegThreads) {
         hi[i] = g_high[i];
@@ -697,120 +709,129 @@ __global__ void __launch_bounds__(kSegThreads, 5)
     for (int i = threadIdx.x; i < kJumpDigits * 64; i += kSegThreads)
         s_jump[i / 64][i % 64] = g_jump[i / 64][i % 64];
     const int64_t su = 6 * (int64_t)w;
-    const int64_t seg0 = (int64_t)blockIdx.x * kSegment;
-    const int64_t first = seg0 + threadIdx.x * kPer;
-    uint8_t m[kPer];
-    load_meta(meta, first, sites, m);
-    uint32_t P, A;
-    site_offsets(m, seg_base, seg_amb, ws, P, A);  // contains __syncthreads
-
-    // ---- phase 1: identity emits; list the attempted sites ---------------
-    uint32_t mine = 0, pp[kPer], aa[kPer];
-    bool listed_here[kPer];
-    bool ok = true;
-#pragma unroll
-    for (int i = 0; i < kPer; ++i) {
-        const int64_t site = first + i;
-        const uint8_t mi = m[i];
-        listed_here[i] = false;
-        pp[i] = P;
-        aa[i] = A;
-        if (site >= su && site < sites) {
-            if (mi & 0x80u) {
-                listed_here[i] = true;
-                ++mine;
-            } else {
-                const int64_t pixel = site - su;
-                const uint2 raw = reinterpret_cast<const uint2 *>(rgbi)[pixel];
-                uint16_t *o = rgb_out + 3 * pixel;
-                o[0] = __ldg(ident + (raw.x & 0xFFFFu));
-                o[1] = __ldg(ident + (raw.x >> 16));
-                o[2] = __ldg(ident + (raw.y & 0xFFFFu));
-                if (changed_out) changed_out[pixel] = 0;
-            }
-        }
-        P += meta_base(mi);
-        A += meta_amb(mi);
-    }
-    uint32_t listed;
-    const uint32_t at = block_exclusive_scan<kSegThreads>(mine, listed, ws);
-    {
-        uint32_t slot = at;
-#pragma unroll
-        for (int i = 0; i < kPer; ++i) {
-            if (listed_here[i]) {
-                s_ref[slot] = ((uint32_t)m[i] << 16) | (uint32_t)(threadIdx.x * kPer + i);
-                s_p[slot] = pp[i];
-                s_a[slot] = aa[i];
-                ++slot;
-            }
-        }
-    }
-    __syncthreads();
-
-    // ---- phase 2: attempted sites, densely ----------------------------------
+    const int64_t segs = (sites + kSegment - 1) / kSegment;
     const DitherConst dc = dither_const(p);
     unsigned long long att = 0, written = 0, changed = 0, draws_total = 0;
-    for (uint32_t k = threadIdx.x; k < listed; k += kSegThreads) {
-        const uint32_t r = s_ref[k];
-        const uint8_t mi = (uint8_t)(r >> 16);
-        const int64_t site = seg0 + (r & 0xFFFFu);
-        const uint32_t pixel = (uint32_t)(site - su);  // H*W < 2^31
-        const uint32_t y = pixel / (uint32_t)w;
-        const uint2 raw = reinterpret_cast<const uint2 *>(rgbi)[pixel];
-        const float orig[3] = {__ldg(lut + (raw.x & 0xFFFFu)), __ldg(lut + (raw.x >> 16)),
-                               __ldg(lut + (raw.y & 0xFFFFu))};
-        const bool floor_enabled = p.driver_gate_primary || stages[y + 6].gate_secondary;
-        float values[3] = {orig[0], orig[1], orig[2]};
-        const uint32_t Ak = s_a[k];
-        const int amb = meta_amb(mi);
-        const uint32_t e_before = extra_before(extra_after, Ak, capacity);
-        const uint32_t extra = extra_before(extra_after, Ak + amb, capacity) - e_before;
-        uint32_t state = jump_by_table(s_jump, s0, (uint64_t)s_p[k] + e_before);
-        const double *cd = cand + 3 * site;
-        const double c3[3] = {cd[0], cd[1], cd[2]};
-        bool valid = true;
+    bool ok = true;
+    // segments by ticket: the tables above are loaded once per block
+    for (;;) {
+        __syncthreads();  // the previous segment's list and ticket are consumed
+        if (threadIdx.x == 0) s_seg = atomicAdd(&ctr->apply_next, 1ull);
+        __syncthreads();
+        const int64_t seg = (int64_t)s_seg;
+        if (seg >= segs) break;
+        const int64_t seg0 = seg * kSegment;
+        const int64_t first = seg0 + threadIdx.x * kPer;
+        uint8_t m[kPer];
+        load_meta(meta, first, sites, m);
+        uint32_t P, A;
+        site_offsets(m, seg_base, seg_amb, seg, ws, P, A);  // contains __syncthreads
+
+        // ---- phase 1: identity emits; list the attempted sites ---------------
+        uint32_t mine = 0, pp[kPer], aa[kPer];
+        bool listed_here[kPer];
 #pragma unroll
-        for (int c = 0; c < 3; ++c) valid &= isfinite(c3[c]) && c3[c] > 0.0;
-        uint32_t draws = 0;
-        if (valid) {
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                int drew;
-                const double firstd = dither_delta(c3[c], p.dither_scales[c], dc, state, drew);
-                draws += drew;
-                if (floor_enabled && c3[c] + firstd <= (double)orig[c]) {
-                    values[c] = orig[c];
+        for (int i = 0; i < kPer; ++i) {
+            const int64_t site = first + i;
+            const uint8_t mi = m[i];
+            listed_here[i] = false;
+            pp[i] = P;
+            aa[i] = A;
+            if (site >= su && site < sites) {
+                if (mi & 0x80u) {
+                    listed_here[i] = true;
+                    ++mine;
                 } else {
-                    double d = firstd;
-                    if (floor_enabled) {
-                        d = dither_delta(c3[c], p.dither_scales[c], dc, state, drew);
-                        draws += drew;
-                    }
-                    values[c] = (float)(c3[c] + d);
+                    const int64_t pixel = site - su;
+                    const uint2 raw = reinterpret_cast<const uint2 *>(rgbi)[pixel];
+                    uint16_t *o = rgb_out + 3 * pixel;
+                    o[0] = __ldg(ident + (raw.x & 0xFFFFu));
+                    o[1] = __ldg(ident + (raw.x >> 16));
+                    o[2] = __ldg(ident + (raw.y & 0xFFFFu));
+                    if (changed_out) changed_out[pixel] = 0;
+                }
+            }
+            P += meta_base(mi);
+            A += meta_amb(mi);
+        }
+        uint32_t listed;
+        const uint32_t at = block_exclusive_scan<kSegThreads>(mine, listed, ws);
+        {
+            uint32_t slot = at;
+#pragma unroll
+            for (int i = 0; i < kPer; ++i) {
+                if (listed_here[i]) {
+                    s_ref[slot] = ((uint32_t)m[i] << 16) | (uint32_t)(threadIdx.x * kPer + i);
+                    s_p[slot] = pp[i];
+                    s_a[slot] = aa[i];
+                    ++slot;
                 }
             }
         }
-        if ((int64_t)(Ak + amb) <= capacity && draws != (uint32_t)meta_base(mi) + extra)
-            raise_error(err, FX_ERR_INTERNAL);
-        att += 1;
-        draws_total += draws;
-        written += (values[0] != orig[0] || values[1] != orig[1] || values[2] != orig[2]);
-        const uint16_t e0[3] = {__ldg(ident + (raw.x & 0xFFFFu)), __ldg(ident + (raw.x >> 16)),
-                                __ldg(ident + (raw.y & 0xFFFFu))};
-        uint16_t e[3];
+        __syncthreads();
+
+        // ---- phase 2: attempted sites, densely ----------------------------------
+        for (uint32_t k = threadIdx.x; k < listed; k += kSegThreads) {
+            const uint32_t r = s_ref[k];
+            const uint8_t mi = (uint8_t)(r >> 16);
+            const int64_t site = seg0 + (r & 0xFFFFu);
+            const uint32_t pixel = (uint32_t)(site - su);  // H*W < 2^31
+            const uint32_t y = pixel / (uint32_t)w;
+            const uint2 raw = reinterpret_cast<const uint2 *>(rgbi)[pixel];
+            const float orig[3] = {__ldg(lut + (raw.x & 0xFFFFu)), __ldg(lut + (raw.x >> 16)),
+                                   __ldg(lut + (raw.y & 0xFFFFu))};
+            const bool floor_enabled = p.driver_gate_primary || stages[y + 6].gate_secondary;
+            float values[3] = {orig[0], orig[1], orig[2]};
+            const uint32_t Ak = s_a[k];
+            const int amb = meta_amb(mi);
+            const uint32_t e_before = extra_before(extra_after, Ak, capacity);
+            const uint32_t extra = extra_before(extra_after, Ak + amb, capacity) - e_before;
+            uint32_t state = jump_by_table(s_jump, s0, (uint64_t)s_p[k] + e_before);
+            const double *cd = cand + 3 * site;
+            const double c3[3] = {cd[0], cd[1], cd[2]};
+            bool valid = true;
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            e[c] = e0[c];
-            if (!(values[c] == orig[c])) ok &= emit_one(values[c], hi, lo, e[c]);
+            for (int c = 0; c < 3; ++c) valid &= isfinite(c3[c]) && c3[c] > 0.0;
+            uint32_t draws = 0;
+            if (valid) {
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    int drew;
+                    const double firstd = dither_delta(c3[c], p.dither_scales[c], dc, state, drew);
+                    draws += drew;
+                    if (floor_enabled && c3[c] + firstd <= (double)orig[c]) {
+                        values[c] = orig[c];
+                    } else {
+                        double d = firstd;
+                        if (floor_enabled) {
+                            d = dither_delta(c3[c], p.dither_scales[c], dc, state, drew);
+                            draws += drew;
+                        }
+                        values[c] = (float)(c3[c] + d);
+                    }
+                }
+            }
+            if ((int64_t)(Ak + amb) <= capacity && draws != (uint32_t)meta_base(mi) + extra)
+                raise_error(err, FX_ERR_INTERNAL);
+            att += 1;
+            draws_total += draws;
+            written += (values[0] != orig[0] || values[1] != orig[1] || values[2] != orig[2]);
+            const uint16_t e0[3] = {__ldg(ident + (raw.x & 0xFFFFu)), __ldg(ident + (raw.x >> 16)),
+                                    __ldg(ident + (raw.y & 0xFFFFu))};
+            uint16_t e[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                e[c] = e0[c];
+                if (!(values[c] == orig[c])) ok &= emit_one(values[c], hi, lo, e[c]);
+            }
+            const bool ch = (e[0] != e0[0]) || (e[1] != e0[1]) || (e[2] != e0[2]);
+            changed += ch;
+            uint16_t *o = rgb_out + 3 * (int64_t)pixel;
+            o[0] = e[0];
+            o[1] = e[1];
+            o[2] = e[2];
+            if (changed_out) changed_out[pixel] = ch ? 1 : 0;
         }
-        const bool ch = (e[0] != e0[0]) || (e[1] != e0[1]) || (e[2] != e0[2]);
-        changed += ch;
-        uint16_t *o = rgb_out + 3 * (int64_t)pixel;
-        o[0] = e[0];
-        o[1] = e[1];
-        o[2] = e[2];
-        if (changed_out) changed_out[pixel] = ch ? 1 : 0;
     }
     if (!ok) raise_error(err, FX_ERR_NONFINITE_WORK);
     // the four counters in one reduction: warps, then thread 0
@@ -899,7 +920,7 @@ cudaError_t launch_writer(const Geometry &g, const uint8_t *meta, const double *
     if (e != cudaSuccess) return e;
     k_startup_counts<<<6, 256, 0, stream>>>(meta, g.w, b.extra_after, s0 & kLcgMask, ctr,
                                             b.capacity, err);
-    k_apply<<<(unsigned)segs, kSegThreads, 0, stream>>>(
+    k_apply<<<(unsigned)std::min<int64_t>(segs, g_apply_blocks), kSegThreads, 0, stream>>>(
         meta, cand, g.sites, g.w, rgbi, lut, high, low, ident, stages, p, b.seg_base, b.seg_amb,
         b.extra_after, s0 & kLcgMask, rgb_out, changed_out, ctr, err, b.capacity);
     k_final<<<1, 1, 0, stream>>>(b.seg_base, b.seg_amb, segs, b.extra_after, s0 & kLcgMask,
