@@ -45,6 +45,7 @@ struct Arena {
     double *cand = nullptr;
     uint8_t *meta = nullptr;
     uint32_t *seg_base = nullptr, *seg_amb = nullptr;
+    uint32_t *seg_raw = nullptr;  // seg_raw_words(segments): per-segment and per-block sums
     AmbEntry *entries = nullptr;
     uint32_t *pos = nullptr, *extra = nullptr;
     uint8_t *chunk_two = nullptr;
@@ -79,6 +80,7 @@ static size_t arena_layout(const Geometry &g, int64_t amb_cap, Arena *a) {
     const size_t o_meta = take(g.sites);
     const size_t o_sb = take((g.segments + 1) * 4);
     const size_t o_sa = take((g.segments + 1) * 4);
+    const size_t o_sr = take(seg_raw_words(g.segments) * 4);
     const size_t o_ent = take(amb_cap * sizeof(AmbEntry) + 64);
     const size_t o_pos = take(amb_cap * 4);
     const size_t o_ext = take(amb_cap * 4);
@@ -102,6 +104,7 @@ static size_t arena_layout(const Geometry &g, int64_t amb_cap, Arena *a) {
         a->meta = (uint8_t *)(b + o_meta);
         a->seg_base = (uint32_t *)(b + o_sb);
         a->seg_amb = (uint32_t *)(b + o_sa);
+        a->seg_raw = (uint32_t *)(b + o_sr);
         a->entries = (AmbEntry *)(b + o_ent);
         a->pos = (uint32_t *)(b + o_pos);
         a->extra = (uint32_t *)(b + o_ext);
@@ -323,7 +326,7 @@ static int enqueue_pass(fx_context *ctx, Slot &s, const Geometry &g, const fx_pa
     // the walk scratch is sized for g_per_wave; a narrower wave uses part of it
     const int wave = (ctx->walk_wave > 0 && ctx->walk_wave < g_per_wave) ? ctx->walk_wave
                                                                          : g_per_wave;
-    WriterBuffers wb{a.seg_base, a.seg_amb, a.entries, a.pos, a.extra, a.counters,
+    WriterBuffers wb{a.seg_base, a.seg_amb, a.seg_raw, a.entries, a.pos, a.extra, a.counters,
                      a.amb_capacity, a.walk, wave, ctx->parallel_walk, ctx->walk_sigmas, cancel,
                      a.chunk_two, ctx->use_priority ? ctx->top_priority : 0};
     FX_CUDA(ctx, launch_writer(g, a.meta, a.cand, d_in, ctx->lut, ctx->high, ctx->low, ctx->ident, a.stages,

@@ -165,8 +165,18 @@ __device__ __forceinline__ double dither_delta(double value, float scale32, cons
 // Writer scratch of one frame.  `capacity` bounds the RNG-dependent channel
 // list; when a frame has more, the counters report it and the host reruns
 // the writer with a larger list (every access below is clamped to it).
+// Words of the chain prefix's partial sums: per segment (fixed << 16 |
+// RNG-dependent, 1024 sites), then per group of kSegGroup segments the
+// exclusive prefixes of fixed draws and of RNG-dependent channels.
+constexpr int kSegGroup = 8;
+__host__ __device__ inline int64_t seg_raw_words(int64_t segments) {
+    const int64_t groups = (segments + kSegGroup - 1) / kSegGroup;
+    return ((segments + 63) / 64) * 64 + 2 * (((groups + 63) / 64) * 64);
+}
+
 struct WriterBuffers {
     uint32_t *seg_base, *seg_amb;  // segments + 1 each
+    uint32_t *seg_raw;             // seg_raw_words(segments): the prefix's partial sums
     AmbEntry *entries;             // capacity (+64 bytes slack)
     uint32_t *pos;                 // capacity
     uint32_t *extra_after;         // capacity
@@ -235,9 +245,12 @@ constexpr double kDefaultWindowSigmas = 4.5;
 // Channels per staged chunk of the window walk; chunks start at multiples
 // of it in list order (segments are whole chunks).
 constexpr int kWalkChunk = 256;
+constexpr uint32_t kWalkSegLen = 4096;  // channels per walk segment (whole chunks)
 __host__ __device__ inline size_t walk_chunks(int64_t capacity) {
     return (size_t)((capacity + kWalkChunk - 1) / kWalkChunk) + 1;
 }
+void walk_segment_stats(void *scratch, int64_t capacity, unsigned long long **copy,
+                        unsigned long long **spread, size_t *bytes_each);
 cudaError_t launch_walk(const AmbEntry *entries, const uint32_t *pos, const uint32_t *n_ptr,
                         int64_t capacity, uint32_t s0, void *scratch, int per_wave,
                         bool parallel, double window_sigmas, const uint8_t *chunk_two,

@@ -31,7 +31,7 @@ constexpr int kWinThreads = 256;
 constexpr int kWinBlocksPerSM = 3;                  // three segments resident per SM
 constexpr int kWinSlots = 16;                       // candidates per thread
 constexpr int kWinMax = kWinThreads * kWinSlots;    // 4096 candidates
-constexpr uint32_t kSegLen = 4096;                  // channels per walk segment
+constexpr uint32_t kSegLen = kWalkSegLen;           // channels per walk segment
 constexpr int kWinChunk = kWalkChunk;               // channels staged per chunk
 constexpr int kWinRing = 3;                         // staged chunks in flight
 constexpr uint32_t kCompactEvery = 512;             // block compaction period (steady state)
@@ -94,50 +94,6 @@ __device__ __forceinline__ bool copies_of(const uint4 &lw, uint32_t T) {
 
 __device__ __forceinline__ uint4 intervals(const AmbEntry &e) {
     return make_uint4(e.l1, e.w1, e.l2, e.w2);
-}
-
-// Expected extras and their variance per segment, from the exact measure of
-// each copy set (a uniformly random first-draw state misses it with
-// probability p).
-__global__ void k_seg_prob(const AmbEntry *__restrict__ entries, const uint32_t *__restrict__ n_ptr,
-                           int64_t capacity, double *__restrict__ seg_mu,
-                           double *__restrict__ seg_var, const uint32_t *__restrict__ err) {
-    __shared__ double s_mu[8], s_var[8];
-    if (pass_stopped(err)) return;
-    const uint32_t n = (uint32_t)min((int64_t)*n_ptr, capacity);
-    const uint32_t i0 = blockIdx.x * kSegLen;
-    if (i0 >= n) return;
-    const uint32_t i1 = min(n, i0 + kSegLen);
-    double mu = 0.0, var = 0.0;
-    for (uint32_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
-        const AmbEntry e = entries[i];
-        double measure = 0.0;
-        if (e.l1 != 0x80u) measure += (double)((e.w1 >> 8) + 1u);
-        if (e.l2 != 0x80u) measure += (double)((e.w2 >> 8) + 1u);
-        const double p = 1.0 - measure * (1.0 / 16777216.0);
-        mu += p;
-        var += p * (1.0 - p);
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        mu += __shfl_down_sync(0xFFFFFFFFu, mu, o);
-        var += __shfl_down_sync(0xFFFFFFFFu, var, o);
-    }
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (lane == 0) {
-        s_mu[warp] = mu;
-        s_var[warp] = var;
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double a = 0.0, b = 0.0;
-        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
-            a += s_mu[k];
-            b += s_var[k];
-        }
-        seg_mu[blockIdx.x] = a;
-        seg_var[blockIdx.x] = b;
-    }
 }
 
 // ---------------------------------------------------------------------------
@@ -347,8 +303,8 @@ __device__ __forceinline__ uint32_t flag_acquire(const uint32_t *p) {
 // which the wave's resolve block waits for.
 __device__ __forceinline__ void window_block(
     const AmbEntry *__restrict__ entries, const uint32_t *__restrict__ pos, uint32_t n,
-    const double *__restrict__ seg_mu, const double *__restrict__ seg_var,
-    const WalkState *st, uint32_t wave, uint32_t per_wave, uint32_t t0,
+    const unsigned long long *__restrict__ seg_copy,
+    const unsigned long long *__restrict__ seg_spread, const WalkState *st, uint32_t wave, uint32_t per_wave, uint32_t t0,
     SegWindow *__restrict__ windows, uint32_t *__restrict__ table, SegList *__restrict__ lists,
     WalkState *stats, double sigmas, const uint8_t *__restrict__ chunk_two, uint32_t blk,
     uint32_t *flags, uint32_t tag) {
@@ -363,10 +319,12 @@ __device__ __forceinline__ void window_block(
 
     // window of candidate entry counts around the prediction
     if (tid < 32) {  // the prediction only centres the window: any summation order
+        // every segment before j is full: kSegLen channels, each drawing an
+        // extra with probability p = 1 - copying states / 2^24
         double mu = 0.0, var = 0.0;
         for (uint32_t k = seg0 + tid; k < j; k += 32) {
-            mu += seg_mu[k];
-            var += seg_var[k];
+            mu += (double)kSegLen - (double)seg_copy[k] * 0x1p-24;
+            var += (double)seg_spread[k] * 0x1p-26;
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
@@ -830,8 +788,8 @@ __device__ void resolve_block(const AmbEntry *__restrict__ entries,
 __global__ void __launch_bounds__(kWinThreads, kWinBlocksPerSM)
     k_wave(const AmbEntry *__restrict__ entries, const uint32_t *__restrict__ pos,
            const uint32_t *__restrict__ n_ptr, int64_t capacity,
-           const double *__restrict__ seg_mu, const double *__restrict__ seg_var, WalkState *st,
-           uint32_t wave, uint32_t per_wave, uint32_t t0, SegWindow *__restrict__ windows,
+           const unsigned long long *__restrict__ seg_copy,
+           const unsigned long long *__restrict__ seg_spread, WalkState *st, uint32_t wave, uint32_t per_wave, uint32_t t0, SegWindow *__restrict__ windows,
            uint32_t *__restrict__ table, SegList *__restrict__ lists,
            uint32_t *__restrict__ e_in_exact, uint32_t serial_below, double sigmas,
            const uint8_t *__restrict__ chunk_two, uint32_t *flags, uint32_t *err) {
@@ -846,7 +804,7 @@ __global__ void __launch_bounds__(kWinThreads, kWinBlocksPerSM)
     }
     const uint32_t b = blockIdx.x - 1;
     if ((wave * per_wave + b) * (uint64_t)kSegLen >= n) return;  // past the chain: no flag
-    window_block(entries, pos, n, seg_mu, seg_var, st, wave, per_wave, t0, windows, table, lists,
+    window_block(entries, pos, n, seg_copy, seg_spread, st, wave, per_wave, t0, windows, table, lists,
                  st, sigmas, chunk_two, b, flags, tag);
 }
 
@@ -994,12 +952,24 @@ __global__ void __launch_bounds__(kRewalkWarps * 32)
 
 int64_t walk_max_segments(int64_t capacity) { return (capacity + kSegLen - 1) / kSegLen + 1; }
 
+// The first two arrays of the walk scratch: per segment, the copying states
+// summed over its channels and the spread (sum of m (2^24 - m) >> 22); k_coef
+// accumulates them, so they are cleared before it.
+void walk_segment_stats(void *scratch, int64_t capacity, unsigned long long **copy,
+                        unsigned long long **spread, size_t *bytes_each) {
+    const size_t each = (size_t)walk_max_segments(capacity) * sizeof(unsigned long long);
+    char *p = reinterpret_cast<char *>(scratch);
+    *copy = reinterpret_cast<unsigned long long *>(p);
+    *spread = reinterpret_cast<unsigned long long *>(p + ((each + 255) & ~(size_t)255));
+    *bytes_each = each;
+}
+
 size_t walk_scratch_bytes(int64_t capacity, int per_wave) {
     const int64_t segs = walk_max_segments(capacity);
     size_t b = 0;
     auto add = [&](size_t n) { b += (n + 255) & ~(size_t)255; };
-    add(segs * sizeof(double));  // mu
-    add(segs * sizeof(double));  // var
+    add(segs * sizeof(unsigned long long));  // copying states per segment
+    add(segs * sizeof(unsigned long long));  // spread per segment
     add(segs * sizeof(uint32_t));  // exact E_in
     add((size_t)per_wave * sizeof(SegWindow));
     add((size_t)per_wave * kWinMax * sizeof(uint32_t));
@@ -1042,8 +1012,9 @@ cudaError_t launch_walk(const AmbEntry *entries, const uint32_t *pos, const uint
         p += (bytes + 255) & ~(size_t)255;
         return r;
     };
-    double *mu = (double *)take(segs_max * sizeof(double));
-    double *var = (double *)take(segs_max * sizeof(double));
+    unsigned long long *copy = (unsigned long long *)take(segs_max * sizeof(unsigned long long));
+    unsigned long long *spread =
+        (unsigned long long *)take(segs_max * sizeof(unsigned long long));
     uint32_t *e_in = (uint32_t *)take(segs_max * sizeof(uint32_t));
     SegWindow *windows = (SegWindow *)take((size_t)per_wave * sizeof(SegWindow));
     uint32_t *table = (uint32_t *)take((size_t)per_wave * kWinMax * sizeof(uint32_t));
@@ -1057,14 +1028,13 @@ cudaError_t launch_walk(const AmbEntry *entries, const uint32_t *pos, const uint
     const uint32_t segs = (uint32_t)segs_max;
     if (parallel) {
         const uint32_t waves = (segs + per_wave - 1) / per_wave;
-        cudaError_t e = launch_prio(k_seg_prob, dim3(segs), dim3(256), 0, stream, priority,
-                                    entries, n_ptr, capacity, mu, var, err);
-        if (e != cudaSuccess) return e;
+        cudaError_t e = cudaSuccess;
         for (uint32_t w = 0; w < waves; ++w) {
             // block 0 resolves the wave, blocks 1.. walk its windows
             const uint32_t blocks = min((uint32_t)per_wave, segs - w * per_wave) + 1u;
             e = launch_prio(k_wave, dim3(blocks), dim3(kWinThreads), sizeof(WindowSmem), stream,
-                            priority, entries, pos, n_ptr, capacity, mu, var, st, w, per_wave, t0,
+                            priority, entries, pos, n_ptr, capacity, copy, spread, st, w, per_wave,
+                            t0,
                             windows, table, lists, e_in, serial_below, window_sigmas, chunk_two,
                             flags, const_cast<uint32_t *>(err));
             if (e != cudaSuccess) return e;

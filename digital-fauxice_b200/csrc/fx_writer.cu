@@ -131,56 +131,88 @@ __device__ __forceinline__ uint32_t packed_site(uint8_t m) {
 
 constexpr int kSegWarps = 8;  // segments per block of the chain kernels (one per warp)
 
-// Fixed draws and RNG-dependent channels of every segment: one warp per
-// segment, 32 sites per lane in two 16-byte loads (the meta array starts on
-// a 256-byte boundary and segments on multiples of 1024 sites).
+static_assert(kSegWarps == kSegGroup, "a k_seg_sums block sums one group of segments");
+
+// The chain prefix's partial sums (seg_raw_words): per-segment sums, then
+// the groups' exclusive prefixes of fixed draws and RNG-dependent channels.
+struct SegRaw {
+    uint32_t *seg, *grp_base, *grp_amb;
+};
+__device__ __forceinline__ SegRaw seg_raw_view(uint32_t *raw, int64_t segs) {
+    const int64_t groups = (segs + kSegGroup - 1) / kSegGroup;
+    SegRaw v;
+    v.seg = raw;
+    v.grp_base = raw + ((segs + 63) / 64) * 64;
+    v.grp_amb = v.grp_base + ((groups + 63) / 64) * 64;
+    return v;
+}
+
+// Fixed draws and RNG-dependent channels of every segment (packed as
+// fixed << 16 | RNG-dependent), and of every group of eight segments: one
+// warp per segment, 32 sites per lane in two 16-byte loads (the meta array
+// starts on a 256-byte boundary and segments on multiples of 1024 sites),
+// one block per group.  The group sums go where k_seg_scan writes the
+// groups' prefixes.
 __global__ void __launch_bounds__(kSegWarps * 32)
     k_seg_sums(const uint8_t *__restrict__ meta, int64_t sites, int64_t segs,
-               uint32_t *__restrict__ seg_base, uint32_t *__restrict__ seg_amb,
-               const uint32_t *__restrict__ err) {
+               uint32_t *__restrict__ raw, const uint32_t *__restrict__ err) {
+    __shared__ uint32_t s_warp[kSegWarps];
     if (pass_stopped(err)) return;
-    const int lane = threadIdx.x & 31;
-    const int64_t seg = (int64_t)blockIdx.x * kSegWarps + (threadIdx.x >> 5);
-    if (seg >= segs) return;
-    const int64_t first = seg * kSegment + lane * 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t seg = (int64_t)blockIdx.x * kSegWarps + warp;
+    const SegRaw v = seg_raw_view(raw, segs);
     uint32_t packed = 0;
-    if (first + 32 <= sites) {
-        const uint4 *q = reinterpret_cast<const uint4 *>(meta + first);
-        const uint4 u = q[0], v = q[1];
-        packed = packed_word(u.x) + packed_word(u.y) + packed_word(u.z) + packed_word(u.w) +
-                 packed_word(v.x) + packed_word(v.y) + packed_word(v.z) + packed_word(v.w);
-    } else {
-        for (int i = 0; i < 32; ++i)
-            if (first + i < sites) packed += packed_site(meta[first + i]);
+    const int64_t first = seg * kSegment + lane * 32;
+    if (seg < segs) {
+        if (first + 32 <= sites) {
+            const uint4 *q = reinterpret_cast<const uint4 *>(meta + first);
+            const uint4 u = q[0], w = q[1];
+            packed = packed_word(u.x) + packed_word(u.y) + packed_word(u.z) + packed_word(u.w) +
+                     packed_word(w.x) + packed_word(w.y) + packed_word(w.z) + packed_word(w.w);
+        } else {
+            for (int i = 0; i < 32; ++i)
+                if (first + i < sites) packed += packed_site(meta[first + i]);
+        }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) packed += __shfl_xor_sync(0xFFFFFFFFu, packed, o);
     if (lane == 0) {
-        seg_base[seg] = packed >> 16;
-        seg_amb[seg] = packed & 0xFFFFu;
+        if (seg < segs) v.seg[seg] = packed;
+        s_warp[warp] = packed;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t g = 0;  // at most 8 x 6144 fixed draws and 8 x 3072 channels
+#pragma unroll
+        for (int k = 0; k < kSegWarps; ++k) g += s_warp[k];
+        v.grp_base[blockIdx.x] = g;
     }
 }
 
-// Exclusive scan of the per-segment sums; entry [n] holds the totals.  One
-// block of 1024 threads, over tiles of 4096 segments: a tile is loaded
-// coalesced into shared memory, each thread scans four neighbouring
-// segments, and one block scan of (fixed << 32 | RNG-dependent) pairs gives
-// the threads' offsets (the RNG-dependent total stays below 2^32: at most
-// three per site).
+// Exclusive scan of the groups' sums into the groups' prefixes; seg_base[n]
+// and seg_amb[n] get the totals (n segments).  One block of 1024 threads,
+// over tiles of 4096 groups (a native frame has 2.8 k): a tile is loaded
+// coalesced into shared memory, each thread scans four neighbouring groups,
+// and one block scan of (fixed << 32 | RNG-dependent) pairs gives the
+// threads' offsets (the RNG-dependent total stays below 2^32: at most three
+// per site).  k_amb adds a segment's offset inside its group.
 __global__ void __launch_bounds__(1024)
-    k_seg_scan(uint32_t *__restrict__ seg_base, uint32_t *__restrict__ seg_amb, int64_t n,
-               const uint32_t *__restrict__ err) {
+    k_seg_scan(uint32_t *__restrict__ raw, int64_t n, uint32_t *__restrict__ seg_base,
+               uint32_t *__restrict__ seg_amb, const uint32_t *__restrict__ err) {
     constexpr int kPerThread = 4, kTile = 1024 * kPerThread;
     __shared__ uint32_t tb[kTile], ta[kTile];
     __shared__ unsigned long long ws[32];
     if (pass_stopped(err)) return;
+    const SegRaw v = seg_raw_view(raw, n);
+    const int64_t groups = (n + kSegGroup - 1) / kSegGroup;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     unsigned long long carry = 0;
-    for (int64_t t0 = 0; t0 < n; t0 += kTile) {
+    for (int64_t t0 = 0; t0 < groups; t0 += kTile) {
         for (int j = tid; j < kTile; j += 1024) {
             const int64_t i = t0 + j;
-            tb[j] = i < n ? seg_base[i] : 0u;
-            ta[j] = i < n ? seg_amb[i] : 0u;
+            const uint32_t g = i < groups ? v.grp_base[i] : 0u;
+            tb[j] = g >> 16;
+            ta[j] = g & 0xFFFFu;
         }
         __syncthreads();
         unsigned long long mine = 0;
@@ -196,31 +228,31 @@ __global__ void __launch_bounds__(1024)
         if (lane == 31) ws[warp] = x;
         __syncthreads();
         if (warp == 0) {
-            unsigned long long v = ws[lane];
+            unsigned long long w = ws[lane];
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
-                const unsigned long long y = __shfl_up_sync(0xFFFFFFFFu, v, o);
-                if (lane >= o) v += y;
+                const unsigned long long y = __shfl_up_sync(0xFFFFFFFFu, w, o);
+                if (lane >= o) w += y;
             }
-            ws[lane] = v;
+            ws[lane] = w;
         }
         __syncthreads();
         unsigned long long run = carry + (warp ? ws[warp - 1] : 0ull) + x - mine;
 #pragma unroll
         for (int k = 0; k < kPerThread; ++k) {
             const int j = kPerThread * tid + k;
-            const unsigned long long v = ((unsigned long long)tb[j] << 32) | ta[j];
+            const unsigned long long val = ((unsigned long long)tb[j] << 32) | ta[j];
             tb[j] = (uint32_t)(run >> 32);
             ta[j] = (uint32_t)run;
-            run += v;
+            run += val;
         }
         carry += ws[31];
         __syncthreads();
         for (int j = tid; j < kTile; j += 1024) {
             const int64_t i = t0 + j;
-            if (i < n) {
-                seg_base[i] = tb[j];
-                seg_amb[i] = ta[j];
+            if (i < groups) {
+                v.grp_base[i] = tb[j];
+                v.grp_amb[i] = ta[j];
             }
         }
         __syncthreads();
@@ -406,9 +438,9 @@ __device__ void copy_intervals(const ChannelView &cv, AmbEntry &e, uint32_t *err
 // are written by consecutive lanes to consecutive list positions.
 __global__ void __launch_bounds__(kSegWarps * 32)
     k_amb(const uint8_t *__restrict__ meta, int64_t sites, int64_t segs,
-          const uint32_t *__restrict__ seg_base, const uint32_t *__restrict__ seg_amb,
-          uint32_t *__restrict__ site_of, uint32_t *__restrict__ pos_out, int64_t capacity,
-          const uint32_t *__restrict__ err) {
+          uint32_t *__restrict__ raw, uint32_t *__restrict__ seg_base,
+          uint32_t *__restrict__ seg_amb, uint32_t *__restrict__ site_of,
+          uint32_t *__restrict__ pos_out, int64_t capacity, const uint32_t *__restrict__ err) {
     if (pass_stopped(err)) return;
     const int lane = threadIdx.x & 31;
     const int64_t seg = (int64_t)blockIdx.x * kSegWarps + (threadIdx.x >> 5);
@@ -417,7 +449,20 @@ __global__ void __launch_bounds__(kSegWarps * 32)
     uint8_t m[32];
 #pragma unroll
     for (int r = 0; r < 32; ++r) m[r] = (first + 32 * r < sites) ? meta[first + 32 * r] : 0;
-    uint32_t P = seg_base[seg], A = seg_amb[seg];
+    // the segment's prefix: its group's, plus the segments before it in the
+    // group (fewer than eight, so the packed halves cannot carry); written
+    // for the kernels after the walk
+    const SegRaw v = seg_raw_view(raw, segs);
+    const int64_t grp = seg / kSegGroup, k0 = grp * kSegGroup;
+    uint32_t before = (k0 + lane < seg) ? v.seg[k0 + lane] : 0u;
+#pragma unroll
+    for (int o = 4; o > 0; o >>= 1) before += __shfl_xor_sync(0xFFFFFFFFu, before, o);
+    before = __shfl_sync(0xFFFFFFFFu, before, 0);
+    uint32_t P = v.grp_base[grp] + (before >> 16), A = v.grp_amb[grp] + (before & 0xFFFFu);
+    if (lane == 0) {
+        seg_base[seg] = P;
+        seg_amb[seg] = A;
+    }
 #pragma unroll
     for (int r = 0; r < 32; ++r) {
         const uint8_t mi = m[r];
@@ -504,7 +549,8 @@ __global__ void k_coef(AmbEntry *__restrict__ entries, const uint32_t *__restric
                        const uint32_t *__restrict__ site_of, const uint8_t *__restrict__ meta,
                        const double *__restrict__ cand, int w, const uint16_t *__restrict__ rgbi,
                        const float *__restrict__ lut, fx_params p, uint32_t *err,
-                       uint8_t *__restrict__ chunk_two) {
+                       uint8_t *__restrict__ chunk_two, unsigned long long *__restrict__ seg_copy,
+                       unsigned long long *__restrict__ seg_spread) {
     if (pass_stopped(err)) return;
     const uint32_t n = (uint32_t)min((int64_t)*n_amb_ptr, capacity);
     const DitherConst dc = dither_const(p);
@@ -536,6 +582,24 @@ __global__ void k_coef(AmbEntry *__restrict__ entries, const uint32_t *__restric
         // a chunk of walk channels with a two-interval entry steps with both
         // interval tests (every other chunk with one)
         if (e.l2 != 0x80u) chunk_two[i / kWalkChunk] = 1;
+        // the walk's prediction for this segment: m copying states of 2^24
+        // (an extra draw with probability p = 1 - m / 2^24), summed exactly
+        // per segment, with the spread m (2^24 - m) >> 22 (p (1 - p) in
+        // units of 2^-26).  A warp holds 32 consecutive entries of one
+        // segment; the lanes past the chain's end have left the loop.
+        {
+            uint32_t m = 0;
+            if (e.l1 != 0x80u) m += (e.w1 >> 8) + 1u;
+            if (e.l2 != 0x80u) m += (e.w2 >> 8) + 1u;
+            const uint32_t q = (uint32_t)(((unsigned long long)m * ((1u << 24) - m)) >> 22);
+            const uint32_t lane = threadIdx.x & 31, live = n - (i - lane);
+            const uint32_t mask = live >= 32u ? 0xFFFFFFFFu : ((1u << live) - 1u);
+            const uint32_t ms = __reduce_add_sync(mask, m), qs = __reduce_add_sync(mask, q);
+            if (lane == 0) {
+                atomicAdd(&seg_copy[i / kWalkSegLen], (unsigned long long)ms);
+                atomicAdd(&seg_spread[i / kWalkSegLen], (unsigned long long)qs);
+            }
+        }
         const uint64_t gap = (i == 0) ? (uint64_t)l0.gap_hi + 1u
                                       : (uint64_t)(uint32_t)(l0.gap_hi - l0.gap_lo);
         const Affine f = lcg_power_t(gap);
@@ -894,19 +958,26 @@ cudaError_t launch_writer(const Geometry &g, const uint8_t *meta, const double *
     const int pr = b.priority;
     const unsigned seg_blocks = (unsigned)((segs + kSegWarps - 1) / kSegWarps);
     e = launch_prio(k_seg_sums, dim3(seg_blocks), dim3(kSegWarps * 32), 0, stream, pr, meta,
-                    g.sites, segs, b.seg_base, b.seg_amb, err);
+                    g.sites, segs, b.seg_raw, err);
     if (e != cudaSuccess) return e;
-    e = launch_prio(k_seg_scan, dim3(1), dim3(1024), 0, stream, pr, b.seg_base, b.seg_amb, segs,
-                    err);
+    e = launch_prio(k_seg_scan, dim3(1), dim3(1024), 0, stream, pr, b.seg_raw, segs, b.seg_base,
+                    b.seg_amb, err);
     if (e != cudaSuccess) return e;
     // the site list lives in extra_after until the walk writes the counts
     e = launch_prio(k_amb, dim3(seg_blocks), dim3(kSegWarps * 32), 0, stream, pr, meta, g.sites,
-                    segs, b.seg_base, b.seg_amb, b.extra_after, b.pos, b.capacity, err);
+                    segs, b.seg_raw, b.seg_base, b.seg_amb, b.extra_after, b.pos, b.capacity,
+                    err);
     if (e != cudaSuccess) return e;
     const uint32_t *n_amb = b.seg_amb + segs;
     cudaMemsetAsync(b.chunk_two, 0, walk_chunks(b.capacity), stream);
+    unsigned long long *seg_copy, *seg_spread;
+    size_t stat_bytes;
+    walk_segment_stats(b.walk_scratch, b.capacity, &seg_copy, &seg_spread, &stat_bytes);
+    cudaMemsetAsync(seg_copy, 0, stat_bytes, stream);
+    cudaMemsetAsync(seg_spread, 0, stat_bytes, stream);
     e = launch_prio(k_coef, dim3(1184), dim3(256), 0, stream, pr, b.entries, b.pos, n_amb,
-                    b.capacity, b.extra_after, meta, cand, g.w, rgbi, lut, p, err, b.chunk_two);
+                    b.capacity, b.extra_after, meta, cand, g.w, rgbi, lut, p, err, b.chunk_two,
+                    seg_copy, seg_spread);
     if (e != cudaSuccess) return e;
     marks.mark(5, stream);
     e = launch_gate(b.cancel, err, stream);
