@@ -979,7 +979,8 @@ cudaError_t launch_analysis(const uint16_t *rgbi, const Geometry &g, const float
                             const fx_stage *stages, const fx_params &p, float *aux, float *hs,
                             float *hwa, float *hwr, int64_t plane, double *cand, uint8_t *meta,
                             uint32_t *err, cudaStream_t stream, const Marks &marks,
-                            int tile_rows) {
+                            int tile_rows, cudaStream_t side, cudaEvent_t fork,
+                            cudaEvent_t join) {
     const CombineConst cc = combine_const(p);
     {
         dim3 block(256), grid((g.pitch + kPlaneCols - 1) / kPlaneCols, g.prow);
@@ -987,6 +988,19 @@ cudaError_t launch_analysis(const uint16_t *rgbi, const Geometry &g, const float
                                              err);
     }
     marks.mark(2, stream);
+    // k_startup (the six hidden stages, 6 W sites: too few blocks to fill the
+    // GPU) runs on `side` beside the stencil: both only read the planes and
+    // they write disjoint sites (startup sites 0 .. 6W-1, public ones after)
+    StartupView v{g, aux, hs, hwa, hwr, plane, p.cross_neighbor ? 5 : 4};
+    const dim3 su_block(128), su_grid((g.w + 127) / 128, 6);
+    if (side) {
+        cudaError_t e = cudaEventRecord(fork, stream);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(side, fork, 0);
+        if (e != cudaSuccess) return e;
+        k_startup<<<su_grid, su_block, 0, side>>>(rgbi, v, lut, stages, p, cc, cand, meta, err);
+        e = cudaEventRecord(join, side);
+        if (e != cudaSuccess) return e;
+    }
     if (tile_rows == 16) {
         dim3 grid(g.tw, g.hp / 16);
         k_stencil<16><<<grid, Tile<16>::THREADS, sizeof(StencilSmem<16>), stream>>>(
@@ -997,11 +1011,11 @@ cudaError_t launch_analysis(const uint16_t *rgbi, const Geometry &g, const float
             rgbi, g, lut, stages, p, cc, aux, hs, hwa, hwr, plane, cand, meta, err);
     }
     marks.mark(3, stream);
-    {
-        StartupView v{g, aux, hs, hwa, hwr, plane, p.cross_neighbor ? 5 : 4};
-        dim3 block(128), grid((g.w + 127) / 128, 6);
-        k_startup<<<grid, block, 0, stream>>>(rgbi, v, lut, stages, p, cc, cand, meta, err);
-    }
+    if (side) {
+        const cudaError_t e = cudaStreamWaitEvent(stream, join, 0);
+        if (e != cudaSuccess) return e;
+    } else
+        k_startup<<<su_grid, su_block, 0, stream>>>(rgbi, v, lut, stages, p, cc, cand, meta, err);
     marks.mark(4, stream);
     return cudaGetLastError();
 }

@@ -123,6 +123,8 @@ static size_t arena_layout(const Geometry &g, int64_t amb_cap, Arena *a) {
 
 struct Slot {
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;  // k_startup, beside the stencil (greatest priority)
+    cudaEvent_t fork = nullptr, join = nullptr;
     cudaStream_t last_stream = nullptr;  // stream of the last device-buffer pass
     cudaEvent_t done = nullptr;
     Arena arena;
@@ -322,7 +324,7 @@ static int enqueue_pass(fx_context *ctx, Slot &s, const Geometry &g, const fx_pa
     FX_CUDA(ctx, launch_gate(cancel, a.err, st));
     FX_CUDA(ctx, launch_analysis(d_in, g, ctx->lut, a.stages, p, a.aux, a.hs, a.hwa, a.hwr,
                                  (int64_t)g.prow * g.pitch, a.cand, a.meta, a.err, st, marks,
-                                 ctx->stencil_rows));
+                                 ctx->stencil_rows, s.side, s.fork, s.join));
     // the walk scratch is sized for g_per_wave; a narrower wave uses part of it
     const int wave = (ctx->walk_wave > 0 && ctx->walk_wave < g_per_wave) ? ctx->walk_wave
                                                                          : g_per_wave;
@@ -404,6 +406,10 @@ static int ensure_slots(fx_context *ctx, int n) {
         ctx->slots.emplace_back();
         Slot &s = ctx->slots.back();
         FX_CUDA(ctx, cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking));
+        FX_CUDA(ctx, cudaStreamCreateWithPriority(&s.side, cudaStreamNonBlocking,
+                                                  ctx->top_priority));
+        FX_CUDA(ctx, cudaEventCreateWithFlags(&s.fork, cudaEventDisableTiming));
+        FX_CUDA(ctx, cudaEventCreateWithFlags(&s.join, cudaEventDisableTiming));
         FX_CUDA(ctx, cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming));
         FX_CUDA(ctx, cudaMallocHost(&s.h_ctr, dev_counters_bytes() + 64));  // + err + count
         void *word = nullptr;
@@ -531,8 +537,14 @@ FX_API void fx_context_destroy(fx_context *ctx) {
         if (s.h_ctr) cudaFreeHost(s.h_ctr);
         if (s.cancel_host) cudaFreeHost(const_cast<uint32_t *>(s.cancel_host));
         if (s.done) cudaEventDestroy(s.done);
+        if (s.fork) cudaEventDestroy(s.fork);
+        if (s.join) cudaEventDestroy(s.join);
         for (cudaEvent_t e : s.chunk_done)
             if (e) cudaEventDestroy(e);
+        if (s.side) {
+            cudaStreamSynchronize(s.side);
+            cudaStreamDestroy(s.side);
+        }
         if (s.stream) cudaStreamDestroy(s.stream);
     }
     for (auto &v : ctx->pending)

@@ -227,7 +227,8 @@ cudaError_t launch_analysis(const uint16_t *rgbi, const Geometry &g, const float
                             const fx_stage *stages, const fx_params &p, float *aux, float *hs,
                             float *hwa, float *hwr, int64_t plane, double *cand, uint8_t *meta,
                             uint32_t *err, cudaStream_t stream, const Marks &marks,
-                            int tile_rows);
+                            int tile_rows, cudaStream_t side, cudaEvent_t fork,
+                            cudaEvent_t join);
 cudaError_t writer_identity_table(const float *lut, const uint32_t *hi, const uint32_t *lo,
                                   uint16_t *ident, uint32_t *bad, cudaStream_t stream);
 cudaError_t launch_writer(const Geometry &g, const uint8_t *meta, const double *cand,

@@ -420,7 +420,10 @@ constexpr int kEpochChunk = 1024;
 
 struct ScanSmem {
     double v[2][3][kScanChunk];
-    float add[2][kEpochChunk];  // the epoch chain's inputs, staged by warp 1
+    float add[2][kEpochChunk];     // the epoch chain's inputs, staged by warp 1
+    double sum[2][kEpochChunk];    // the chain's binary64 sums (den, num) per epoch
+    float q[2][kEpochChunk];       // (p1, p2) of epochs with a nonzero denominator
+    uint8_t defined[kEpochChunk];  // 1 when the epoch's denominator is nonzero
 };
 
 __device__ __forceinline__ void scan_barrier() {
@@ -433,8 +436,8 @@ __global__ void __launch_bounds__(kScanThreads) k_producer_scan(int h, int ne, P
     const int tid = threadIdx.x;
     if (tid >= 32 && tid < 64) {
         // the epoch chain: warp 1 stages each chunk of its inputs into shared
-        // memory (coalesced), lane 0 walks it (shared loads do not wait for
-        // the chain's global stores)
+        // memory (coalesced); lane 0 runs the accumulations, the warp the
+        // quotients (off the chain), lane 0 carries the last defined pair
         const int lane = tid - 32;
         float den = 0.0f, num = 0.0f, p1 = kInitialScale, p2 = kInitialScale;
         for (int e0 = 0; e0 < ne; e0 += kEpochChunk) {
@@ -444,20 +447,45 @@ __global__ void __launch_bounds__(kScanThreads) k_producer_scan(int h, int ne, P
                 S.add[1][k] = b.add[ne + e0 + k];
             }
             __syncwarp();
+            // the float accumulations are the only dependence between
+            // epochs: lane 0 runs them alone and keeps each epoch's sums
             if (lane == 0) {
                 for (int k = 0; k < n; ++k) {
                     const double dw = (double)den + (double)S.add[0][k];
                     const double nw = (double)num + (double)S.add[1][k];
                     den = (float)dw;
                     num = (float)nw;
-                    if (dw != 0.0) {
-                        const double ratio = nw / dw;
-                        p2 = (float)ratio;
-                        p1 = (float)((double)kScaleMultiplier * ratio);
-                    }
-                    b.p_epoch[e0 + k] = p1;
-                    b.p_epoch[ne + e0 + k] = p2;
+                    S.sum[0][k] = dw;
+                    S.sum[1][k] = nw;
                 }
+            }
+            __syncwarp();
+            // each epoch's quotient on its own lane
+            for (int k = lane; k < n; k += 32) {
+                const double dw = S.sum[0][k];
+                S.defined[k] = dw != 0.0;
+                if (dw != 0.0) {
+                    const double ratio = S.sum[1][k] / dw;
+                    S.q[1][k] = (float)ratio;
+                    S.q[0][k] = (float)((double)kScaleMultiplier * ratio);
+                }
+            }
+            __syncwarp();
+            // an epoch without a denominator keeps the last defined pair
+            if (lane == 0) {
+                for (int k = 0; k < n; ++k) {
+                    if (S.defined[k]) {
+                        p1 = S.q[0][k];
+                        p2 = S.q[1][k];
+                    }
+                    S.q[0][k] = p1;
+                    S.q[1][k] = p2;
+                }
+            }
+            __syncwarp();
+            for (int k = lane; k < n; k += 32) {
+                b.p_epoch[e0 + k] = S.q[0][k];
+                b.p_epoch[ne + e0 + k] = S.q[1][k];
             }
             __syncwarp();
         }
