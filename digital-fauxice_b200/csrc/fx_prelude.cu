@@ -173,6 +173,11 @@ __device__ void finish_terms(const float vq[4], const float iq[4], uint32_t raw_
 constexpr int kRowTile = 64;          // columns per tile (8 cells)
 constexpr int kRowWarps = 16;
 constexpr int kRowPitch = kRowTile + 1;
+// Staged sample rows are 68 samples (544 bytes) apart: consecutive rows then
+// start 8 banks apart, so the four rows of a cell's failing-position ballot
+// (8 lanes per row, 64 bytes each) take the two wavefronts 256 bytes need,
+// where a 512-byte pitch put all four rows on the same 16 banks.
+constexpr int kRawPitch = kRowTile + 4;
 constexpr int kProductWarps = 14;     // warps 1..14
 constexpr int kStageRows = kRowWarps * 32 / kRowTile;  // rows one staging pass covers
 // Rows per block: five 8-row epochs, so a native frame (5782 rows) is 145
@@ -185,7 +190,7 @@ static_assert(kRows % 8 == 0 && kRows % kStageRows == 0 && kRows > 32 && kRows <
               "warp 0 sums kRows rows in two lane sets");
 
 struct RowSmem {
-    uint2 raw[2][kRows][kRowTile];     // staged RGBI samples
+    uint2 raw[2][kRows][kRawPitch];    // staged RGBI samples
     double p[2][3][kRows][kRowPitch];  // [buffer][visible, infrared, weight][row][column]
     int fp[kRowBlocks][8];             // first failing position per (8-row block, cell)
     float qv[2][kTileCells][8];        // quadrant trees per tile cell (rb * 8 + cc)

@@ -822,11 +822,27 @@ constexpr int kGroup = 8;
 // A warp walks kRewalkLanes segments at once, one per lane, so resident
 // warps no longer each issue a full instruction stream for a single chain
 // (with one walking lane, lane 0 measured 61 cycles per channel against 30
-// for the bare step).  216 KB: one block of 16 segments per SM.
-struct RewalkSmem {
-    AmbEntry ring[kRewalkWarps][kRewalkLanes][kRewalkRing][kRewalkChunk];
-    uint32_t out[kRewalkWarps][kRewalkLanes][kRewalkRing][kRewalkChunk];
+// for the bare step).  217 KB: one block of 16 segments per SM.
+// A segment's ring and output rows are padded (32 bytes and one word), so
+// that the four walking lanes of a warp, which read and write the same
+// offset of four different segments, fall into different shared-memory
+// banks (unpadded, the segments' strides are multiples of 128 bytes and
+// every entry load was a four-way conflict).
+struct RewalkRing {
+    AmbEntry e[kRewalkRing][kRewalkChunk];
+    uint4 pad[2];
 };
+struct RewalkOut {
+    uint32_t v[kRewalkRing][kRewalkChunk];
+    uint32_t pad;
+};
+struct RewalkSmem {
+    RewalkRing ring[kRewalkWarps][kRewalkLanes];
+    RewalkOut out[kRewalkWarps][kRewalkLanes];
+};
+static_assert(sizeof(RewalkRing) % 128 == 32 && sizeof(RewalkOut) / 4 % 32 == 1,
+              "the walking lanes' segments start in different banks");
+static_assert(sizeof(RewalkSmem) <= 232448, "one rewalk block fits an SM's shared memory");
 
 __device__ __forceinline__ void step(const uint4 &lw, const uint4 &ac, uint32_t &T, uint32_t &extra,
                                      uint32_t &E) {
@@ -870,7 +886,7 @@ __global__ void __launch_bounds__(kRewalkWarps * 32)
                 if (first >= s_i1[q]) continue;  // warp-uniform
                 const uint32_t count = min((uint32_t)kRewalkChunk, s_i1[q] - first);
                 const uint4 *src = reinterpret_cast<const uint4 *>(entries + first);
-                uint4 *dst = reinterpret_cast<uint4 *>(S.ring[warp][q][k % kRewalkRing]);
+                uint4 *dst = reinterpret_cast<uint4 *>(S.ring[warp][q].e[k % kRewalkRing]);
                 for (uint32_t v = lane; v < 2 * count; v += 32) {
                     const uint32_t sa = (uint32_t)__cvta_generic_to_shared(dst + v);
                     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa),
@@ -902,8 +918,8 @@ __global__ void __launch_bounds__(kRewalkWarps * 32)
         if (walker && first < i1) {
             const uint32_t count = min((uint32_t)kRewalkChunk, i1 - first);
             const uint4 *__restrict__ e4 =
-                reinterpret_cast<const uint4 *>(S.ring[warp][me][k % kRewalkRing]);
-            uint32_t *__restrict__ o = S.out[warp][me][k % kRewalkRing];
+                reinterpret_cast<const uint4 *>(S.ring[warp][me].e[k % kRewalkRing]);
+            uint32_t *__restrict__ o = S.out[warp][me].v[k % kRewalkRing];
             uint32_t i = 0;
             if (k == 0) {
                 // the first channel needs no transition: its state is the jump
@@ -938,7 +954,7 @@ __global__ void __launch_bounds__(kRewalkWarps * 32)
             const uint32_t f = s_i0[q] + k * kRewalkChunk;
             if (f >= s_i1[q]) continue;  // warp-uniform
             const uint32_t count = min((uint32_t)kRewalkChunk, s_i1[q] - f);
-            const uint32_t *o = S.out[warp][q][k % kRewalkRing];
+            const uint32_t *o = S.out[warp][q].v[k % kRewalkRing];
             for (uint32_t r = lane; r < count; r += 32) extra_after[f + r] = o[r];
         }
         __syncwarp();
