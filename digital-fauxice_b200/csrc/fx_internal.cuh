@@ -140,21 +140,37 @@ __device__ __forceinline__ double dither_raw_delta(double cand, double envelope,
     return envelope * random_value;
 }
 
-// conditional_dither_delta with the state advanced in place.  Returns the
-// accepted delta (or 0).  `drew` reports whether the LCG advanced.
-__device__ __forceinline__ double dither_delta(double value, float scale32, const DitherConst &dc,
-                                               uint32_t &state, int &drew) {
+// conditional_dither_delta split in two: the state-free part of one
+// channel (whether it draws, the float32-rounded candidate, the binary64
+// envelope and the float32 span), computed once for both draws a channel
+// may take, and one draw with the state advanced in place.
+struct DitherChannel {
+    double cand, envelope;
+    float span;
+    bool draws;
+};
+
+__device__ __forceinline__ DitherChannel dither_channel(double value, float scale32,
+                                                        const DitherConst &dc) {
+    DitherChannel ch;
     const float cand32 = (float)value;
-    const double cand = (double)cand32;
+    ch.cand = (double)cand32;
+    ch.draws = dc.low_lt_high && dc.low < ch.cand && ch.cand < dc.high;
+    ch.envelope = ((dc.high - ch.cand) * (ch.cand - dc.low)) * dc.coefficient;
+    ch.span = (float)((double)scale32 * ch.cand);
+    return ch;
+}
+
+// One draw: the accepted delta (or 0).  `drew` reports whether the LCG
+// advanced.
+__device__ __forceinline__ double dither_draw(const DitherChannel &ch, const DitherConst &dc,
+                                              uint32_t &state, int &drew) {
     drew = 0;
-    if (!dc.low_lt_high) return 0.0;
-    if (!(dc.low < cand && cand < dc.high)) return 0.0;
-    const double envelope = ((dc.high - cand) * (cand - dc.low)) * dc.coefficient;
-    const float span = (float)((double)scale32 * cand);
+    if (!ch.draws) return 0.0;
     state = (125u * state + 1u) & kLcgMask;
     drew = 1;
-    const double d = dither_raw_delta(cand, envelope, span, state);
-    const double changed = cand + d;
+    const double d = dither_raw_delta(ch.cand, ch.envelope, ch.span, state);
+    const double changed = ch.cand + d;
     return (dc.low < changed && changed < dc.high) ? d : 0.0;
 }
 

@@ -814,20 +814,18 @@ __global__ void __launch_bounds__(kWinThreads, kWinBlocksPerSM)
 // ---------------------------------------------------------------------------
 
 constexpr int kRewalkWarps = 4;
-constexpr int kRewalkWalkers = 4;  // walking lanes per warp (lanes 0..3)
-constexpr int kRewalkPairs = 2;    // segments per walking lane, stepped alternately
-constexpr int kRewalkLanes = kRewalkWalkers * kRewalkPairs;  // segments per warp
-constexpr int kRewalkChunk = 64;   // channels per staged chunk and segment
+constexpr int kRewalkLanes = 4;    // segments per warp: lane l < 4 walks one
+constexpr int kRewalkChunk = 128;  // channels per staged chunk and segment
 constexpr int kRewalkRing = 3;
-constexpr int kGroup = 8;      // staged loads per step run with one segment
-constexpr int kPairGroup = 4;  // ... and with two
+constexpr int kGroup = 8;
 
-// A warp walks kRewalkLanes segments at once: four walking lanes, each with
-// two segments whose steps alternate, so that one chain's step issues while
-// the other's waits on its dependences (a segment's walk is one dependent
-// chain of 4096 steps: the kernel's time is one chain's latency).  With one
-// walking lane, lane 0 measured 61 cycles per channel against 30 for the
-// bare step.  217 KB: one block of 32 segments per SM.
+// A warp walks kRewalkLanes segments at once, one per lane, so resident
+// warps no longer each issue a full instruction stream for a single chain
+// (with one walking lane, lane 0 measured 61 cycles per channel against 30
+// for the bare step).  217 KB: one block of 16 segments per SM.  Two
+// segments per walking lane, stepped alternately in 64-channel chunks,
+// measured 301 us against 125 us: no overlap of the two chains' steps, and
+// half the SMs.
 // A segment's ring and output rows are padded (32 bytes and one word), so
 // that the four walking lanes of a warp, which read and write the same
 // offset of four different segments, fall into different shared-memory
@@ -903,105 +901,54 @@ __global__ void __launch_bounds__(kRewalkWarps * 32)
     };
 #pragma unroll
     for (int k = 0; k < kRewalkRing - 1; ++k) issue(k);
-    // this lane's own segments: walking lane w takes segments w and
-    // w + kRewalkWalkers of the warp
-    uint32_t T[kRewalkPairs], E[kRewalkPairs], extra[kRewalkPairs];
-    uint32_t i0[kRewalkPairs], i1[kRewalkPairs];
-    int me[kRewalkPairs];
-#pragma unroll
-    for (int c = 0; c < kRewalkPairs; ++c) {
-        const int q = (lane < kRewalkWalkers ? lane : 0) + kRewalkWalkers * c;
-        const uint64_t a = (uint64_t)(jbase + q) * seg_len;
-        const bool live = lane < kRewalkWalkers && a < n;
-        me[c] = q;
-        i0[c] = live ? (uint32_t)a : 0u;
-        i1[c] = live ? (uint32_t)min((uint64_t)n, a + seg_len) : 0u;
-        T[c] = 0u;
-        E[c] = 0u;
-        extra[c] = 0u;
-        if (live) {
-            const uint32_t e_in = serial ? 0u : e_in_exact[jbase + q];
-            T[c] = jump_t(t0, (uint64_t)pos[i0[c]] + 1u + e_in);  // state at i0's first draw
-            E[c] = e_in;
-        }
+    // this lane's own segment (lanes 0..kRewalkLanes-1)
+    const uint64_t my_a = (uint64_t)(jbase + (lane < kRewalkLanes ? lane : 0)) * seg_len;
+    const bool walker = lane < kRewalkLanes && my_a < n;
+    const int me = walker ? lane : 0;
+    const uint32_t i0 = walker ? (uint32_t)my_a : 0u;
+    const uint32_t i1 = walker ? (uint32_t)min((uint64_t)n, my_a + seg_len) : 0u;
+    uint32_t T = 0, E = 0, extra = 0u;
+    if (walker) {
+        const uint32_t e_in = serial ? 0u : e_in_exact[jbase + me];
+        T = jump_t(t0, (uint64_t)pos[i0] + 1u + e_in);  // state at channel i0's first draw
+        E = e_in;
     }
     for (uint32_t k = 0; k < chunks; ++k) {
         issue(k + kRewalkRing - 1);
         asm volatile("cp.async.wait_group %0;\n" ::"n"(kRewalkRing - 1));
         __syncwarp();
-        uint32_t count[kRewalkPairs];
-        const uint4 *e4[kRewalkPairs];
-        uint32_t *o[kRewalkPairs];
-#pragma unroll
-        for (int c = 0; c < kRewalkPairs; ++c) {
-            const uint32_t first = i0[c] + k * kRewalkChunk;
-            count[c] = first < i1[c] ? min((uint32_t)kRewalkChunk, i1[c] - first) : 0u;
-            e4[c] = reinterpret_cast<const uint4 *>(S.ring[warp][me[c]].e[k % kRewalkRing]);
-            o[c] = S.out[warp][me[c]].v[k % kRewalkRing];
-        }
-        uint32_t i = 0;
-        if (k == 0) {
-            // the first channel needs no transition: its state is the jump
-#pragma unroll
-            for (int c = 0; c < kRewalkPairs; ++c)
-                if (count[c]) {
-                    extra[c] = copies(e4[c][0], T[c]) ? 0u : 1u;
-                    E[c] += extra[c];
-                    o[c][0] = E[c];
-                }
-            i = 1;
-        }
-        if (count[0] == (uint32_t)kRewalkChunk && count[1] == (uint32_t)kRewalkChunk) {
-            // both chains have a full chunk: their steps alternate
-            const uint32_t groups = (kRewalkChunk - i) / kPairGroup;
-            for (uint32_t g = 0; g < groups; ++g) {
-                const uint32_t base = i + g * kPairGroup;
-                uint4 lw[kRewalkPairs][kPairGroup], ac[kRewalkPairs][kPairGroup];
-#pragma unroll
-                for (int q = 0; q < kPairGroup; ++q)
-#pragma unroll
-                    for (int c = 0; c < kRewalkPairs; ++c) {
-                        lw[c][q] = e4[c][2 * (base + q)];
-                        ac[c][q] = e4[c][2 * (base + q) + 1];
-                    }
-#pragma unroll
-                for (int q = 0; q < kPairGroup; ++q)
-#pragma unroll
-                    for (int c = 0; c < kRewalkPairs; ++c) {
-                        step(lw[c][q], ac[c][q], T[c], extra[c], E[c]);
-                        o[c][base + q] = E[c];
-                    }
+        const uint32_t first = i0 + k * kRewalkChunk;
+        if (walker && first < i1) {
+            const uint32_t count = min((uint32_t)kRewalkChunk, i1 - first);
+            const uint4 *__restrict__ e4 =
+                reinterpret_cast<const uint4 *>(S.ring[warp][me].e[k % kRewalkRing]);
+            uint32_t *__restrict__ o = S.out[warp][me].v[k % kRewalkRing];
+            uint32_t i = 0;
+            if (k == 0) {
+                // the first channel needs no transition: its state is the jump
+                extra = copies(e4[0], T) ? 0u : 1u;
+                E += extra;
+                o[0] = E;
+                i = 1;
             }
-            for (uint32_t r = i + groups * kPairGroup; r < (uint32_t)kRewalkChunk; ++r)
+            const uint32_t groups = (count - i) / kGroup;
+            for (uint32_t g = 0; g < groups; ++g) {
+                const uint32_t base = i + g * kGroup;
+                uint4 lw[kGroup], ac[kGroup];
 #pragma unroll
-                for (int c = 0; c < kRewalkPairs; ++c) {
-                    step(e4[c][2 * r], e4[c][2 * r + 1], T[c], extra[c], E[c]);
-                    o[c][r] = E[c];
+                for (int q = 0; q < kGroup; ++q) {
+                    lw[q] = e4[2 * (base + q)];
+                    ac[q] = e4[2 * (base + q) + 1];
                 }
-        } else {
-            // a chain's last chunk, or one chain: one after the other
 #pragma unroll
-            for (int c = 0; c < kRewalkPairs; ++c) {
-                if (count[c] <= i) continue;
-                const uint32_t groups = (count[c] - i) / kGroup;
-                for (uint32_t g = 0; g < groups; ++g) {
-                    const uint32_t base = i + g * kGroup;
-                    uint4 lw[kGroup], ac[kGroup];
-#pragma unroll
-                    for (int q = 0; q < kGroup; ++q) {
-                        lw[q] = e4[c][2 * (base + q)];
-                        ac[q] = e4[c][2 * (base + q) + 1];
-                    }
-#pragma unroll
-                    for (int q = 0; q < kGroup; ++q) {
-                        step(lw[q], ac[q], T[c], extra[c], E[c]);
-                        o[c][base + q] = E[c];
-                    }
+                for (int q = 0; q < kGroup; ++q) {
+                    step(lw[q], ac[q], T, extra, E);
+                    o[base + q] = E;
                 }
-                for (uint32_t r = i + groups * kGroup; r < count[c]; ++r) {
-                    step(e4[c][2 * r], e4[c][2 * r + 1], T[c], extra[c], E[c]);
-                    o[c][r] = E[c];
-                }
+            }
+            for (uint32_t r = i + groups * kGroup; r < count; ++r) {
+                step(e4[2 * r], e4[2 * r + 1], T, extra, E);
+                o[r] = E;
             }
         }
         __syncwarp();

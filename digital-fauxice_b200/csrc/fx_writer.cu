@@ -861,14 +861,15 @@ __global__ void __launch_bounds__(kSegThreads, kApplyBlocksPerSM)
 #pragma unroll
                 for (int c = 0; c < 3; ++c) {
                     int drew;
-                    const double firstd = dither_delta(c3[c], p.dither_scales[c], dc, state, drew);
+                    const DitherChannel ch = dither_channel(c3[c], p.dither_scales[c], dc);
+                    const double firstd = dither_draw(ch, dc, state, drew);
                     draws += drew;
                     if (floor_enabled && c3[c] + firstd <= (double)orig[c]) {
                         values[c] = orig[c];
                     } else {
                         double d = firstd;
                         if (floor_enabled) {
-                            d = dither_delta(c3[c], p.dither_scales[c], dc, state, drew);
+                            d = dither_draw(ch, dc, state, drew);
                             draws += drew;
                         }
                         values[c] = (float)(c3[c] + d);
