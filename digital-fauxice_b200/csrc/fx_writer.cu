@@ -544,7 +544,7 @@ __device__ __forceinline__ CoefSite coef_site(const CoefList &l, bool live, int6
 // while entry i's interval search computes, the site of entry i + 2 stride
 // and the meta, pixel and candidates of entry i + stride are in flight, so
 // the dependent gathers overlap the arithmetic instead of stalling it.
-__global__ void __launch_bounds__(256, 5) k_coef(AmbEntry *__restrict__ entries, const uint32_t *__restrict__ pos,
+__global__ void __launch_bounds__(256, 4) k_coef(AmbEntry *__restrict__ entries, const uint32_t *__restrict__ pos,
                        const uint32_t *__restrict__ n_amb_ptr, int64_t capacity,
                        const uint32_t *__restrict__ site_of, const uint8_t *__restrict__ meta,
                        const double *__restrict__ cand, int w, const uint16_t *__restrict__ rgbi,
@@ -712,7 +712,7 @@ cudaError_t writer_identity_table(const float *lut, const uint32_t *hi, const ui
 // below 2^36 draws is six table lookups and compositions.
 constexpr int kJumpDigits = 6;
 __device__ Affine g_jump[kJumpDigits][64];
-constexpr int kApplyBlocksPerSM = 6;  // k_apply's resident blocks per SM
+constexpr int kApplyBlocksPerSM = 5;  // k_apply's resident blocks per SM
 static int g_apply_blocks = kApplyBlocksPerSM * 148;
 
 cudaError_t writer_init() {
