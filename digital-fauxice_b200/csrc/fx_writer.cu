@@ -433,9 +433,10 @@ __device__ void copy_intervals(const ChannelView &cv, AmbEntry &e, uint32_t *err
 // Lists every RNG-dependent channel in chain order: entry a gets its site
 // (site_of[a], a compact array so the writes coalesce) and its draw
 // position; k_coef fills in the intervals and jumps.  One warp per segment,
-// in 32 rounds of 32 consecutive sites (all the segment's meta loads issued
-// first); a round's offsets come from one warp scan, so a round's entries
-// are written by consecutive lanes to consecutive list positions.
+// in 16 rounds of 64 consecutive sites, two neighbouring sites per lane (all
+// the segment's meta loads issued first); a round's offsets come from one
+// warp scan, so a round's entries are written by consecutive lanes to
+// consecutive list positions.
 __global__ void __launch_bounds__(kSegWarps * 32)
     k_amb(const uint8_t *__restrict__ meta, int64_t sites, int64_t segs,
           uint32_t *__restrict__ raw, uint32_t *__restrict__ seg_base,
@@ -445,10 +446,16 @@ __global__ void __launch_bounds__(kSegWarps * 32)
     const int lane = threadIdx.x & 31;
     const int64_t seg = (int64_t)blockIdx.x * kSegWarps + (threadIdx.x >> 5);
     if (seg >= segs) return;
-    const int64_t first = seg * kSegment + lane;
-    uint8_t m[32];
+    const int64_t first = seg * kSegment + 2 * lane;  // sites first + 64 r, + 1
+    uint32_t m2[16];  // the two meta bytes of round r
 #pragma unroll
-    for (int r = 0; r < 32; ++r) m[r] = (first + 32 * r < sites) ? meta[first + 32 * r] : 0;
+    for (int r = 0; r < 16; ++r) {
+        const int64_t s0 = first + 64 * r;
+        if (s0 + 1 < sites)
+            m2[r] = *reinterpret_cast<const uint16_t *>(meta + s0);  // even offset
+        else
+            m2[r] = s0 < sites ? meta[s0] : 0u;
+    }
     // the segment's prefix: its group's, plus the segments before it in the
     // group (fewer than eight, so the packed halves cannot carry); written
     // for the kernels after the walk
@@ -464,9 +471,9 @@ __global__ void __launch_bounds__(kSegWarps * 32)
         seg_amb[seg] = A;
     }
 #pragma unroll
-    for (int r = 0; r < 32; ++r) {
-        const uint8_t mi = m[r];
-        const uint32_t x = packed_site(mi);
+    for (int r = 0; r < 16; ++r) {
+        const uint8_t mb[2] = {(uint8_t)(m2[r] & 0xFFu), (uint8_t)(m2[r] >> 8)};
+        const uint32_t x0 = packed_site(mb[0]), x = x0 + packed_site(mb[1]);
         uint32_t inc = x;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -474,21 +481,26 @@ __global__ void __launch_bounds__(kSegWarps * 32)
             if (lane >= o) inc += y;
         }
         const uint32_t total = __shfl_sync(0xFFFFFFFFu, inc, 31);
-        const uint32_t ex = inc - x;
         if (x & 0xFFFFu) {
+            const uint32_t ex = inc - x;
             uint32_t pos = P + (ex >> 16), a = A + (ex & 0xFFFFu);
 #pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                const int code = meta_code(mi, c);
-                if (code == 3) {
-                    if ((int64_t)a < capacity) {
-                        site_of[a] = (uint32_t)(first + 32 * r);
-                        pos_out[a] = pos;
+            for (int h = 0; h < 2; ++h) {
+                const uint8_t mi = mb[h];
+                pos = P + ((ex + (h ? x0 : 0u)) >> 16);
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    const int code = meta_code(mi, c);
+                    if (code == 3) {
+                        if ((int64_t)a < capacity) {
+                            site_of[a] = (uint32_t)(first + 64 * r + h);
+                            pos_out[a] = pos;
+                        }
+                        ++a;
+                        pos += 1u;
+                    } else {
+                        pos += (uint32_t)code;
                     }
-                    ++a;
-                    pos += 1u;
-                } else {
-                    pos += (uint32_t)code;
                 }
             }
         }
