@@ -47,29 +47,31 @@ struct DevCounters {
 // Block scan helpers (256 threads)
 // ---------------------------------------------------------------------------
 
+// Exclusive scan of 64-bit values (packed counters) over a block of NT threads.
 template <int NT>
-__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t &total,
-                                                         uint32_t *warp_sums) {
+__device__ __forceinline__ unsigned long long block_exclusive_scan64(unsigned long long v,
+                                                                    unsigned long long &total,
+                                                                    unsigned long long *warp_sums) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint32_t x = v;
+    unsigned long long x = v;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        const unsigned long long y = __shfl_up_sync(0xFFFFFFFFu, x, o);
         if (lane >= o) x += y;
     }
     if (lane == 31) warp_sums[warp] = x;
     __syncthreads();
     if (warp == 0) {
-        uint32_t s = (lane < NT / 32) ? warp_sums[lane] : 0u;
+        unsigned long long w = (lane < NT / 32) ? warp_sums[lane] : 0ull;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, s, o);
-            if (lane >= o) s += y;
+            const unsigned long long y = __shfl_up_sync(0xFFFFFFFFu, w, o);
+            if (lane >= o) w += y;
         }
-        if (lane < NT / 32) warp_sums[lane] = s;
+        if (lane < NT / 32) warp_sums[lane] = w;
     }
     __syncthreads();
-    const uint32_t prefix = warp ? warp_sums[warp - 1] : 0u;
+    const unsigned long long prefix = warp ? warp_sums[warp - 1] : 0ull;
     total = warp_sums[NT / 32 - 1];
     __syncthreads();
     return prefix + x - v;
@@ -261,19 +263,6 @@ __global__ void __launch_bounds__(1024)
         seg_base[n] = (uint32_t)(carry >> 32);
         seg_amb[n] = (uint32_t)carry;
     }
-}
-
-// Per-site exclusive chain offsets inside segment `seg`, one block.
-__device__ __forceinline__ void site_offsets(const uint8_t m[kPer], const uint32_t *seg_base,
-                                             const uint32_t *seg_amb, int64_t seg,
-                                             uint32_t *warp_sums, uint32_t &P, uint32_t &A) {
-    uint32_t packed = 0;
-#pragma unroll
-    for (int i = 0; i < kPer; ++i) packed += ((uint32_t)meta_base(m[i]) << 16) | meta_amb(m[i]);
-    uint32_t total;
-    const uint32_t ex = block_exclusive_scan<kSegThreads>(packed, total, warp_sums);
-    P = seg_base[seg] + (ex >> 16);
-    A = seg_amb[seg] + (ex & 0xFFFFu);
 }
 
 struct SiteInfo {
@@ -771,12 +760,12 @@ __global__ void __launch_bounds__(kSegThreads, kApplyBlocksPerSM)
             const uint32_t *__restrict__ extra_after, uint32_t s0, uint16_t *__restrict__ rgb_out,
             uint8_t *__restrict__ changed_out, DevCounters *ctr, uint32_t *err,
             int64_t capacity) {
-    __shared__ uint32_t ws[kSegThreads / 32];
     __shared__ uint32_t hi[256], lo[256];
     __shared__ unsigned long long s_sums[kSegThreads / 32][4];
     __shared__ Affine s_jump[kJumpDigits][64];
     __shared__ uint32_t s_ref[kSegment], s_p[kSegment], s_a[kSegment];
     __shared__ unsigned long long s_seg;
+    __shared__ unsigned long long ws64[kSegThreads / 32];
     if (pass_stopped(err)) return;  // cancelled: the output stays untouched
     for (int i = threadIdx.x; i < 256; i += kSegThreads) {
         hi[i] = g_high[i];
@@ -800,48 +789,48 @@ __global__ void __launch_bounds__(kSegThreads, kApplyBlocksPerSM)
         const int64_t first = seg0 + threadIdx.x * kPer;
         uint8_t m[kPer];
         load_meta(meta, first, sites, m);
-        uint32_t P, A;
-        site_offsets(m, seg_base, seg_amb, seg, ws, P, A);  // contains __syncthreads
-
-        // ---- phase 1: identity emits; list the attempted sites ---------------
-        uint32_t mine = 0, pp[kPer], aa[kPer];
-        bool listed_here[kPer];
+        // one block scan gives each thread its sites' chain offsets (fixed
+        // draws, RNG-dependent channels) and its first slot in the list of
+        // attempted public sites: (fixed << 40 | channels << 20 | attempted)
+        unsigned long long mine = 0;
 #pragma unroll
         for (int i = 0; i < kPer; ++i) {
             const int64_t site = first + i;
-            const uint8_t mi = m[i];
-            listed_here[i] = false;
-            pp[i] = P;
-            aa[i] = A;
-            if (site >= su && site < sites) {
-                if (mi & 0x80u) {
-                    listed_here[i] = true;
-                    ++mine;
-                } else {
-                    const int64_t pixel = site - su;
-                    const uint2 raw = reinterpret_cast<const uint2 *>(rgbi)[pixel];
-                    uint16_t *o = rgb_out + 3 * pixel;
-                    o[0] = __ldg(ident + (raw.x & 0xFFFFu));
-                    o[1] = __ldg(ident + (raw.x >> 16));
-                    o[2] = __ldg(ident + (raw.y & 0xFFFFu));
-                    if (changed_out) changed_out[pixel] = 0;
-                }
-            }
-            P += meta_base(mi);
-            A += meta_amb(mi);
+            const bool listed = site >= su && site < sites && (m[i] & 0x80u);
+            mine += ((unsigned long long)meta_base(m[i]) << 40) |
+                    ((unsigned long long)meta_amb(m[i]) << 20) | (listed ? 1ull : 0ull);
         }
-        uint32_t listed;
-        const uint32_t at = block_exclusive_scan<kSegThreads>(mine, listed, ws);
+        unsigned long long total;
+        const unsigned long long ex = block_exclusive_scan64<kSegThreads>(mine, total, ws64);
+        uint32_t P = seg_base[seg] + (uint32_t)(ex >> 40);
+        uint32_t A = seg_amb[seg] + (uint32_t)((ex >> 20) & 0xFFFFFu);
+        const uint32_t listed = (uint32_t)(total & 0xFFFFFu);
+
+        // ---- phase 1: identity emits; list the attempted sites ---------------
         {
-            uint32_t slot = at;
+            uint32_t slot = (uint32_t)(ex & 0xFFFFFu);
 #pragma unroll
             for (int i = 0; i < kPer; ++i) {
-                if (listed_here[i]) {
-                    s_ref[slot] = ((uint32_t)m[i] << 16) | (uint32_t)(threadIdx.x * kPer + i);
-                    s_p[slot] = pp[i];
-                    s_a[slot] = aa[i];
-                    ++slot;
+                const int64_t site = first + i;
+                const uint8_t mi = m[i];
+                if (site >= su && site < sites) {
+                    if (mi & 0x80u) {
+                        s_ref[slot] = ((uint32_t)mi << 16) | (uint32_t)(threadIdx.x * kPer + i);
+                        s_p[slot] = P;
+                        s_a[slot] = A;
+                        ++slot;
+                    } else {
+                        const int64_t pixel = site - su;
+                        const uint2 raw = reinterpret_cast<const uint2 *>(rgbi)[pixel];
+                        uint16_t *o = rgb_out + 3 * pixel;
+                        o[0] = __ldg(ident + (raw.x & 0xFFFFu));
+                        o[1] = __ldg(ident + (raw.x >> 16));
+                        o[2] = __ldg(ident + (raw.y & 0xFFFFu));
+                        if (changed_out) changed_out[pixel] = 0;
+                    }
                 }
+                P += meta_base(mi);
+                A += meta_amb(mi);
             }
         }
         __syncthreads();
