@@ -181,13 +181,13 @@ constexpr int kRawPitch = kRowTile + 4;
 constexpr int kProductWarps = 14;     // warps 1..14
 constexpr int kStageRows = kRowWarps * 32 / kRowTile;  // rows one staging pass covers
 // Rows per block: five 8-row epochs, so a native frame (5782 rows) is 145
-// blocks, one wave on 148 SMs.  Warp 0 sums rows 0..31 on its lanes and rows
-// 32..39 on lanes 0..7 as a second, interleaved set of chains.
+// blocks, one wave on 148 SMs.  Warp 0 sums rows 0..31 on its lanes; rows
+// 32..39 are summed on lanes 0..7 of the last warp, beside it.
 constexpr int kRows = 40;
 constexpr int kRowBlocks = kRows / 8;
 constexpr int kTileCells = kRowBlocks * 8;  // epoch cells of one tile
 static_assert(kRows % 8 == 0 && kRows % kStageRows == 0 && kRows > 32 && kRows <= 64,
-              "warp 0 sums kRows rows in two lane sets");
+              "rows 0..31 and 32..kRows-1 are summed by two warps");
 
 struct RowSmem {
     uint2 raw[2][kRows][kRawPitch];    // staged RGBI samples
@@ -235,7 +235,7 @@ __global__ void __launch_bounds__(kRowWarps * 32, 1)
     stage(0);
     double rv = 0.0, ri = 0.0, rw = 0.0;     // row r0 + lane
     double rv2 = 0.0, ri2 = 0.0, rw2 = 0.0;  // row r0 + 32 + lane (lanes < kRows - 32)
-    const int lane2 = lane < kRows - 32 ? lane + 32 : lane;  // other lanes re-read their row
+    const int lane2 = lane < kRows - 32 ? lane + 32 : lane;
     double den = 0.0, num = 0.0;  // lane rb < kRowBlocks: epoch (r0 / 8 + rb) sums
     for (int t = 0; t <= tiles; ++t) {
         asm volatile("cp.async.wait_group 0;\n" ::);
@@ -363,33 +363,38 @@ __global__ void __launch_bounds__(kRowWarps * 32, 1)
                 }
             }
             __syncwarp();
-            // the ordered row sums, two rows per lane interleaved
+            // the ordered row sums of rows 0..31 (one row per lane)
             const int n = min(kRowTile, active_width - u * kRowTile);
             const double *pv = S.p[u & 1][0][lane];
             const double *pi = S.p[u & 1][1][lane];
             const double *pw = S.p[u & 1][2][lane];
-            const double *pv2 = S.p[u & 1][0][lane2];
-            const double *pi2 = S.p[u & 1][1][lane2];
-            const double *pw2 = S.p[u & 1][2][lane2];
             if (n == kRowTile) {
 #pragma unroll 16
                 for (int j = 0; j < kRowTile; ++j) {
                     rv += pv[j];
                     ri += pi[j];
                     rw += pw[j];
-                    rv2 += pv2[j];
-                    ri2 += pi2[j];
-                    rw2 += pw2[j];
                 }
             } else {
                 for (int j = 0; j < n; ++j) {
                     rv += pv[j];
                     ri += pi[j];
                     rw += pw[j];
-                    rv2 += pv2[j];
-                    ri2 += pi2[j];
-                    rw2 += pw2[j];
                 }
+            }
+        }
+        if (warp == kRowWarps - 1 && t > 0 && lane < kRows - 32) {
+            // the ordered row sums of rows 32..kRows-1, beside warp 0 (the
+            // previous tile's products stay in their buffer until tile t+1's)
+            const int u = t - 1;
+            const int n = min(kRowTile, active_width - u * kRowTile);
+            const double *pv2 = S.p[u & 1][0][lane2];
+            const double *pi2 = S.p[u & 1][1][lane2];
+            const double *pw2 = S.p[u & 1][2][lane2];
+            for (int j = 0; j < n; ++j) {
+                rv2 += pv2[j];
+                ri2 += pi2[j];
+                rw2 += pw2[j];
             }
         }
     }
@@ -401,7 +406,7 @@ __global__ void __launch_bounds__(kRowWarps * 32, 1)
         b.row_sums[2 * h + row] = rw;
     }
     const int row2 = r0 + 32 + lane;
-    if (warp == 0 && lane < kRows - 32 && row2 < h) {
+    if (warp == kRowWarps - 1 && lane < kRows - 32 && row2 < h) {
         b.row_sums[row2] = rv2;
         b.row_sums[h + row2] = ri2;
         b.row_sums[2 * h + row2] = rw2;
