@@ -186,6 +186,7 @@ constexpr int kStageRows = kRowWarps * 32 / kRowTile;  // rows one staging pass 
 constexpr int kRows = 40;
 constexpr int kRowBlocks = kRows / 8;
 constexpr int kTileCells = kRowBlocks * 8;  // epoch cells of one tile
+static_assert((kRawPitch * 8) % 16 == 0, "staged rows keep 16-byte copies aligned");
 static_assert(kRows % 8 == 0 && kRows % kStageRows == 0 && kRows > 32 && kRows <= 64,
               "rows 0..31 and 32..kRows-1 are summed by two warps");
 
@@ -199,6 +200,11 @@ struct RowSmem {
     double2 tq[kTileCells][4];         // finished terms of the previous tile's cells
     int tok[kTileCells];               // 1: the cell's terms count (passing)
 };
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+}
 
 __device__ __forceinline__ void cp_async8(void *smem, const void *gmem) {
     const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
@@ -215,19 +221,36 @@ __global__ void __launch_bounds__(kRowWarps * 32, 1)
     const int tiles = (active_width + kRowTile - 1) / kRowTile;
     const int ne = h / 8;  // complete 8-row blocks
     const double thr = (double)kIrThreshold;
-    // staging: thread tid copies column tid % 64 of rows tid / 64 + 4 m
-    const int sj = tid % kRowTile, sk0 = tid / kRowTile;
+    // staging.  With an even width and a 16-byte aligned frame, every pair
+    // of samples starting at an even column is one 16-byte cp.async: thread
+    // tid copies pair tid % 32 of rows tid / 32 + 16 m (half the copy
+    // instructions of the 8-byte form, which thread tid issues for column
+    // tid % 64 of rows tid / 64 + 8 m).
+    const bool wide = (w & 1) == 0 && (reinterpret_cast<uintptr_t>(rgbi) & 15u) == 0;
+    const int sj = wide ? 2 * (tid % 32) : tid % kRowTile;
+    const int sk0 = wide ? tid / 32 : tid / kRowTile;
+    const int srows = wide ? 2 * kStageRows : kStageRows;  // rows one staging pass covers
     const uint16_t *srow = rgbi + ((int64_t)(r0 + sk0) * w + sj) * 4;
-    const int64_t srow_step = (int64_t)kStageRows * w * 4;  // kStageRows rows of samples
+    const int64_t srow_step = (int64_t)srows * w * 4;
     auto stage = [&](int t) {
         if (t < tiles) {
             const int col = t * kRowTile + sj;
             const uint16_t *src = srow + (int64_t)t * kRowTile * 4;
+            if (wide) {
 #pragma unroll
-            for (int m = 0; m < kRows / kStageRows; ++m) {
-                const int k = sk0 + kStageRows * m;
-                if (r0 + k < h && col < active_width) cp_async8(&S.raw[t & 1][k][sj], src);
-                src += srow_step;
+                for (int m = 0; m < (kRows + 2 * kStageRows - 1) / (2 * kStageRows); ++m) {
+                    const int k = sk0 + 2 * kStageRows * m;
+                    if (k < kRows && r0 + k < h && col < active_width)
+                        cp_async16(&S.raw[t & 1][k][sj], src);
+                    src += srow_step;
+                }
+            } else {
+#pragma unroll
+                for (int m = 0; m < kRows / kStageRows; ++m) {
+                    const int k = sk0 + kStageRows * m;
+                    if (r0 + k < h && col < active_width) cp_async8(&S.raw[t & 1][k][sj], src);
+                    src += srow_step;
+                }
             }
         }
         asm volatile("cp.async.commit_group;\n" ::);
