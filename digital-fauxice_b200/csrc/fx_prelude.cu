@@ -154,22 +154,20 @@ __device__ void finish_terms(const float vq[4], const float iq[4], uint32_t raw_
 }
 
 // ---------------------------------------------------------------------------
-// Cells and per-row sums in one pass over the frame.  A block of 16 warps
-// owns 40 rows (five 8-row blocks) and walks 40 x 64 tiles, the next tile's
-// samples arriving by cp.async while the current one is worked on:
-//   * warps 1..15 find, by ballot, the first IR position in each 8x8 cell
-//     that fails the threshold (cells of the tile);
-//   * warps 1..14 compute the per-pixel products of the row sums (zero where
+// Cells and per-row sums in one pass over the frame.  A block owns 32 rows
+// (four 8-row blocks) and walks 32 x 64 tiles, the next tile's samples
+// arriving by cp.async while the current one is worked on:
+//   * every warp but the first finds, by ballot, the first IR position in
+//     each 8x8 cell that fails the threshold (cells of the tile);
+//   * warps 1..7 compute the quadrant trees of complete passing cells of
+//     complete 8-row blocks (the scale epochs), one tree per thread, and
+//     warp 7 the cells' raw IR totals; warp 0 finishes the cells' terms one
+//     tile later;
+//   * warps 1..6 compute the per-pixel products of the row sums (zero where
 //     the cell failed earlier: adding +0.0 leaves a non-negative sum
-//     unchanged) into shared memory, and warps 1..10 the quadrant trees of
-//     complete passing cells of complete 8-row blocks (the scale epochs),
-//     one tree per thread;
-//   * warp 15 takes the cells' status and raw IR totals; one tile later
-//     warps 11..14 finish the cells' terms, and one tile after that warp 0
-//     adds them to the epoch sums in the reference's cell order;
-//   * warp 0 (rows 0..31) and warp 15 (rows 32..39) add the previous tile's
-//     products, one row per lane, in strict column order -- the sequential
-//     binary64 chains that set the pace of a tile.
+//     unchanged) into shared memory;
+//   * warp 0 adds the previous tile's products, one row per lane, in strict
+//     column order -- the only sequential part.
 // ---------------------------------------------------------------------------
 
 constexpr int kRowTile = 64;          // columns per tile (8 cells)
@@ -189,8 +187,6 @@ constexpr int kRows = 40;
 constexpr int kRowBlocks = kRows / 8;
 constexpr int kTileCells = kRowBlocks * 8;  // epoch cells of one tile
 static_assert((kRawPitch * 8) % 16 == 0, "staged rows keep 16-byte copies aligned");
-static_assert(kRowWarps == 16 && kProductWarps == 14 && kTileCells <= 40,
-              "warps 11..14 finish a tile's cells, ten each");
 static_assert(kRows % 8 == 0 && kRows % kStageRows == 0 && kRows > 32 && kRows <= 64,
               "rows 0..31 and 32..kRows-1 are summed by two warps");
 
@@ -201,8 +197,8 @@ struct RowSmem {
     float qv[2][kTileCells][8];        // quadrant trees per tile cell (rb * 8 + cc)
     uint32_t rsum[2][kTileCells];      // raw IR total per tile cell
     int flag[2][kTileCells];           // 0: no complete epoch cell, 1: failing, 2: passing
-    double2 tq[2][kTileCells][4];      // finished terms of a tile's cells (by tile parity)
-    int tok[2][kTileCells];            // 1: the cell's terms count (passing)
+    double2 tq[kTileCells][4];         // finished terms of the previous tile's cells
+    int tok[kTileCells];               // 1: the cell's terms count (passing)
 };
 
 __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
@@ -264,7 +260,7 @@ __global__ void __launch_bounds__(kRowWarps * 32, 1)
     double rv2 = 0.0, ri2 = 0.0, rw2 = 0.0;  // row r0 + 32 + lane (lanes < kRows - 32)
     const int lane2 = lane < kRows - 32 ? lane + 32 : lane;
     double den = 0.0, num = 0.0;  // lane rb < kRowBlocks: epoch (r0 / 8 + rb) sums
-    for (int t = 0; t <= tiles + 1; ++t) {
+    for (int t = 0; t <= tiles; ++t) {
         asm volatile("cp.async.wait_group 0;\n" ::);
         __syncthreads();  // tile t staged; tile t-1's products complete
         stage(t + 1);
@@ -358,14 +354,12 @@ __global__ void __launch_bounds__(kRowWarps * 32, 1)
                 }
             }
         }
-        if (warp >= kRowWarps - 5 && warp <= kRowWarps - 2 && t > 0 && t <= tiles) {
-            // finish the previous tile's epoch cells: warps 11..14 (products
-            // only otherwise), ten cells each
+        if (warp == 0 && t > 0) {
+            // finish the previous tile's epoch cells (lane = tile cell)
             const int u = t - 1, ub = u & 1;
-            const int cl = (warp - (kRowWarps - 5)) + 4 * lane;
-            if (lane < 10 && cl < kTileCells) {
+            for (int cl = lane; cl < kTileCells; cl += 32) {
                 const int flag = S.flag[ub][cl];
-                S.tok[ub][cl] = flag == 2;
+                S.tok[cl] = flag == 2;
                 if (flag == 2) {
                     const float *qv = S.qv[ub][cl];
                     const float vq[4] = {qv[0], qv[1], qv[2], qv[3]};
@@ -373,30 +367,25 @@ __global__ void __launch_bounds__(kRowWarps * 32, 1)
                     double2 terms[4];
                     finish_terms(vq, iq, S.rsum[ub][cl], terms);
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) S.tq[ub][cl][q] = terms[q];
+                    for (int q = 0; q < 4; ++q) S.tq[cl][q] = terms[q];
                 }
             }
-        }
-        if (warp == 0 && t > 1) {
-            // the epoch sums of tile t-2, whose cells were finished in the
-            // previous iteration (producer_parameters.py epoch cell order):
-            // cells in column order, quadrants in order, passing cells only
-            const int vb = (t - 2) & 1;
+            __syncwarp();
+            // the epoch sums (producer_parameters.py epoch cell order): cells
+            // in column order, quadrants in order, passing cells only
             if (lane < kRowBlocks) {
                 for (int cc = 0; cc < 8; ++cc) {
                     const int cl = lane * 8 + cc;
-                    if (S.tok[vb][cl]) {
+                    if (S.tok[cl]) {
 #pragma unroll
                         for (int q = 0; q < 4; ++q) {
-                            den += S.tq[vb][cl][q].x;
-                            num += S.tq[vb][cl][q].y;
+                            den += S.tq[cl][q].x;
+                            num += S.tq[cl][q].y;
                         }
                     }
                 }
             }
-        }
-        if (warp == 0 && t > 0 && t <= tiles) {
-            const int u = t - 1;
+            __syncwarp();
             // the ordered row sums of rows 0..31 (one row per lane)
             const int n = min(kRowTile, active_width - u * kRowTile);
             const double *pv = S.p[u & 1][0][lane];
@@ -417,7 +406,7 @@ __global__ void __launch_bounds__(kRowWarps * 32, 1)
                 }
             }
         }
-        if (warp == kRowWarps - 1 && t > 0 && t <= tiles && lane < kRows - 32) {
+        if (warp == kRowWarps - 1 && t > 0 && lane < kRows - 32) {
             // the ordered row sums of rows 32..kRows-1, beside warp 0 (the
             // previous tile's products stay in their buffer until tile t+1's)
             const int u = t - 1;
