@@ -535,30 +535,42 @@ __global__ void __launch_bounds__(Tile<TH>::THREADS, Tile<TH>::BLOCKS_PER_SM)
     if (tid == 0) S.nrec = 0;
 
     // ---- stage the tile ---------------------------------------------------
-    // 16-byte copies, 11 per staged row: rows 0..PR-1 score, PR..2PR-1 waux
-    // (padded rows y0..), then 3 x RR rgb rows and RR aux rows (padded rows
-    // y0+1..).  All requests are in flight at once; one wait covers them.
+    // 16-byte copies, 11 per staged row, in two groups: first what the
+    // decision reads (PR score rows from padded row y0, RR aux rows from
+    // padded row y0+1), then the waux rows and the 3 x RR rgb rows.  The
+    // decision runs while the second group is in flight.
     {
-        constexpr int kRows = 2 * PR + 4 * RR, kVec = T::SW / 4;
+        constexpr int kVec = T::SW / 4;
         const int64_t col = x0;
-        for (int i = tid; i < kRows * kVec; i += NT) {
+        constexpr int kRowsA = PR + RR, kRowsB = PR + 3 * RR;
+        for (int i = tid; i < kRowsA * kVec; i += NT) {
+            const int row = i / kVec, v = i % kVec;
+            const bool score = row < PR;
+            const int r = score ? row : row - PR;
+            const float *src = (score ? hs + (int64_t)(y0 + r) * g.pitch
+                                      : auxp + (int64_t)(y0 + 1 + r) * g.pitch) + col;
+            float *dst = score ? S.hs[r] : S.auxt[r];
+            const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst + 4 * v);
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src + 4 * v));
+        }
+        asm volatile("cp.async.commit_group;\n" ::);
+        for (int i = tid; i < kRowsB * kVec; i += NT) {
             const int row = i / kVec, v = i % kVec;
             const float *src;
             float *dst;
-            if (row < 2 * PR) {
-                const int r = row < PR ? row : row - PR;
-                src = (row < PR ? hs : hwa) + (int64_t)(y0 + r) * g.pitch + col;
-                dst = row < PR ? S.hs[r] : S.hwa[r];
+            if (row < PR) {
+                src = hwa + (int64_t)(y0 + row) * g.pitch + col;
+                dst = S.hwa[row];
             } else {
-                const int q = row - 2 * PR, k = q / RR, r = q % RR;  // k 0..2 rgb, 3 aux
-                src = (k < 3 ? hwr + k * plane : auxp) + (int64_t)(y0 + 1 + r) * g.pitch + col;
-                dst = k < 3 ? S.hwr[k][r] : S.auxt[r];
+                const int q = row - PR, k = q / RR, r = q % RR;  // rgb plane k
+                src = hwr + k * plane + (int64_t)(y0 + 1 + r) * g.pitch + col;
+                dst = S.hwr[k][r];
             }
             const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst + 4 * v);
             asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src + 4 * v));
         }
         asm volatile("cp.async.commit_group;\n" ::);
-        asm volatile("cp.async.wait_group 0;\n" ::);
+        asm volatile("cp.async.wait_group 1;\n" ::);  // the first group
     }
     const float thr = p.decision_threshold;
     __syncthreads();
@@ -616,7 +628,10 @@ __global__ void __launch_bounds__(Tile<TH>::THREADS, Tile<TH>::BLOCKS_PER_SM)
         const uint32_t bal = __ballot_sync(0xFFFFFFFFu, eligible);
         if (dtx == 0) S.rowbal[dty] = bal;
     }
-    if (!__syncthreads_or(eligible)) return;  // no attempted pixel in the tile
+    if (!__syncthreads_or(eligible)) {  // no attempted pixel in the tile
+        asm volatile("cp.async.wait_group 0;\n" ::);  // no copy outlives the block
+        return;
+    }
 
     // The record positions an attempted pixel reads, listed densely (any
     // order: each record is computed alone): record row r is the centre row
@@ -634,6 +649,9 @@ __global__ void __launch_bounds__(Tile<TH>::THREADS, Tile<TH>::BLOCKS_PER_SM)
         if (r >= 2) need |= (unsigned long long)S.rowbal[r - 2] << 1;
         if ((need >> c) & 1ull) S.reclist[atomicAdd(&S.nrec, 1)] = (uint16_t)i;
     }
+
+    asm volatile("cp.async.wait_group 0;\n" ::);  // the waux and rgb rows
+    __syncthreads();
 
     // One work item is a vertical run of column sums in one column: the
     // samples are loaded and widened once and shared by the run's chains.
