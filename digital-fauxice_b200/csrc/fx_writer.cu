@@ -778,18 +778,17 @@ __global__ void __launch_bounds__(kSegThreads, kApplyBlocksPerSM)
     const DitherConst dc = dither_const(p);
     unsigned long long att = 0, written = 0, changed = 0, draws_total = 0;
     bool ok = true;
-    // segments by ticket: the tables above are loaded once per block.  The
-    // next segment's ticket and meta bytes are fetched before the current
-    // segment's dense phase, so their latency hides behind it.
-    if (threadIdx.x == 0) s_seg = atomicAdd(&ctr->apply_next, 1ull);
-    __syncthreads();
-    int64_t seg = (int64_t)s_seg;
-    uint8_t m[kPer];
-    load_meta(meta, seg * kSegment + threadIdx.x * kPer, sites, m);
+    // segments by ticket: the tables above are loaded once per block
     for (;;) {
+        __syncthreads();  // the previous segment's list and ticket are consumed
+        if (threadIdx.x == 0) s_seg = atomicAdd(&ctr->apply_next, 1ull);
+        __syncthreads();
+        const int64_t seg = (int64_t)s_seg;
         if (seg >= segs) break;
         const int64_t seg0 = seg * kSegment;
         const int64_t first = seg0 + threadIdx.x * kPer;
+        uint8_t m[kPer];
+        load_meta(meta, first, sites, m);
         // one block scan gives each thread its sites' chain offsets (fixed
         // draws, RNG-dependent channels) and its first slot in the list of
         // attempted public sites: (fixed << 40 | channels << 20 | attempted)
@@ -834,11 +833,7 @@ __global__ void __launch_bounds__(kSegThreads, kApplyBlocksPerSM)
                 A += meta_amb(mi);
             }
         }
-        if (threadIdx.x == 0) s_seg = atomicAdd(&ctr->apply_next, 1ull);
         __syncthreads();
-        const int64_t next = (int64_t)s_seg;
-        uint8_t m_next[kPer];
-        load_meta(meta, next * kSegment + threadIdx.x * kPer, sites, m_next);
 
         // ---- phase 2: attempted sites, densely ----------------------------------
         for (uint32_t k = threadIdx.x; k < listed; k += kSegThreads) {
@@ -903,10 +898,6 @@ __global__ void __launch_bounds__(kSegThreads, kApplyBlocksPerSM)
             o[2] = e[2];
             if (changed_out) changed_out[pixel] = ch ? 1 : 0;
         }
-        __syncthreads();  // the list is consumed before the next segment's
-        seg = next;
-#pragma unroll
-        for (int i = 0; i < kPer; ++i) m[i] = m_next[i];
     }
     if (!ok) raise_error(err, FX_ERR_NONFINITE_WORK);
     // the four counters in one reduction: warps, then thread 0
