@@ -449,13 +449,16 @@ struct Tile {
 };
 
 // A feature record of the stencil (streaming.py:236-308): the four feature
-// values and the W of its score patch (the consumer's weights when it is the
-// centre record).  A lane that takes the consumer row's fallback value holds
-// kFallbackBits, a NaN: the feature values are quotients and aux values of
-// finite planes, never NaN, so the marker cannot collide with a value.
-struct StencilRecord {
-    float a[4];
-    float w[3];
+// values (one 16-byte vector, read by a consumer pixel in one load) and the
+// W of its score patch (the consumer's weights when it is the centre
+// record), kept in three separate planes.  A lane that takes the consumer
+// row's fallback value holds kFallbackBits, a NaN: the feature values are
+// quotients and aux values of finite planes, never NaN, so the marker
+// cannot collide with a value.
+template <int CR, int RECC>
+struct StencilRecords {
+    float4 a[CR][RECC];
+    float w[3][CR][RECC];
 };
 constexpr uint32_t kFallbackBits = 0x7FC0FB00u;
 
@@ -467,7 +470,7 @@ struct StencilSmem {
     __align__(16) float hs[T::PR][T::SW];
     union __align__(16) {
         float hwa[T::PR][T::SW];                // waux tile: dead after the column sums
-        StencilRecord rec[T::CR][T::RECC];      // written by the records phase
+        StencilRecords<T::CR, T::RECC> rec;     // written by the records phase
     };
     __align__(16) float hwr[3][T::RR][T::SW];   // staged column j: logical col j - RO
     float cs[2][5][T::CR][T::CC];               // [score|waux][S3,S5,S7,S9,B16]
@@ -703,11 +706,11 @@ __global__ void __launch_bounds__(Tile<TH>::THREADS, Tile<TH>::BLOCKS_PER_SM)
         const int i = S.reclist[k];
         const int r = i / RECC, c = i % RECC;
         const int xx = x0 - 1 + c;
-        StencilRecord rec;
+        float ra[4], rw[3];
         if (xx < 0 || xx >= w) {
             // horizontal guard records stay zero (streaming.py:281-282)
-            rec.a[0] = rec.a[1] = rec.a[2] = rec.a[3] = 0.0f;
-            rec.w[0] = rec.w[1] = rec.w[2] = 0.0f;
+            ra[0] = ra[1] = ra[2] = ra[3] = 0.0f;
+            rw[0] = rw[1] = rw[2] = 0.0f;
         } else {
             double wq[3], nq[3];
 #pragma unroll
@@ -730,13 +733,16 @@ __global__ void __launch_bounds__(Tile<TH>::THREADS, Tile<TH>::BLOCKS_PER_SM)
             const float point_score = S.hs[r + 4][c + 4];
 #pragma unroll
             for (int l = 0; l < 3; ++l) {
-                rec.a[l] = wq[l] > 0.0 ? (float)(nq[l] / wq[l]) : __uint_as_float(kFallbackBits);
-                rec.w[l] = (float)wq[l];
+                ra[l] = wq[l] > 0.0 ? (float)(nq[l] / wq[l]) : __uint_as_float(kFallbackBits);
+                rw[l] = (float)wq[l];
             }
-            rec.a[3] = point_score > 0.0f ? S.auxt[r + 3][c + 3 + RO]  // xx is inside the row
-                                          : __uint_as_float(kFallbackBits);
+            ra[3] = point_score > 0.0f ? S.auxt[r + 3][c + 3 + RO]  // xx is inside the row
+                                       : __uint_as_float(kFallbackBits);
         }
-        S.rec[r][c] = rec;
+        S.rec.a[r][c] = make_float4(ra[0], ra[1], ra[2], ra[3]);
+        S.rec.w[0][r][c] = rw[0];
+        S.rec.w[1][r][c] = rw[1];
+        S.rec.w[2][r][c] = rw[2];
     }
     __syncthreads();
 
@@ -779,19 +785,19 @@ __global__ void __launch_bounds__(Tile<TH>::THREADS, Tile<TH>::BLOCKS_PER_SM)
     const int rr[5] = {ty + 1, ty + 1, ty + 1, ty, ty + 2};
     const int rc[5] = {tx + 1, tx, tx + 2, tx + 1, tx + 1};
     for (int k = 0; k < records; ++k) {
-        const StencilRecord &rec = S.rec[rr[k]][rc[k]];
+        const float4 q = S.rec.a[rr[k]][rc[k]];
+        const float rec_a[4] = {q.x, q.y, q.z, q.w};
 #pragma unroll
         for (int l = 0; l < 4; ++l)
-            feats[k][l] = __float_as_uint(rec.a[l]) == kFallbackBits ? fallback : rec.a[l];
+            feats[k][l] = __float_as_uint(rec_a[l]) == kFallbackBits ? fallback : rec_a[l];
     }
     // W of the centre record (record row ty + 1, column tx + 1): the score
     // patch averages its record phase computed, and the point score
     float weights[4];
     {
-        const StencilRecord &centre = S.rec[ty + 1][tx + 1];
-        weights[0] = centre.w[0];
-        weights[1] = centre.w[1];
-        weights[2] = centre.w[2];
+        weights[0] = S.rec.w[0][ty + 1][tx + 1];
+        weights[1] = S.rec.w[1][ty + 1][tx + 1];
+        weights[2] = S.rec.w[2][ty + 1][tx + 1];
         weights[3] = S.hs[ty + 5][tx + 5];
     }
 
