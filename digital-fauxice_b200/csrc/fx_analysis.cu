@@ -443,7 +443,7 @@ struct Tile {
     static constexpr int RECC = TW + 2;  // record cols (x0-1 .. x0+TW)
     static constexpr int SW = 44;        // staged floats per row (11 x 16 bytes)
     static constexpr int RO = 1;         // staged column of rgb / decision col 0
-    static constexpr int WA_RUN = TH == 8 ? 10 : 6;  // score / waux column-sum run
+    static constexpr int WA_RUN = TH == 8 ? 5 : 6;  // score / waux column-sum run
     static constexpr int RGB_RUN = 4;               // rgb column-sum run
     static constexpr int BLOCKS_PER_SM = TH == 8 ? 4 : 2;
 };
