@@ -183,3 +183,35 @@ def test_warm_slots_are_sized_for_the_largest_request():
     big = dev.frame_bytes(100, 100)
     assert sorted(dev.arena)[-2:] == [big, big]
     assert dev.grows == 0
+
+
+def test_a_blocking_device_call_is_reported_and_gc_is_restored():
+    """A device call that blocks the single-threaded loop shows up in the
+    report (slowest call per kind, calls over 20 ms); the loop runs without
+    cyclic garbage collection and turns it back on afterwards."""
+
+    import gc
+    import time
+
+    class SlowSubmit(FakeDevice):
+        def __init__(self, slots):
+            super().__init__(slots)
+            self.slow_once = True
+
+        def submit(self, st):
+            if self.slow_once:
+                self.slow_once = False
+                time.sleep(0.03)
+            return super().submit(st)
+
+    dev = SlowSubmit(2)
+    sizes = [(10, 10), (12, 12), (14, 14)]
+    assert gc.isenabled()
+    report = serve.serve(None, _fake_requests(sizes, 0.001), max_slots=2,
+                         budget_bytes=1 << 30, warm_slots=0, device=dev)
+    assert gc.isenabled()
+    summary = report.summary()
+    assert summary["calls_over_20ms"] >= 1
+    assert summary["slowest_call_ms"]["submit"] >= 20.0
+    assert summary["longest_stalls"][0][1] == "submit"
+    assert summary["capacity_reruns"] == 0
