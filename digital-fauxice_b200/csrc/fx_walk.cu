@@ -14,7 +14,8 @@
 // A wave of segments is one launch of k_wave.  Its window blocks each walk
 // one segment for a window of candidate E_in values around the predicted
 // value (expected extras from the exact state-space measure of every copy
-// set), merging candidates as they meet and compacting the survivors, and
+// set, summed per segment by k_coef), merging candidates as they meet and
+// compacting the survivors, and
 // write a dense E_in -> E_out table and a compact survivor list.  Block 0
 // chains the exact E through the wave with one list read per segment, each
 // segment as soon as its window block has finished (per-segment completion
